@@ -1,0 +1,331 @@
+/*
+ * merle_b200.h - C ABI of the B200 (sm_100a) fused bitmap-index query engine.
+ *
+ * The hot path this library implements is the reference's fused bitmap-index
+ * query path:
+ *   1. bitmap-index creation over fact columns (bmpidx_create.cu:14-136,
+ *      kernels primitive.cuh:88-118);
+ *   2. the virtual bitmap program (VBP) that combines predicate bitmaps with
+ *      AND / OR / NOT / ANDM / ORM without materialising intermediates
+ *      (primitive.cuh:165-338);
+ *   3. the fused dimension join-probe plus group-by SUM (primitive.cuh:340-445
+ *      driving the op functors of ssb/lambdas.cuh:19-152 and synth/synthdemo.cu:7-53).
+ *
+ * Conventions (all entry points):
+ *  - Every function returns an mb_status; on failure mb_last_error() gives a
+ *    thread-local message.  Nothing calls exit() and no kernel traps.
+ *  - Pointers documented as "device" are CUDA device addresses; "host" are
+ *    host addresses.  `stream` is a cudaStream_t passed as void* (NULL = legacy
+ *    default stream).  Asynchronous calls return once the work is enqueued.
+ *  - Bitmaps: bit i of 32-bit word w is row 32*w + i (LSB first), as the
+ *    reference's __ballot_sync layout (primitive.cuh:96-98).  A bitmap over n
+ *    rows has mb_bitmap_words(n) = ceil(n/32) words; bits of rows >= n are 0.
+ *    Bitmaps produced by this library are padded to mb_bitmap_stride(n) words
+ *    (a multiple of 32 words) and 256-byte aligned.
+ *  - Group results are int64 sums (two's complement wrap), where the reference
+ *    sums uint32 (primitive.cuh:395,444): (uint32)result equals the reference's
+ *    value on the same inputs.
+ */
+#ifndef MERLE_B200_H
+#define MERLE_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+/* Symbols of the shared library are exported with default visibility; the
+ * library is compiled with -fvisibility=hidden so nothing else leaks. */
+#if defined(MB_BUILDING_LIBRARY) && defined(__GNUC__)
+#define MB_API __attribute__((visibility("default")))
+#else
+#define MB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Status                                                                    */
+/* ------------------------------------------------------------------------- */
+typedef enum mb_status {
+  MB_OK = 0,
+  MB_ERR_INVALID = 1,     /* bad argument, limit exceeded, misaligned pointer */
+  MB_ERR_OOM = 2,         /* device or host allocation failed */
+  MB_ERR_CUDA = 3,        /* a CUDA runtime call or launch failed */
+  MB_ERR_TIMEOUT = 4,     /* a bounded device-side wait ran out */
+  MB_ERR_UNSUPPORTED = 5, /* feature not available in this build */
+  MB_ERR_IO = 6           /* file open / read / write failed */
+} mb_status;
+
+/* Thread-local message for the last failing call on this thread. */
+MB_API const char *mb_last_error(void);
+/* Library version string. */
+MB_API const char *mb_version(void);
+
+/* Words of a bitmap over n rows: ceil(n / 32) (bmpidx_create.cu:40). */
+MB_API uint64_t mb_bitmap_words(uint64_t nrows);
+/* Padded word stride this library uses between bitmaps of one slab. */
+MB_API uint64_t mb_bitmap_stride(uint64_t nrows);
+
+/* ------------------------------------------------------------------------- */
+/* Limits (the reference's are MAXBIN_PERCOL=4, MAXCOLS=4, MAXNINSTR=6,      */
+/* primitive.cuh:121; these are raised so that e.g. a 25-bin OR fits)       */
+/* ------------------------------------------------------------------------- */
+#define MB_MAXCOLS 8     /* memory operands of one program */
+#define MB_MAXBINS 64    /* middle bins of one memory operand */
+#define MB_MAXPTRS 128   /* all bitmaps of one program */
+#define MB_MAXNINSTR 16  /* instructions of one program */
+#define MB_NREGS 4       /* virtual registers (reference: 3) */
+#define MB_MAXSRC 8      /* value sources of one op */
+#define MB_MAXCLAUSE 6   /* AND-ed filter clauses of one op */
+#define MB_MAXTERM 16    /* range terms over all clauses of one op */
+#define MB_MAXKEY 4      /* group-key fields of one op */
+
+/* ------------------------------------------------------------------------- */
+/* Virtual bitmap program (primitive.cuh:135-198)                            */
+/* ------------------------------------------------------------------------- */
+/* Opcodes keep the reference's numbering (enum ops, primitive.cuh:169-173). */
+typedef enum mb_opcode {
+  MB_END = 0,  /* no more instructions */
+  MB_AND = 1,  /* r[dst] &= r[src1] */
+  MB_OR = 2,   /* r[dst] |= r[src1] */
+  MB_NOT = 3,  /* r[dst] = ~r[src1] */
+  MB_ANDM = 4, /* r[dst] &= OR of the bins of cols[src1] */
+  MB_ORM = 5   /* r[dst] |= OR of the bins of cols[src1] */
+} mb_opcode;
+
+/* One instruction (struct vprg::instr, primitive.cuh:176-181). */
+typedef struct mb_instr {
+  uint8_t opcode, dstreg, src1, src2;
+} mb_instr;
+
+/* Bitmap index of one column restricted to a query range (struct col,
+ * primitive.cuh:135-162): middle bins lie inside the range; leftmost and
+ * rightmost are edge bins that need the candidate check. */
+typedef struct mb_col {
+  uint32_t nmiddle;                /* <= MB_MAXBINS */
+  const uint32_t *const *middle;   /* host array of nmiddle device bitmaps */
+  const uint32_t *leftmost;        /* device bitmap or NULL */
+  const uint32_t *rightmost;       /* device bitmap or NULL */
+} mb_col;
+
+/* The program (struct vprg, primitive.cuh:165-198).  The result is r0.  The
+ * instruction list ends at the first MB_END or after MB_MAXNINSTR. */
+typedef struct mb_vprg {
+  uint64_t factsz;                 /* rows */
+  uint32_t ncols;                  /* memory operands in use */
+  mb_col cols[MB_MAXCOLS];
+  mb_instr instrs[MB_MAXNINSTR];
+} mb_vprg;
+
+/* 1 if no operand has an edge bin (vprg::is_nochk, primitive.cuh:190-195). */
+MB_API int mb_vprg_is_nochk(const mb_vprg *p);
+
+/* ------------------------------------------------------------------------- */
+/* Query operator (the op functors of ssb/lambdas.cuh:19-152 and             */
+/* synth/synthdemo.cu:7-53, restated declaratively so they cross a C ABI)    */
+/* ------------------------------------------------------------------------- */
+/* A value source: a fact column read at the row, or a dimension attribute
+ * read through a foreign key: dim[fk[row]] (the join probe). */
+typedef struct mb_src {
+  const void *col;      /* device: fact column, or dimension array when fk != NULL */
+  const uint32_t *fk;   /* device foreign-key fact column, or NULL */
+  uint64_t dimsz;       /* fk != NULL and dimsz != 0: keys >= dimsz eliminate the row */
+  uint32_t width;       /* element bytes: 1, 2, 4 or 8 (unsigned) */
+  uint32_t pad_;
+} mb_src;
+
+/* Range term lo <= value < hi (all reference ranges are half-open). */
+typedef struct mb_term {
+  uint32_t src;
+  uint32_t pad_;
+  uint64_t lo, hi;
+} mb_term;
+
+/* Group-key field: mul * (xform(value) - base), summed over fields in uint32
+ * arithmetic (the mixed-radix group indices of s2op..s4op). */
+typedef enum mb_xform {
+  MB_X_ID = 0,   /* value */
+  MB_X_DIV = 1,  /* value / div (the /10 nation and /40 category scaling) */
+  MB_X_YEAR = 2  /* ssbDateToYear(value) (ssb/ssbdemo.h:28-39) */
+} mb_xform;
+
+typedef struct mb_key {
+  uint32_t src, xform, div, base, mul;
+} mb_key;
+
+typedef enum mb_vkind {
+  MB_V_ONE = 0,  /* COUNT: value 1 */
+  MB_V_COL = 1,  /* src[va] */
+  MB_V_MUL = 2,  /* src[va] * src[vb] (int64, exact) */
+  MB_V_SUB = 3   /* src[va] - src[vb] (int64, exact) */
+} mb_vkind;
+
+/* The operator applied to every selected row (op(row, chk) of
+ * primitive.cuh:383-384,431-432).  When the row is uncertain (chk) all filter
+ * clauses are re-evaluated: the row passes if every clause has a satisfied
+ * term.  The group index is the key sum; indices >= nr_grp eliminate the row
+ * (primitive.cuh:34,385,433). */
+typedef struct mb_op {
+  uint32_t nsrc;
+  mb_src src[MB_MAXSRC];
+  uint32_t nclause;
+  uint32_t clause_len[MB_MAXCLAUSE];   /* terms of each clause, in order */
+  mb_term terms[MB_MAXTERM];
+  uint32_t nkey;
+  mb_key keys[MB_MAXKEY];
+  uint32_t vkind, va, vb;
+  uint32_t pad_;
+} mb_op;
+
+/* ------------------------------------------------------------------------- */
+/* Launch / plan knobs for the fused kernel                                  */
+/* ------------------------------------------------------------------------- */
+typedef enum mb_grp_strategy {
+  MB_GRP_AUTO = 0,
+  MB_GRP_SHARED = 1,  /* dense per-CTA shared-memory partial table */
+  MB_GRP_GLOBAL = 2,  /* warp-aggregated atomics straight into global memory */
+  MB_GRP_HASH = 3     /* per-CTA shared-memory hash table over (group, sum),
+                         for large group domains that few rows touch */
+} mb_grp_strategy;
+
+typedef struct mb_launch {
+  uint32_t grp_strategy;  /* mb_grp_strategy */
+  uint32_t warps_per_cta; /* 0 = auto (4 / 8 / 16) */
+  uint32_t ctas_per_sm;   /* 0 = auto (occupancy) */
+  uint32_t words_per_lane;/* 0 = auto; 1, 2 or 4 bitmap words per lane */
+} mb_launch;
+
+/* ------------------------------------------------------------------------- */
+/* L2 kernels over raw device buffers                                        */
+/* ------------------------------------------------------------------------- */
+
+/* One pass over a column writes nbins bin bitmaps, bin j = [lo[j], hi[j])
+ * (create_bin, bmpidx_create.cu:14-56, kernel primitive.cuh:102-118).  When
+ * src->fk != NULL the value is dim[fk[row]] and keys >= dimsz give no bit
+ * (bmpidx_create.cu:26-27).  out: device, nbins bitmaps at a stride of
+ * `stride_words` words (>= mb_bitmap_words(n), multiple of 4); popcounts:
+ * optional device uint64[nbins] (accumulated: zero it first), or NULL. */
+MB_API mb_status mb_bitmap_create(const mb_src *src, uint64_t nrows, const uint64_t *lo,
+                           const uint64_t *hi, uint32_t nbins, uint32_t *out,
+                           uint64_t stride_words, uint64_t *popcounts, void *stream);
+
+/* Materialised stage 1 (abla::_stg1, primitive_abla.cuh:262-288): runs the
+ * program and writes the possible bitmap (and, when chk, the uncertain one).
+ * chk selects vprg::chk vs vprg::nochk semantics.  popcount: optional device
+ * uint64 (accumulated) of possible bits. */
+MB_API mb_status mb_vprg_eval(const mb_vprg *p, int chk, uint32_t *possible,
+                       uint32_t *uncertain, uint64_t *popcount, void *stream);
+
+/* Materialised stage 2 (abla::_stg2, primitive_abla.cuh:290-354): bitmap to a
+ * row-id list in ascending row order; uncertain rows carry bit 31
+ * (primitive_abla.cuh:346).  count: device uint64, set (not accumulated).
+ * rows: device, capacity >= popcount of `possible`. */
+MB_API mb_status mb_bitmap_to_rows(const uint32_t *possible, const uint32_t *uncertain,
+                            uint64_t nrows, uint32_t *rows, uint64_t *count,
+                            void *stream);
+
+/* Materialised stage 3 (abla::_stg3, primitive_abla.cuh:356-394): applies the
+ * op to a row list and aggregates.  The row count is read on the device (no
+ * host round trip, unlike primitive_abla.cuh:437).  out: device int64[nr_grp]
+ * and qualifying-row count: device uint64; both overwritten. */
+MB_API mb_status mb_rows_grpby(const uint32_t *rows, const uint64_t *count, uint64_t capacity,
+                        const mb_op *op, uint32_t nr_grp, int64_t *out,
+                        uint64_t *nqual, void *stream);
+
+/* The fused kernel (vprg_grpby, primitive.cuh:340-445): program -> compaction
+ * -> op -> group-by in one launch.  Uses the chk algebra iff the program has
+ * edge bins.  out: device int64[nr_grp], nqual: device uint64 (rows
+ * aggregated); both overwritten.  launch may be NULL (auto). */
+MB_API mb_status mb_vprg_grpby(const mb_vprg *p, const mb_op *op, uint32_t nr_grp,
+                        int64_t *out, uint64_t *nqual, const mb_launch *launch,
+                        void *stream);
+
+/* No-index plan (grpby, primitive.cuh:16-48): every row runs the op with the
+ * candidate check on.  out / nqual as mb_vprg_grpby. */
+MB_API mb_status mb_join_grpby(uint64_t nrows, const mb_op *op, uint32_t nr_grp,
+                        int64_t *out, uint64_t *nqual, void *stream);
+
+/* ------------------------------------------------------------------------- */
+/* Host planning helpers of the reference's operator API                     */
+/* ------------------------------------------------------------------------- */
+/* col::from_bin (bmpidx_create.cu:138-163): maps [min, max) onto bins
+ * bins[0..nbin) with bounds[0..nbin]: bins fully inside become middle bins,
+ * partially covered end bins become leftmost / rightmost (candidate check).
+ * An empty col (nmiddle 0, no edges) means the range is not coverable.
+ * `mid_storage` (host, MB_MAXBINS entries) receives the middle pointers and
+ * out->middle points into it.  Host-only: never dereferences the bitmaps.
+ * Returns MB_ERR_INVALID if more than MB_MAXBINS middle bins are needed (the
+ * reference silently overflows its 4-entry array, primitive.cuh:155). */
+MB_API mb_status mb_col_from_bin(uint32_t nbin, const uint32_t *const *bins,
+                                 const uint64_t *bounds, uint64_t min, uint64_t max,
+                                 mb_col *out, const uint32_t **mid_storage);
+
+/* col::from_bin2 (bmpidx_create.cu:165-173): coarse bins first; if they need a
+ * candidate check, the fine bins instead. */
+MB_API mb_status mb_col_from_bin2(uint32_t nc, const uint32_t *const *coarse,
+                                  const uint64_t *cbounds, uint32_t nf,
+                                  const uint32_t *const *fine, const uint64_t *fbounds,
+                                  uint64_t min, uint64_t max, mb_col *out,
+                                  const uint32_t **mid_storage);
+
+/* struct recipe (primitive.cuh:448-474): per-query bitmaps for up to
+ * MB_RECIPE_COLS predicates, built on the device from a column (fk == NULL,
+ * create_select) or a dimension attribute through a foreign key (create_join,
+ * keys >= dimsz give no bit; 0xffffffff = no check). */
+#define MB_RECIPE_COLS 4
+typedef struct mb_recipe {
+  uint64_t factsz;
+  uint32_t nbit[MB_RECIPE_COLS];          /* attribute bits: <=8, <=16, <=32, <=64 */
+  uint32_t min[MB_RECIPE_COLS], max[MB_RECIPE_COLS], dimsz[MB_RECIPE_COLS];
+  const uint32_t *fk[MB_RECIPE_COLS];     /* device */
+  const void *attr[MB_RECIPE_COLS];       /* device; NULL = unused */
+} mb_recipe;
+
+typedef enum mb_recipe_kind {
+  MB_RECIPE_PERFECT = 0, /* recipe::perfect, bmpidx_create.cu:228-239 */
+  MB_RECIPE_MANY_OR = 1, /* recipe::many_or, bmpidx_create.cu:241-262 */
+  MB_RECIPE_CANDCHK = 2  /* recipe::candchk, bmpidx_create.cu:264-316 */
+} mb_recipe_kind;
+
+/* A program owning its bitmaps (allocated here; free with mb_owned_vprg_release). */
+typedef struct mb_owned_vprg {
+  mb_vprg prg;
+  const uint32_t *mid[MB_MAXCOLS][MB_MAXBINS]; /* storage of prg.cols[c].middle */
+  uint32_t *owned[MB_MAXPTRS];                 /* device bitmaps to free */
+  uint32_t nowned;
+} mb_owned_vprg;
+
+/* Builds the recipe's bitmaps (one mb_bitmap_create launch each, on `stream`)
+ * and the program with `instrs` (MB_MAXNINSTR entries, END-terminated). */
+MB_API mb_status mb_recipe_build(const mb_recipe *r, int kind, const mb_instr *instrs,
+                                 mb_owned_vprg *out, void *stream);
+/* Frees the bitmaps of a recipe-built program (vprg::release, primitive.cuh:186-189). */
+MB_API mb_status mb_owned_vprg_release(mb_owned_vprg *p);
+
+/* ------------------------------------------------------------------------- */
+/* Synthetic data generation on the device (seeded, counter-based)           */
+/* ------------------------------------------------------------------------- */
+/* Flat 5-column int32 table a, b, c, d, e (any may be NULL), rows [row0, row0+n). */
+MB_API mb_status mb_gen_flat(uint64_t seed, uint64_t row0, uint64_t n, int32_t *a, int32_t *b,
+                      int32_t *c, int32_t *d, int32_t *e, void *stream);
+
+/* Star schema fact columns for rows [row0, row0 + n) at scale k.  Each output
+ * may be NULL.  width4 = 1: every fact column is 4 bytes (uint32); width4 = 0:
+ * the reference's ssb_schema widths (ssb/ssbdemo.h:41-49): orderdate u16,
+ * quantity/discount/suppcity u8, the rest u32. */
+typedef struct mb_star_cols {
+  void *custkey, *partkey, *suppkey, *orderdate, *quantity, *discount;
+  void *extendedprice, *revenue, *supplycost, *suppcity;
+} mb_star_cols;
+MB_API mb_status mb_gen_star(uint64_t seed, uint32_t k, uint64_t row0, uint64_t n,
+                      int width4, const mb_star_cols *out, void *stream);
+
+/* Star schema dimension arrays, indexed by key with the zero pad at 0:
+ * custcity (u8, ncust+1), suppcity (u8, nsupp+1), partmfgr (u16, npart+1). */
+MB_API mb_status mb_gen_star_dims(uint64_t seed, uint32_t k, uint8_t *custcity,
+                           uint8_t *suppcity, uint16_t *partmfgr, void *stream);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+#endif /* MERLE_B200_H */

@@ -1,0 +1,119 @@
+"""ctypes mirror of the C ABI in include/merle_b200.h.
+
+The structs below must stay byte-for-byte equal to the C declarations;
+tests/test_abi.py checks their sizes against the library's own view.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+MB_MAXCOLS = 8
+MB_MAXBINS = 64
+MB_MAXPTRS = 128
+MB_MAXNINSTR = 16
+MB_NREGS = 4
+MB_MAXSRC = 8
+MB_MAXCLAUSE = 6
+MB_MAXTERM = 16
+MB_MAXKEY = 4
+
+# mb_status
+MB_OK, MB_ERR_INVALID, MB_ERR_OOM, MB_ERR_CUDA, MB_ERR_TIMEOUT, MB_ERR_UNSUPPORTED, MB_ERR_IO = range(7)
+STATUS_NAMES = ["MB_OK", "MB_ERR_INVALID", "MB_ERR_OOM", "MB_ERR_CUDA", "MB_ERR_TIMEOUT",
+                "MB_ERR_UNSUPPORTED", "MB_ERR_IO"]
+
+# mb_opcode (the reference's enum ops, primitive.cuh:169-173)
+END, AND, OR, NOT, ANDM, ORM = range(6)
+# mb_xform
+X_ID, X_DIV, X_YEAR = range(3)
+# mb_vkind
+V_ONE, V_COL, V_MUL, V_SUB = range(4)
+# mb_grp_strategy
+GRP_AUTO, GRP_SHARED, GRP_GLOBAL, GRP_HASH = range(4)
+
+
+class mb_instr(C.Structure):
+    _fields_ = [("opcode", C.c_uint8), ("dstreg", C.c_uint8), ("src1", C.c_uint8), ("src2", C.c_uint8)]
+
+
+class mb_col(C.Structure):
+    _fields_ = [("nmiddle", C.c_uint32), ("middle", C.POINTER(C.c_void_p)),
+                ("leftmost", C.c_void_p), ("rightmost", C.c_void_p)]
+
+
+class mb_vprg(C.Structure):
+    _fields_ = [("factsz", C.c_uint64), ("ncols", C.c_uint32), ("cols", mb_col * MB_MAXCOLS),
+                ("instrs", mb_instr * MB_MAXNINSTR)]
+
+
+class mb_src(C.Structure):
+    _fields_ = [("col", C.c_void_p), ("fk", C.c_void_p), ("dimsz", C.c_uint64),
+                ("width", C.c_uint32), ("pad_", C.c_uint32)]
+
+
+class mb_term(C.Structure):
+    _fields_ = [("src", C.c_uint32), ("pad_", C.c_uint32), ("lo", C.c_uint64), ("hi", C.c_uint64)]
+
+
+class mb_key(C.Structure):
+    _fields_ = [("src", C.c_uint32), ("xform", C.c_uint32), ("div", C.c_uint32),
+                ("base", C.c_uint32), ("mul", C.c_uint32)]
+
+
+class mb_op(C.Structure):
+    _fields_ = [("nsrc", C.c_uint32), ("src", mb_src * MB_MAXSRC),
+                ("nclause", C.c_uint32), ("clause_len", C.c_uint32 * MB_MAXCLAUSE),
+                ("terms", mb_term * MB_MAXTERM),
+                ("nkey", C.c_uint32), ("keys", mb_key * MB_MAXKEY),
+                ("vkind", C.c_uint32), ("va", C.c_uint32), ("vb", C.c_uint32), ("pad_", C.c_uint32)]
+
+
+class mb_launch(C.Structure):
+    _fields_ = [("grp_strategy", C.c_uint32), ("warps_per_cta", C.c_uint32),
+                ("ctas_per_sm", C.c_uint32), ("words_per_lane", C.c_uint32)]
+
+
+class mb_star_cols(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("custkey", "partkey", "suppkey", "orderdate", "quantity",
+                                          "discount", "extendedprice", "revenue", "supplycost", "suppcity")]
+
+
+VOIDP = C.c_void_p
+U32 = C.c_uint32
+U64 = C.c_uint64
+I32 = C.c_int
+
+# name -> (restype, argtypes) of every C ABI entry point (include/merle_b200.h)
+SIGNATURES: dict[str, tuple] = {
+    "mb_last_error": (C.c_char_p, []),
+    "mb_version": (C.c_char_p, []),
+    "mb_bitmap_words": (U64, [U64]),
+    "mb_bitmap_stride": (U64, [U64]),
+    "mb_vprg_is_nochk": (I32, [C.POINTER(mb_vprg)]),
+    "mb_bitmap_create": (I32, [C.POINTER(mb_src), U64, C.POINTER(U64), C.POINTER(U64), U32, VOIDP, U64,
+                               VOIDP, VOIDP]),
+    "mb_vprg_eval": (I32, [C.POINTER(mb_vprg), I32, VOIDP, VOIDP, VOIDP, VOIDP]),
+    "mb_bitmap_to_rows": (I32, [VOIDP, VOIDP, U64, VOIDP, VOIDP, VOIDP]),
+    "mb_rows_grpby": (I32, [VOIDP, VOIDP, U64, C.POINTER(mb_op), U32, VOIDP, VOIDP, VOIDP]),
+    "mb_vprg_grpby": (I32, [C.POINTER(mb_vprg), C.POINTER(mb_op), U32, VOIDP, VOIDP,
+                            C.POINTER(mb_launch), VOIDP]),
+    "mb_join_grpby": (I32, [U64, C.POINTER(mb_op), U32, VOIDP, VOIDP, VOIDP]),
+    "mb_gen_flat": (I32, [U64, U64, U64, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP]),
+    "mb_gen_star": (I32, [U64, U32, U64, U64, I32, C.POINTER(mb_star_cols), VOIDP]),
+    "mb_gen_star_dims": (I32, [U64, U32, VOIDP, VOIDP, VOIDP, VOIDP]),
+}
+
+
+def bind(lib: C.CDLL, sigs: dict[str, tuple]) -> None:
+    for name, (res, args) in sigs.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+
+
+def header_symbols(header: Path) -> list[str]:
+    """Names of the functions declared MB_API in a C ABI header."""
+    import re
+    text = header.read_text()
+    return re.findall(r"^MB_API[^(]*?\b(\w+)\s*\(", text, flags=re.M)

@@ -1,0 +1,311 @@
+// bitmap.cu - one-pass multi-bin bitmap-index creation (mb_bitmap_create).
+//
+// Reference: create_bin (bmpidx_create.cu:14-56) launching the multi-bin
+// bmpcreate kernel (primitive.cuh:102-118): one thread per row, one
+// __ballot_sync per (row-word, bin), lane 0 storing each word to HBM.
+//
+// B200 design:
+//  - Persistent CTAs (SMs x occupancy) walk 4096-row tiles.  A 3-stage ring of
+//    column tiles is filled by 1-D TMA bulk copies (cp.async.bulk) with mbarrier
+//    completion, so HBM reads stream ahead of the compute.  For join bitmaps the
+//    staged column is the foreign key and the dimension value is gathered from
+//    the (L2-resident) dimension array.
+//  - Bins that partition a value range (equal-width, or sorted and disjoint)
+//    cost one bin lookup per row plus one __match_any_sync per 32-row word: the
+//    peer mask of a bin IS that bin's word.  Arbitrary (overlapping) bins fall
+//    back to one ballot per bin, as the reference does.
+//  - Words are assembled in a shared-memory tile [bin][128 words] and written
+//    out with coalesced 128-bit stores, instead of one 4-byte store per word.
+//  - The tail is exact: bits of rows >= n are zero (the reference's
+//    single-predicate kernel writes past the bitmap end, primitive.cuh:94-99,
+//    and its multi-bin kernel breaks out of a full-mask ballot,
+//    primitive.cuh:110-113; neither happens here).
+#include "common.cuh"
+#include "tma.cuh"
+
+namespace mb {
+
+constexpr int BC_THREADS = 256;
+constexpr int BC_TILE_ROWS = 4096;
+constexpr int BC_TILE_WORDS = BC_TILE_ROWS / 32;  // 128
+constexpr int BC_STAGES = 3;
+constexpr int BC_MAXBINS = 256;
+constexpr uint32_t BC_NOBIN = 0xffffffffu;
+
+enum { BC_BALLOT = 0, BC_EQUAL = 1, BC_SORTED = 2 };
+
+struct BinSpec {
+  uint32_t nbins;
+  uint32_t pad_;
+  uint64_t lo0, width;  // BC_EQUAL: bin = (v - lo0) / width
+  uint64_t lo[BC_MAXBINS], hi[BC_MAXBINS];
+};
+
+template <int MODE>
+__device__ __forceinline__ uint32_t find_bin(const BinSpec &S, uint64_t v) {
+  if (MODE == BC_EQUAL) {
+    if (v < S.lo0) return BC_NOBIN;
+    uint64_t d = v - S.lo0;
+    uint64_t b = S.width == 1 ? d : d / S.width;
+    return b < S.nbins ? (uint32_t)b : BC_NOBIN;
+  } else {  // BC_SORTED: last bin with lo <= v, then v < hi
+    if (v < S.lo[0]) return BC_NOBIN;
+    uint32_t lo = 0, hi = S.nbins - 1;
+    while (lo < hi) {
+      uint32_t mid = (lo + hi + 1) >> 1;
+      if (S.lo[mid] <= v) lo = mid; else hi = mid - 1;
+    }
+    return v < S.hi[lo] ? lo : BC_NOBIN;
+  }
+}
+
+template <int W>
+__device__ __forceinline__ uint64_t ld_smem_w(const uint8_t *p, uint32_t i) {
+  if (W == 1) return p[i];
+  if (W == 2) return reinterpret_cast<const uint16_t *>(p)[i];
+  if (W == 4) return reinterpret_cast<const uint32_t *>(p)[i];
+  return reinterpret_cast<const unsigned long long *>(p)[i];
+}
+
+// W: bytes of the staged column element (4 for join: the foreign key);
+// DW: bytes of the dimension element (join only).
+template <int W, bool JOIN, int DW, int MODE>
+__global__ void __launch_bounds__(BC_THREADS)
+bitmap_create_kernel(const __grid_constant__ BinSpec S, const void *__restrict__ col,
+                     const void *__restrict__ dim, uint64_t dimsz, uint64_t n,
+                     uint32_t *__restrict__ out, uint64_t stride,
+                     unsigned long long *__restrict__ pop, uint32_t *errw) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  constexpr uint32_t STAGE_BYTES = BC_TILE_ROWS * W;
+  uint8_t *stage = smem;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + BC_STAGES * STAGE_BYTES);
+  uint32_t *obuf = reinterpret_cast<uint32_t *>(smem + BC_STAGES * STAGE_BYTES + 128);
+  unsigned long long *cnt = reinterpret_cast<unsigned long long *>(obuf + S.nbins * BC_TILE_WORDS);
+
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t nwords = (n + 31) / 32;
+  const uint64_t ntiles = (n + BC_TILE_ROWS - 1) / BC_TILE_ROWS;
+  const uint8_t *colb = reinterpret_cast<const uint8_t *>(col);
+
+  if (pop)
+    for (uint32_t b = tid; b < S.nbins; b += BC_THREADS) cnt[b] = 0;
+  if (MODE != BC_BALLOT)
+    for (uint32_t i = tid; i < S.nbins * BC_TILE_WORDS; i += BC_THREADS) obuf[i] = 0;
+  if (tid == 0) {
+    for (int s = 0; s < BC_STAGES; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  // Bytes of tile t that the bulk copy moves: whole 16-byte chunks only.
+  auto tile_bulk_bytes = [&](uint64_t t) -> uint32_t {
+    uint64_t rows = n - t * BC_TILE_ROWS;
+    if (rows > BC_TILE_ROWS) rows = BC_TILE_ROWS;
+    return (uint32_t)((rows * W) & ~(uint64_t)15);
+  };
+  auto issue = [&](uint64_t t, int s) {
+    uint32_t bytes = tile_bulk_bytes(t);
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&bars[s], bytes);
+    if (bytes) bulk_g2s(stage + s * STAGE_BYTES, colb + t * (uint64_t)STAGE_BYTES, bytes, &bars[s]);
+  };
+
+  if (tid == 0) {
+    uint64_t t = blockIdx.x;
+    for (int s = 0; s < BC_STAGES && t < ntiles; ++s, t += gridDim.x) issue(t, s);
+  }
+
+  uint32_t it = 0;
+  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+    const int s = it % BC_STAGES;
+    const uint32_t parity = (it / BC_STAGES) & 1u;
+    // Every thread waits (bounded) for the stage; the block leaves together if
+    // any wait ran out, after one more bounded wait for the copy in flight.
+    const bool arrived = mbar_wait_bounded(&bars[s], parity, errw, MB_DEVERR_TMA_WAIT);
+    if (!__syncthreads_and(arrived)) {
+      if (tid == 0) mbar_wait_bounded(&bars[s], parity, nullptr, 0, 1u << 16);
+      return;
+    }
+    const uint8_t *sp = stage + s * STAGE_BYTES;
+    const uint32_t bulk_rows = tile_bulk_bytes(t) / W;
+    const uint64_t row0 = t * BC_TILE_ROWS;
+
+    for (uint32_t wi = warp; wi < BC_TILE_WORDS; wi += BC_THREADS / 32) {
+      const uint32_t r = wi * 32 + lane;
+      const uint64_t row = row0 + r;
+      bool valid = row < n;
+      uint64_t v = 0;
+      if (valid) {
+        uint64_t x = r < bulk_rows ? ld_smem_w<W>(sp, r) : load_width(col, row, W);
+        if (JOIN) {
+          if (dimsz != 0 && x >= dimsz) valid = false;
+          else v = load_width(dim, x, DW);
+        } else {
+          v = x;
+        }
+      }
+      if (MODE == BC_BALLOT) {
+        for (uint32_t b = 0; b < S.nbins; ++b) {
+          uint32_t m = __ballot_sync(0xffffffffu, valid && v >= S.lo[b] && v < S.hi[b]);
+          if (lane == (b & 31)) obuf[b * BC_TILE_WORDS + wi] = m;
+        }
+      } else {
+        uint32_t bin = valid ? find_bin<MODE>(S, v) : BC_NOBIN;
+        uint32_t peers = __match_any_sync(0xffffffffu, bin);
+        if (bin != BC_NOBIN && lane == (uint32_t)(__ffs(peers) - 1))
+          obuf[bin * BC_TILE_WORDS + wi] = peers;
+      }
+    }
+    __syncthreads();  // stage s fully read, obuf complete
+
+    if (tid == 0 && t + (uint64_t)BC_STAGES * gridDim.x < ntiles)
+      issue(t + (uint64_t)BC_STAGES * gridDim.x, s);
+
+    // Coalesced write-out: per bin 128 consecutive words = 32 x uint4.
+    const uint64_t w0 = t * BC_TILE_WORDS;
+    for (uint32_t i = tid; i < S.nbins * (BC_TILE_WORDS / 4); i += BC_THREADS) {
+      const uint32_t b = i / (BC_TILE_WORDS / 4), q = i % (BC_TILE_WORDS / 4);
+      const uint64_t w = w0 + q * 4;
+      if (w >= nwords) continue;  // obuf beyond the last word is never written
+      uint4 v4 = *reinterpret_cast<const uint4 *>(&obuf[b * BC_TILE_WORDS + q * 4]);
+      if (MODE != BC_BALLOT)  // leave the tile zeroed for the next one
+        *reinterpret_cast<uint4 *>(&obuf[b * BC_TILE_WORDS + q * 4]) = make_uint4(0, 0, 0, 0);
+      uint32_t *dst = out + b * stride + w;
+      if (w + 4 <= nwords) {
+        *reinterpret_cast<uint4 *>(dst) = v4;
+      } else {
+        dst[0] = v4.x;
+        if (w + 1 < nwords) dst[1] = v4.y;
+        if (w + 2 < nwords) dst[2] = v4.z;
+      }
+      if (pop) {
+        uint32_t c = __popc(v4.x) + __popc(v4.y) + __popc(v4.z) + __popc(v4.w);
+        if (c) atomicAdd(&cnt[b], (unsigned long long)c);
+      }
+    }
+    __syncthreads();  // obuf reused by the next tile
+  }
+  if (pop) {
+    __syncthreads();
+    for (uint32_t b = tid; b < S.nbins; b += BC_THREADS)
+      if (cnt[b]) atomicAdd(&pop[b], cnt[b]);
+  }
+}
+
+// ---------------------------------------------------------------- host
+template <int W, bool JOIN, int DW, int MODE>
+static mb_status launch_bc(const BinSpec &S, const mb_src *src, uint64_t n, uint32_t *out,
+                           uint64_t stride, uint64_t *pop, cudaStream_t st) {
+  auto kern = bitmap_create_kernel<W, JOIN, DW, MODE>;
+  size_t smem = (size_t)BC_STAGES * BC_TILE_ROWS * W + 128 +
+                (size_t)S.nbins * BC_TILE_WORDS * 4 + (size_t)S.nbins * 8;
+  MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, BC_THREADS, smem));
+  if (occ < 1) return fail(MB_ERR_INVALID, "bitmap_create: %u bins do not fit in shared memory", S.nbins);
+  uint64_t ntiles = ceil_div(n, BC_TILE_ROWS);
+  uint64_t grid = (uint64_t)dev_info().sms * occ;
+  if (grid > ntiles) grid = ntiles;
+  uint32_t *errw = device_error_word();
+  if (!errw) return fail(MB_ERR_OOM, "bitmap_create: device error word");
+  const void *colp = JOIN ? (const void *)src->fk : src->col;
+  const void *dimp = JOIN ? src->col : nullptr;
+  kern<<<(unsigned)grid, BC_THREADS, smem, st>>>(S, colp, dimp, src->dimsz, n, out, stride,
+                                                 reinterpret_cast<unsigned long long *>(pop), errw);
+  MB_LAUNCH_CHECK("bitmap_create_kernel");
+  return MB_OK;
+}
+
+template <int W, bool JOIN, int DW>
+static mb_status dispatch_mode(int mode, const BinSpec &S, const mb_src *src, uint64_t n,
+                               uint32_t *out, uint64_t stride, uint64_t *pop, cudaStream_t st) {
+  switch (mode) {
+  case BC_EQUAL: return launch_bc<W, JOIN, DW, BC_EQUAL>(S, src, n, out, stride, pop, st);
+  case BC_SORTED: return launch_bc<W, JOIN, DW, BC_SORTED>(S, src, n, out, stride, pop, st);
+  default: return launch_bc<W, JOIN, DW, BC_BALLOT>(S, src, n, out, stride, pop, st);
+  }
+}
+
+template <bool JOIN, int DW>
+static mb_status dispatch_w(uint32_t w, int mode, const BinSpec &S, const mb_src *src, uint64_t n,
+                            uint32_t *out, uint64_t stride, uint64_t *pop, cudaStream_t st) {
+  switch (w) {
+  case 1: return dispatch_mode<1, JOIN, DW>(mode, S, src, n, out, stride, pop, st);
+  case 2: return dispatch_mode<2, JOIN, DW>(mode, S, src, n, out, stride, pop, st);
+  case 4: return dispatch_mode<4, JOIN, DW>(mode, S, src, n, out, stride, pop, st);
+  default: return dispatch_mode<8, JOIN, DW>(mode, S, src, n, out, stride, pop, st);
+  }
+}
+
+static int classify_bins(const uint64_t *lo, const uint64_t *hi, uint32_t nb, uint64_t *lo0,
+                         uint64_t *width) {
+  if (nb <= 4) return BC_BALLOT;
+  bool equal = true, sorted = true;
+  uint64_t w = hi[0] - lo[0];
+  for (uint32_t j = 0; j < nb; ++j) {
+    if (hi[j] <= lo[j]) return BC_BALLOT;  // empty bins: keep the generic path
+    if (hi[j] - lo[j] != w) equal = false;
+    if (j + 1 < nb) {
+      if (lo[j + 1] != hi[j]) equal = false;
+      if (lo[j + 1] < hi[j]) sorted = false;
+    }
+  }
+  if (equal) {
+    *lo0 = lo[0];
+    *width = w;
+    return BC_EQUAL;
+  }
+  return sorted ? BC_SORTED : BC_BALLOT;
+}
+
+}  // namespace mb
+
+using namespace mb;
+
+extern "C" mb_status mb_bitmap_create(const mb_src *src, uint64_t nrows, const uint64_t *lo,
+                                      const uint64_t *hi, uint32_t nbins, uint32_t *out,
+                                      uint64_t stride_words, uint64_t *popcounts, void *stream) {
+  if (!src || !lo || !hi || !out) return fail(MB_ERR_INVALID, "mb_bitmap_create: NULL argument");
+  if (nbins == 0) return MB_OK;
+  uint32_t w = src->width;
+  if (w != 1 && w != 2 && w != 4 && w != 8)
+    return fail(MB_ERR_INVALID, "mb_bitmap_create: width %u not in {1,2,4,8}", w);
+  if (!src->col) return fail(MB_ERR_INVALID, "mb_bitmap_create: column is NULL");
+  if (stride_words < mb_bitmap_words(nrows) || (stride_words & 3) != 0)
+    return fail(MB_ERR_INVALID, "mb_bitmap_create: stride %llu < words or not a multiple of 4",
+                (unsigned long long)stride_words);
+  if (((uintptr_t)out & 15) != 0)
+    return fail(MB_ERR_INVALID, "mb_bitmap_create: output not 16-byte aligned");
+  const void *staged = src->fk ? (const void *)src->fk : src->col;
+  if (((uintptr_t)staged & 15) != 0)
+    return fail(MB_ERR_INVALID, "mb_bitmap_create: staged column not 16-byte aligned");
+  if (nrows == 0) return MB_OK;
+  cudaStream_t st = as_stream(stream);
+  // More bins than one shared-memory tile holds: split into passes.
+  for (uint32_t b0 = 0; b0 < nbins; b0 += BC_MAXBINS) {
+    uint32_t nb = nbins - b0 < (uint32_t)BC_MAXBINS ? nbins - b0 : (uint32_t)BC_MAXBINS;
+    BinSpec S;
+    memset(&S, 0, sizeof(S));
+    S.nbins = nb;
+    for (uint32_t j = 0; j < nb; ++j) {
+      S.lo[j] = lo[b0 + j];
+      S.hi[j] = hi[b0 + j];
+    }
+    int mode = classify_bins(S.lo, S.hi, nb, &S.lo0, &S.width);
+    uint32_t *o = out + (uint64_t)b0 * stride_words;
+    uint64_t *p = popcounts ? popcounts + b0 : nullptr;
+    mb_status r;
+    if (src->fk == nullptr) {
+      r = dispatch_w<false, 1>(w, mode, S, src, nrows, o, stride_words, p, st);
+    } else {
+      switch (w) {  // staged column is the 4-byte key; w is the dimension width
+      case 1: r = dispatch_mode<4, true, 1>(mode, S, src, nrows, o, stride_words, p, st); break;
+      case 2: r = dispatch_mode<4, true, 2>(mode, S, src, nrows, o, stride_words, p, st); break;
+      case 4: r = dispatch_mode<4, true, 4>(mode, S, src, nrows, o, stride_words, p, st); break;
+      default: r = dispatch_mode<4, true, 8>(mode, S, src, nrows, o, stride_words, p, st); break;
+      }
+    }
+    if (r != MB_OK) return r;
+  }
+  return MB_OK;
+}

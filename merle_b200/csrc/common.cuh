@@ -1,0 +1,78 @@
+// common.cuh - shared host/device helpers of the merle_b200 CUDA library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string>
+#include "merle_b200.h"
+
+namespace mb {
+
+// ---------------------------------------------------------------- errors
+// Thread-local message of the last failing call (mb_last_error()).
+void set_error(const char *fmt, ...);
+mb_status fail(mb_status st, const char *fmt, ...);
+mb_status cuda_fail(cudaError_t e, const char *what);
+
+#define MB_CUDA(call)                                                        \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess) return ::mb::cuda_fail(e_, #call);                \
+  } while (0)
+
+#define MB_CHECK(st)                                                         \
+  do {                                                                       \
+    mb_status s_ = (st);                                                     \
+    if (s_ != MB_OK) return s_;                                              \
+  } while (0)
+
+// Launch check: reports configuration errors of the last launch.
+#define MB_LAUNCH_CHECK(what)                                                \
+  do {                                                                       \
+    cudaError_t e_ = cudaGetLastError();                                     \
+    if (e_ != cudaSuccess) return ::mb::cuda_fail(e_, what);                 \
+  } while (0)
+
+// ---------------------------------------------------------------- device info
+struct DevInfo {
+  int device = -1;
+  int sms = 148;
+  int max_smem_optin = 227 * 1024;
+  int max_threads_sm = 2048;
+};
+// Properties of the current device (cached per device).
+const DevInfo &dev_info();
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+inline uint64_t round_up(uint64_t a, uint64_t b) { return ceil_div(a, b) * b; }
+
+// ---------------------------------------------------------------- device
+// Error word written by kernels whose bounded waits ran out.  Index 0 is a
+// flag, index 1 a code (which wait), index 2 the block that gave up.
+enum { MB_DEVERR_NONE = 0, MB_DEVERR_TMA_WAIT = 1 };
+uint32_t *device_error_word();   // per-device, allocated on first use
+mb_status check_device_error(cudaStream_t s);
+
+// ssbDateToYear (ssb/ssbdemo.h:28-39): day 0 = 1992-01-01.
+__host__ __device__ inline uint32_t date_to_year(uint32_t d) {
+  return d >= 2192 ? 6u : d >= 1827 ? 5u : d >= 1461 ? 4u :
+         d >= 1096 ? 3u : d >= 731 ? 2u : d >= 366 ? 1u : 0u;
+}
+
+__device__ __forceinline__ uint64_t load_width(const void *p, uint64_t i, uint32_t w) {
+  switch (w) {
+  case 1: return __ldg(reinterpret_cast<const uint8_t *>(p) + i);
+  case 2: return __ldg(reinterpret_cast<const uint16_t *>(p) + i);
+  case 4: return __ldg(reinterpret_cast<const uint32_t *>(p) + i);
+  default: return __ldg(reinterpret_cast<const unsigned long long *>(p) + i);
+  }
+}
+
+// Streaming 128-bit load of 4 bitmap words (read once: evict-first in L1).
+__device__ __forceinline__ uint4 ld_stream4(const uint32_t *p) {
+  return __ldcs(reinterpret_cast<const uint4 *>(p));
+}
+
+}  // namespace mb

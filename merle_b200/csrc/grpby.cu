@@ -1,0 +1,582 @@
+// grpby.cu - the query kernels: fused program -> compaction -> op -> group-by
+// (mb_vprg_grpby), the no-index scan (mb_join_grpby) and the three
+// materialised stages (mb_vprg_eval, mb_bitmap_to_rows, mb_rows_grpby).
+//
+// Reference kernels: vprg_grpby (primitive.cuh:340-445), grpby
+// (primitive.cuh:16-48), abla::_stg1/_stg2/_stg3 (primitive_abla.cuh:262-394).
+//
+// B200 design of the fused kernel:
+//  - Persistent grid (SMs x occupancy).  Work unit = one warp tile of 32*V
+//    bitmap words (V = 4: 4096 rows); warps of a CTA take adjacent tiles.
+//  - The program runs in registers (vbp.cuh) with 128-bit streaming loads.
+//  - Compaction is per warp: popcounts, a 5-step shuffle scan, and the set
+//    bits' row offsets (12 bits + the uncertain flag in bit 15) written to a
+//    warp-private 16-bit list in shared memory.  No block barrier sits
+//    between a warp's tiles, and every lane then takes one listed row per
+//    round, so lanes stay busy at any selectivity (the reference switches to
+//    a per-bit loop above nt*vt0 hits, primitive.cuh:373-397).
+//  - Group-by: dense shared-memory int64 table (GS_SHARED), warp-aggregated
+//    global atomics (GS_GLOBAL), a shared-memory hash table (GS_HASH), or a
+//    register accumulator when there is one group (GS_SCALAR).
+#include <string.h>
+#include "common.cuh"
+#include "opeval.cuh"
+#include "vbp.cuh"
+
+namespace mb {
+
+// ------------------------------------------------------------ validation
+mb_status flatten_prg(const mb_vprg *p, int chk, DevPrg *o, bool *vec4) {
+  if (!p) return fail(MB_ERR_INVALID, "program is NULL");
+  if (p->ncols > MB_MAXCOLS) return fail(MB_ERR_INVALID, "program: %u operands > %d", p->ncols, MB_MAXCOLS);
+  memset(o, 0, sizeof(*o));
+  o->nrows = p->factsz;
+  o->nwords = (p->factsz + 31) / 32;
+  o->chk = chk ? 1u : 0u;
+  bool v4 = true;
+  uint32_t np = 0;
+  for (uint32_t c = 0; c < p->ncols; ++c) {
+    const mb_col &col = p->cols[c];
+    if (col.nmiddle > MB_MAXBINS) return fail(MB_ERR_INVALID, "operand %u: %u bins > %d", c, col.nmiddle, MB_MAXBINS);
+    uint32_t ne = (col.leftmost ? 1 : 0) + (col.rightmost ? 1 : 0);
+    if (np + col.nmiddle + ne > MB_MAXPTRS) return fail(MB_ERR_INVALID, "program: more than %d bitmaps", MB_MAXPTRS);
+    if (col.nmiddle && !col.middle) return fail(MB_ERR_INVALID, "operand %u: middle array is NULL", c);
+    o->off[c] = (uint8_t)np;
+    o->nmid[c] = (uint8_t)col.nmiddle;
+    o->nedge[c] = (uint8_t)ne;
+    for (uint32_t k = 0; k < col.nmiddle; ++k) {
+      if (!col.middle[k]) return fail(MB_ERR_INVALID, "operand %u: middle bin %u is NULL", c, k);
+      o->ptr[np++] = col.middle[k];
+    }
+    if (col.leftmost) o->ptr[np++] = col.leftmost;
+    if (col.rightmost) o->ptr[np++] = col.rightmost;
+  }
+  for (uint32_t i = 0; i < np; ++i)
+    if (((uintptr_t)o->ptr[i] & 15) != 0) v4 = false;
+  uint32_t n = 0;
+  for (; n < MB_MAXNINSTR; ++n) {
+    const mb_instr in = p->instrs[n];
+    if (in.opcode == MB_END) break;
+    if (in.opcode > MB_ORM) return fail(MB_ERR_INVALID, "instruction %u: bad opcode %u", n, in.opcode);
+    if (in.dstreg >= MB_NREGS) return fail(MB_ERR_INVALID, "instruction %u: register %u >= %d", n, in.dstreg, MB_NREGS);
+    if (in.opcode == MB_ANDM || in.opcode == MB_ORM) {
+      if (in.src1 >= p->ncols) return fail(MB_ERR_INVALID, "instruction %u: operand %u >= ncols %u", n, in.src1, p->ncols);
+    } else if (in.src1 >= MB_NREGS) {
+      return fail(MB_ERR_INVALID, "instruction %u: register %u >= %d", n, in.src1, MB_NREGS);
+    }
+    o->ins[n] = in;
+  }
+  o->ninstr = n;
+  *vec4 = v4;
+  return MB_OK;
+}
+
+static mb_status validate_op(const mb_op *op) {
+  if (!op) return fail(MB_ERR_INVALID, "op is NULL");
+  if (op->nsrc > MB_MAXSRC) return fail(MB_ERR_INVALID, "op: %u sources > %d", op->nsrc, MB_MAXSRC);
+  for (uint32_t i = 0; i < op->nsrc; ++i) {
+    const mb_src &s = op->src[i];
+    if (!s.col) return fail(MB_ERR_INVALID, "op source %u: column is NULL", i);
+    if (s.width != 1 && s.width != 2 && s.width != 4 && s.width != 8)
+      return fail(MB_ERR_INVALID, "op source %u: width %u", i, s.width);
+  }
+  if (op->nclause > MB_MAXCLAUSE) return fail(MB_ERR_INVALID, "op: %u clauses > %d", op->nclause, MB_MAXCLAUSE);
+  uint32_t nt = 0;
+  for (uint32_t c = 0; c < op->nclause; ++c) nt += op->clause_len[c];
+  if (nt > MB_MAXTERM) return fail(MB_ERR_INVALID, "op: %u terms > %d", nt, MB_MAXTERM);
+  for (uint32_t t = 0; t < nt; ++t)
+    if (op->terms[t].src >= op->nsrc) return fail(MB_ERR_INVALID, "op term %u: source %u", t, op->terms[t].src);
+  if (op->nkey > MB_MAXKEY) return fail(MB_ERR_INVALID, "op: %u key fields > %d", op->nkey, MB_MAXKEY);
+  for (uint32_t k = 0; k < op->nkey; ++k) {
+    const mb_key &kk = op->keys[k];
+    if (kk.src >= op->nsrc) return fail(MB_ERR_INVALID, "op key %u: source %u", k, kk.src);
+    if (kk.xform > MB_X_YEAR) return fail(MB_ERR_INVALID, "op key %u: xform %u", k, kk.xform);
+    if (kk.xform == MB_X_DIV && kk.div == 0) return fail(MB_ERR_INVALID, "op key %u: div 0", k);
+  }
+  if (op->vkind > MB_V_SUB) return fail(MB_ERR_INVALID, "op: value kind %u", op->vkind);
+  if (op->vkind != MB_V_ONE && op->va >= op->nsrc) return fail(MB_ERR_INVALID, "op: value source %u", op->va);
+  if ((op->vkind == MB_V_MUL || op->vkind == MB_V_SUB) && op->vb >= op->nsrc)
+    return fail(MB_ERR_INVALID, "op: value source %u", op->vb);
+  return MB_OK;
+}
+
+// ----------------------------------------------------------- fused kernel
+template <int V>
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
+  const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= (uint32_t)d) x += y;
+  }
+  return x;
+}
+
+template <int V, bool CHK, int GS>
+__global__ void __launch_bounds__(512)
+vbp_grpby_kernel(const __grid_constant__ DevPrg P, const __grid_constant__ mb_op O, uint32_t nr_grp,
+                 uint32_t hcap, unsigned long long *__restrict__ out, unsigned long long *__restrict__ nqual) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ uint64_t red[64];
+  constexpr uint32_t WT_WORDS = 32 * V;  // words of one warp tile
+  constexpr uint32_t WT_ROWS = WT_WORDS * 32;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const size_t gbytes = (grp_smem_bytes(GS, nr_grp, hcap) + 15) & ~(size_t)15;
+  GrpCtx G = grp_init<GS>(smem, nr_grp, hcap, out);
+  uint16_t *buf = reinterpret_cast<uint16_t *>(smem + gbytes) + (size_t)warp * WT_ROWS;
+  __syncthreads();
+
+  int64_t acc = 0;
+  uint64_t cnt = 0;
+  const uint64_t ntiles = (P.nwords + WT_WORDS - 1) / WT_WORDS;
+  for (uint64_t t = (uint64_t)blockIdx.x * nw + warp; t < ntiles; t += (uint64_t)gridDim.x * nw) {
+    const uint64_t w0 = t * WT_WORDS + lane * V;
+    uint32_t p[V], u[V];
+    vbp_eval<V, CHK>(P, w0, p, u);
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < V; ++k) c += __popc(p[k]);
+    const uint32_t incl = warp_incl_scan<V>(c);
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0) continue;
+    uint32_t off = incl - c;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      uint32_t m = p[k];
+      const uint32_t base = (lane * V + k) * 32;
+      while (m) {
+        const uint32_t b = __ffs(m) - 1;
+        m &= m - 1;
+        uint32_t e = base + b;
+        if (CHK && ((u[k] >> b) & 1u)) e |= 0x8000u;
+        buf[off++] = (uint16_t)e;
+      }
+    }
+    __syncwarp();
+    const uint32_t row0 = (uint32_t)(t * WT_ROWS);
+    for (uint32_t base = 0; base < total; base += 32) {
+      const uint32_t j = base + lane;
+      bool kept = false;
+      int64_t val = 0;
+      uint32_t grp = 0;
+      if (j < total) {
+        const uint32_t e = buf[j];
+        kept = op_eval(O, row0 + (e & 0x7fffu), CHK && (e & 0x8000u), nr_grp, val, grp);
+      }
+      cnt += kept ? 1u : 0u;
+      aggregate<GS>(G, kept, grp, val, acc);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  grp_flush<GS>(G, nr_grp, acc, cnt, nqual, red);
+}
+
+// -------------------------------------------------------- no-index scan
+template <int GS>
+__global__ void __launch_bounds__(512)
+join_grpby_kernel(uint64_t nrows, const __grid_constant__ mb_op O, uint32_t nr_grp, uint32_t hcap,
+                  unsigned long long *__restrict__ out, unsigned long long *__restrict__ nqual) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ uint64_t red[64];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  GrpCtx G = grp_init<GS>(smem, nr_grp, hcap, out);
+  __syncthreads();
+  int64_t acc = 0;
+  uint64_t cnt = 0;
+  const uint64_t nchunks = (nrows + 31) / 32;
+  for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nchunks; ch += (uint64_t)gridDim.x * nw) {
+    const uint64_t row = ch * 32 + lane;
+    bool kept = false;
+    int64_t val = 0;
+    uint32_t grp = 0;
+    if (row < nrows) kept = op_eval(O, (uint32_t)row, true, nr_grp, val, grp);
+    cnt += kept ? 1u : 0u;
+    aggregate<GS>(G, kept, grp, val, acc);
+  }
+  __syncthreads();
+  grp_flush<GS>(G, nr_grp, acc, cnt, nqual, red);
+}
+
+// ------------------------------------------------ materialised stage 1
+template <int V, bool CHK>
+__global__ void __launch_bounds__(256)
+vbp_eval_kernel(const __grid_constant__ DevPrg P, uint32_t *__restrict__ poss, uint32_t *__restrict__ unc,
+                unsigned long long *__restrict__ pop) {
+  __shared__ uint64_t red[64];
+  uint64_t c = 0;
+  const uint64_t nvec = (P.nwords + V - 1) / V;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nvec; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t w0 = i * V;
+    uint32_t p[V], u[V];
+    vbp_eval<V, CHK>(P, w0, p, u);
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      if (w0 + k < P.nwords) {
+        poss[w0 + k] = p[k];
+        if (unc) unc[w0 + k] = u[k];
+        c += __popc(p[k]);
+      }
+    }
+  }
+  uint64_t z = 0;
+  block_sum2(c, z, red);
+  if (threadIdx.x == 0 && pop && c) atomicAdd(pop, (unsigned long long)c);
+}
+
+// ------------------------------------------------ materialised stage 2
+// Row list in ascending order: per-segment counts, one-CTA exclusive scan,
+// then each segment writes its rows at its offset.
+constexpr uint32_t RL_THREADS = 256;
+constexpr uint32_t RL_SEG_WORDS = RL_THREADS * 8;  // 2048 words per segment
+
+__global__ void __launch_bounds__(RL_THREADS)
+rows_count_kernel(const uint32_t *__restrict__ poss, uint64_t nrows, uint32_t *__restrict__ segcnt) {
+  __shared__ uint64_t red[64];
+  const uint64_t nwords = (nrows + 31) / 32;
+  const uint64_t w0 = (uint64_t)blockIdx.x * RL_SEG_WORDS;
+  uint64_t c = 0;
+  const uint32_t tail = (uint32_t)(nrows & 31);
+  for (uint32_t k = threadIdx.x; k < RL_SEG_WORDS; k += RL_THREADS) {
+    const uint64_t w = w0 + k;
+    if (w < nwords) {
+      uint32_t m = poss[w];
+      if (tail && w + 1 == nwords) m &= (1u << tail) - 1u;
+      c += __popc(m);
+    }
+  }
+  uint64_t z = 0;
+  block_sum2(c, z, red);
+  if (threadIdx.x == 0) segcnt[blockIdx.x] = (uint32_t)c;
+}
+
+// Exclusive scan of nseg counts in place (one CTA of 1024 threads); the total
+// goes to *count.
+__global__ void __launch_bounds__(1024)
+rows_scan_kernel(uint32_t *__restrict__ seg, uint64_t nseg, unsigned long long *__restrict__ count) {
+  __shared__ uint64_t part[1024];
+  const uint64_t per = (nseg + 1023) / 1024;
+  const uint64_t b = threadIdx.x * per, e = b + per < nseg ? b + per : nseg;
+  uint64_t s = 0;
+  for (uint64_t i = b; i < e; ++i) s += seg[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (uint32_t d = 1; d < 1024; d <<= 1) {  // Hillis-Steele inclusive scan
+    uint64_t v = threadIdx.x >= d ? part[threadIdx.x - d] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  uint64_t run = part[threadIdx.x] - s;
+  for (uint64_t i = b; i < e; ++i) {
+    const uint32_t v = seg[i];
+    seg[i] = (uint32_t)run;
+    run += v;
+  }
+  if (threadIdx.x == 1023) *count = part[1023];
+}
+
+__global__ void __launch_bounds__(RL_THREADS)
+rows_write_kernel(const uint32_t *__restrict__ poss, const uint32_t *__restrict__ unc, uint64_t nrows,
+                  const uint32_t *__restrict__ segoff, uint32_t *__restrict__ rows) {
+  __shared__ uint32_t wsum[RL_THREADS / 32];
+  const uint64_t nwords = (nrows + 31) / 32;
+  const uint32_t tail = (uint32_t)(nrows & 31);
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // thread t owns words w0 + t*8 .. +8 (contiguous, so row order is kept)
+  const uint64_t w0 = (uint64_t)blockIdx.x * RL_SEG_WORDS + threadIdx.x * 8;
+  uint32_t m[8], uu[8], c = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint64_t w = w0 + k;
+    m[k] = w < nwords ? poss[w] : 0u;
+    if (tail && w + 1 == nwords) m[k] &= (1u << tail) - 1u;
+    uu[k] = (unc && w < nwords) ? unc[w] : 0u;
+    c += __popc(m[k]);
+  }
+  uint32_t incl = c;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= (uint32_t)d) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  uint32_t before = 0;
+  for (uint32_t w = 0; w < warp; ++w) before += wsum[w];
+  uint64_t off = (uint64_t)segoff[blockIdx.x] + before + incl - c;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    uint32_t x = m[k];
+    while (x) {
+      const uint32_t b = __ffs(x) - 1;
+      x &= x - 1;
+      uint32_t r = (uint32_t)((w0 + k) * 32 + b);
+      if ((uu[k] >> b) & 1u) r |= 0x80000000u;
+      rows[off++] = r;
+    }
+  }
+}
+
+// ------------------------------------------------ materialised stage 3
+template <int GS>
+__global__ void __launch_bounds__(512)
+rows_grpby_kernel(const uint32_t *__restrict__ rows, const unsigned long long *__restrict__ count, uint64_t capacity,
+                  const __grid_constant__ mb_op O, uint32_t nr_grp, uint32_t hcap,
+                  unsigned long long *__restrict__ out, unsigned long long *__restrict__ nqual) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ uint64_t red[64];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  GrpCtx G = grp_init<GS>(smem, nr_grp, hcap, out);
+  __syncthreads();
+  uint64_t n = *count;
+  if (n > capacity) n = capacity;
+  int64_t acc = 0;
+  uint64_t cnt = 0;
+  const uint64_t nchunks = (n + 31) / 32;
+  for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nchunks; ch += (uint64_t)gridDim.x * nw) {
+    const uint64_t i = ch * 32 + lane;
+    bool kept = false;
+    int64_t val = 0;
+    uint32_t grp = 0;
+    if (i < n) {
+      const uint32_t r = __ldcs(rows + i);
+      kept = op_eval(O, r & 0x7fffffffu, (r >> 31) != 0, nr_grp, val, grp);
+    }
+    cnt += kept ? 1u : 0u;
+    aggregate<GS>(G, kept, grp, val, acc);
+  }
+  __syncthreads();
+  grp_flush<GS>(G, nr_grp, acc, cnt, nqual, red);
+}
+
+// ------------------------------------------------------------------ host
+constexpr uint32_t DEFAULT_HCAP = 4096;
+constexpr uint32_t SHARED_MAX_GROUPS = 8192;
+
+static int pick_gs(uint32_t nr_grp, uint32_t requested) {
+  if (nr_grp == 1 && requested != MB_GRP_GLOBAL && requested != MB_GRP_HASH) return GS_SCALAR;
+  switch (requested) {
+  case MB_GRP_SHARED: return GS_SHARED;
+  case MB_GRP_GLOBAL: return GS_GLOBAL;
+  case MB_GRP_HASH: return GS_HASH;
+  default: return nr_grp <= SHARED_MAX_GROUPS ? GS_SHARED : GS_GLOBAL;
+  }
+}
+
+struct LaunchShape {
+  unsigned grid, block;
+  size_t smem;
+};
+
+template <typename K>
+static mb_status shape_for(K kern, uint32_t warps, size_t smem, uint64_t units_per_warp_total, LaunchShape *ls,
+                           uint32_t ctas_per_sm) {
+  const DevInfo &di = dev_info();
+  if (smem > (size_t)di.max_smem_optin)
+    return fail(MB_ERR_INVALID, "launch needs %zu bytes of shared memory > %d", smem, di.max_smem_optin);
+  MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, (int)(warps * 32), smem));
+  if (occ < 1) return fail(MB_ERR_INVALID, "kernel does not fit on an SM (smem %zu)", smem);
+  if (ctas_per_sm && (int)ctas_per_sm < occ) occ = (int)ctas_per_sm;
+  uint64_t grid = (uint64_t)di.sms * occ;
+  const uint64_t need = (units_per_warp_total + warps - 1) / warps;
+  if (grid > need) grid = need ? need : 1;
+  ls->grid = (unsigned)grid;
+  ls->block = warps * 32;
+  ls->smem = smem;
+  return MB_OK;
+}
+
+template <int V, bool CHK, int GS>
+static mb_status launch_fused(const DevPrg &P, const mb_op &O, uint32_t nr_grp, uint32_t hcap, int64_t *out,
+                              uint64_t *nqual, uint32_t warps, uint32_t cps, cudaStream_t st) {
+  auto kern = vbp_grpby_kernel<V, CHK, GS>;
+  const size_t gbytes = (grp_smem_bytes(GS, nr_grp, hcap) + 15) & ~(size_t)15;
+  const size_t smem = gbytes + (size_t)warps * (32 * V * 32) * 2;
+  const uint64_t ntiles = (P.nwords + 32 * V - 1) / (32 * V);
+  LaunchShape ls;
+  MB_CHECK(shape_for(kern, warps, smem, ntiles, &ls, cps));
+  kern<<<ls.grid, ls.block, ls.smem, st>>>(P, O, nr_grp, hcap, reinterpret_cast<unsigned long long *>(out),
+                                           reinterpret_cast<unsigned long long *>(nqual));
+  MB_LAUNCH_CHECK("vbp_grpby_kernel");
+  return MB_OK;
+}
+
+template <int V, bool CHK>
+static mb_status fused_gs(int gs, const DevPrg &P, const mb_op &O, uint32_t nr_grp, uint32_t hcap, int64_t *out,
+                          uint64_t *nqual, uint32_t warps, uint32_t cps, cudaStream_t st) {
+  switch (gs) {
+  case GS_SCALAR: return launch_fused<V, CHK, GS_SCALAR>(P, O, nr_grp, hcap, out, nqual, warps, cps, st);
+  case GS_SHARED: return launch_fused<V, CHK, GS_SHARED>(P, O, nr_grp, hcap, out, nqual, warps, cps, st);
+  case GS_GLOBAL: return launch_fused<V, CHK, GS_GLOBAL>(P, O, nr_grp, hcap, out, nqual, warps, cps, st);
+  default: return launch_fused<V, CHK, GS_HASH>(P, O, nr_grp, hcap, out, nqual, warps, cps, st);
+  }
+}
+
+}  // namespace mb
+
+using namespace mb;
+
+extern "C" mb_status mb_vprg_grpby(const mb_vprg *p, const mb_op *op, uint32_t nr_grp, int64_t *out,
+                                   uint64_t *nqual, const mb_launch *launch, void *stream) {
+  if (!out || !nqual) return fail(MB_ERR_INVALID, "mb_vprg_grpby: NULL output");
+  if (nr_grp == 0) return fail(MB_ERR_INVALID, "mb_vprg_grpby: nr_grp == 0");
+  const int chk = !mb_vprg_is_nochk(p);
+  DevPrg P;
+  bool v4 = false;
+  MB_CHECK(flatten_prg(p, chk, &P, &v4));
+  MB_CHECK(validate_op(op));
+  if (P.nrows >= (1ull << 32)) return fail(MB_ERR_INVALID, "mb_vprg_grpby: %llu rows >= 2^32", (unsigned long long)P.nrows);
+  cudaStream_t st = as_stream(stream);
+  MB_CUDA(cudaMemsetAsync(out, 0, (size_t)nr_grp * sizeof(int64_t), st));
+  MB_CUDA(cudaMemsetAsync(nqual, 0, sizeof(uint64_t), st));
+  if (P.nrows == 0) return MB_OK;
+  mb_launch L = launch ? *launch : mb_launch{0, 0, 0, 0};
+  const int gs = pick_gs(nr_grp, L.grp_strategy);
+  const uint32_t warps = L.warps_per_cta ? L.warps_per_cta : 8;
+  if (warps > 16 || warps == 0) return fail(MB_ERR_INVALID, "mb_vprg_grpby: warps_per_cta %u", warps);
+  uint32_t V = L.words_per_lane ? L.words_per_lane : 4;
+  if (V != 1 && V != 2 && V != 4) return fail(MB_ERR_INVALID, "mb_vprg_grpby: words_per_lane %u", V);
+  if (!v4 && V == 4) V = 2;  // 8-byte aligned pairs still vectorise poorly: use scalar loads
+  if (!v4) V = 1;
+  const uint32_t hcap = DEFAULT_HCAP;
+  if (V == 4) return chk ? fused_gs<4, true>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st)
+                         : fused_gs<4, false>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st);
+  if (V == 2) return chk ? fused_gs<2, true>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st)
+                         : fused_gs<2, false>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st);
+  return chk ? fused_gs<1, true>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st)
+             : fused_gs<1, false>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st);
+}
+
+template <int GS>
+static mb_status launch_join(uint64_t n, const mb_op &O, uint32_t nr_grp, uint32_t hcap, int64_t *out,
+                             uint64_t *nqual, cudaStream_t st) {
+  auto kern = join_grpby_kernel<GS>;
+  const uint32_t warps = 8;
+  const size_t smem = (grp_smem_bytes(GS, nr_grp, hcap) + 15) & ~(size_t)15;
+  LaunchShape ls;
+  MB_CHECK(shape_for(kern, warps, smem, (n + 31) / 32, &ls, 0));
+  kern<<<ls.grid, ls.block, ls.smem, st>>>(n, O, nr_grp, hcap, reinterpret_cast<unsigned long long *>(out),
+                                           reinterpret_cast<unsigned long long *>(nqual));
+  MB_LAUNCH_CHECK("join_grpby_kernel");
+  return MB_OK;
+}
+
+extern "C" mb_status mb_join_grpby(uint64_t nrows, const mb_op *op, uint32_t nr_grp, int64_t *out,
+                                   uint64_t *nqual, void *stream) {
+  if (!out || !nqual) return fail(MB_ERR_INVALID, "mb_join_grpby: NULL output");
+  if (nr_grp == 0) return fail(MB_ERR_INVALID, "mb_join_grpby: nr_grp == 0");
+  MB_CHECK(validate_op(op));
+  if (nrows >= (1ull << 32)) return fail(MB_ERR_INVALID, "mb_join_grpby: rows >= 2^32");
+  cudaStream_t st = as_stream(stream);
+  MB_CUDA(cudaMemsetAsync(out, 0, (size_t)nr_grp * sizeof(int64_t), st));
+  MB_CUDA(cudaMemsetAsync(nqual, 0, sizeof(uint64_t), st));
+  if (nrows == 0) return MB_OK;
+  const int gs = pick_gs(nr_grp, MB_GRP_AUTO);
+  switch (gs) {
+  case GS_SCALAR: return launch_join<GS_SCALAR>(nrows, *op, nr_grp, DEFAULT_HCAP, out, nqual, st);
+  case GS_SHARED: return launch_join<GS_SHARED>(nrows, *op, nr_grp, DEFAULT_HCAP, out, nqual, st);
+  default: return launch_join<GS_GLOBAL>(nrows, *op, nr_grp, DEFAULT_HCAP, out, nqual, st);
+  }
+}
+
+extern "C" mb_status mb_vprg_eval(const mb_vprg *p, int chk, uint32_t *possible, uint32_t *uncertain,
+                                  uint64_t *popcount, void *stream) {
+  if (!possible) return fail(MB_ERR_INVALID, "mb_vprg_eval: possible is NULL");
+  DevPrg P;
+  bool v4 = false;
+  MB_CHECK(flatten_prg(p, chk, &P, &v4));
+  if (((uintptr_t)possible & 15) || ((uintptr_t)uncertain & 15)) v4 = false;
+  if (P.nrows == 0) return MB_OK;
+  cudaStream_t st = as_stream(stream);
+  const uint64_t nvec = v4 ? (P.nwords + 3) / 4 : P.nwords;
+  uint64_t grid = (nvec + 255) / 256, cap = (uint64_t)dev_info().sms * 8;
+  if (grid > cap) grid = cap;
+  unsigned long long *pc = reinterpret_cast<unsigned long long *>(popcount);
+  if (v4) {
+    if (chk) vbp_eval_kernel<4, true><<<(unsigned)grid, 256, 0, st>>>(P, possible, uncertain, pc);
+    else vbp_eval_kernel<4, false><<<(unsigned)grid, 256, 0, st>>>(P, possible, uncertain, pc);
+  } else {
+    if (chk) vbp_eval_kernel<1, true><<<(unsigned)grid, 256, 0, st>>>(P, possible, uncertain, pc);
+    else vbp_eval_kernel<1, false><<<(unsigned)grid, 256, 0, st>>>(P, possible, uncertain, pc);
+  }
+  MB_LAUNCH_CHECK("vbp_eval_kernel");
+  return MB_OK;
+}
+
+namespace mb {
+// Segment-offset scratch of mb_bitmap_to_rows: one grow-only buffer per device.
+static uint32_t *seg_scratch(uint64_t nseg) {
+  static uint32_t *bufs[64] = {nullptr};
+  static uint64_t caps[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return nullptr;
+  if (caps[dev] < nseg) {
+    if (bufs[dev]) cudaFree(bufs[dev]);
+    bufs[dev] = nullptr;
+    caps[dev] = 0;
+    uint64_t cap = nseg < 4096 ? 4096 : nseg;
+    if (cudaMalloc(&bufs[dev], cap * sizeof(uint32_t)) != cudaSuccess) return nullptr;
+    caps[dev] = cap;
+  }
+  return bufs[dev];
+}
+}  // namespace mb
+
+extern "C" mb_status mb_bitmap_to_rows(const uint32_t *possible, const uint32_t *uncertain, uint64_t nrows,
+                                       uint32_t *rows, uint64_t *count, void *stream) {
+  if (!possible || !rows || !count) return fail(MB_ERR_INVALID, "mb_bitmap_to_rows: NULL argument");
+  if (nrows >= (1ull << 31)) return fail(MB_ERR_INVALID, "mb_bitmap_to_rows: row ids must be < 2^31");
+  cudaStream_t st = as_stream(stream);
+  if (nrows == 0) {
+    MB_CUDA(cudaMemsetAsync(count, 0, sizeof(uint64_t), st));
+    return MB_OK;
+  }
+  const uint64_t nwords = (nrows + 31) / 32;
+  const uint64_t nseg = (nwords + RL_SEG_WORDS - 1) / RL_SEG_WORDS;
+  uint32_t *seg = seg_scratch(nseg);
+  if (!seg) return fail(MB_ERR_OOM, "mb_bitmap_to_rows: scratch allocation failed");
+  rows_count_kernel<<<(unsigned)nseg, RL_THREADS, 0, st>>>(possible, nrows, seg);
+  MB_LAUNCH_CHECK("rows_count_kernel");
+  rows_scan_kernel<<<1, 1024, 0, st>>>(seg, nseg, reinterpret_cast<unsigned long long *>(count));
+  MB_LAUNCH_CHECK("rows_scan_kernel");
+  rows_write_kernel<<<(unsigned)nseg, RL_THREADS, 0, st>>>(possible, uncertain, nrows, seg, rows);
+  MB_LAUNCH_CHECK("rows_write_kernel");
+  return MB_OK;
+}
+
+template <int GS>
+static mb_status launch_rows(const uint32_t *rows, const uint64_t *count, uint64_t cap, const mb_op &O,
+                             uint32_t nr_grp, uint32_t hcap, int64_t *out, uint64_t *nqual, cudaStream_t st) {
+  auto kern = rows_grpby_kernel<GS>;
+  const uint32_t warps = 8;
+  const size_t smem = (grp_smem_bytes(GS, nr_grp, hcap) + 15) & ~(size_t)15;
+  LaunchShape ls;
+  MB_CHECK(shape_for(kern, warps, smem, (cap + 31) / 32, &ls, 0));
+  kern<<<ls.grid, ls.block, ls.smem, st>>>(rows, reinterpret_cast<const unsigned long long *>(count), cap, O,
+                                           nr_grp, hcap, reinterpret_cast<unsigned long long *>(out),
+                                           reinterpret_cast<unsigned long long *>(nqual));
+  MB_LAUNCH_CHECK("rows_grpby_kernel");
+  return MB_OK;
+}
+
+extern "C" mb_status mb_rows_grpby(const uint32_t *rows, const uint64_t *count, uint64_t capacity,
+                                   const mb_op *op, uint32_t nr_grp, int64_t *out, uint64_t *nqual,
+                                   void *stream) {
+  if (!rows || !count || !out || !nqual) return fail(MB_ERR_INVALID, "mb_rows_grpby: NULL argument");
+  if (nr_grp == 0) return fail(MB_ERR_INVALID, "mb_rows_grpby: nr_grp == 0");
+  MB_CHECK(validate_op(op));
+  cudaStream_t st = as_stream(stream);
+  MB_CUDA(cudaMemsetAsync(out, 0, (size_t)nr_grp * sizeof(int64_t), st));
+  MB_CUDA(cudaMemsetAsync(nqual, 0, sizeof(uint64_t), st));
+  if (capacity == 0) return MB_OK;
+  const int gs = pick_gs(nr_grp, MB_GRP_AUTO);
+  switch (gs) {
+  case GS_SCALAR: return launch_rows<GS_SCALAR>(rows, count, capacity, *op, nr_grp, DEFAULT_HCAP, out, nqual, st);
+  case GS_SHARED: return launch_rows<GS_SHARED>(rows, count, capacity, *op, nr_grp, DEFAULT_HCAP, out, nqual, st);
+  default: return launch_rows<GS_GLOBAL>(rows, count, capacity, *op, nr_grp, DEFAULT_HCAP, out, nqual, st);
+  }
+}
