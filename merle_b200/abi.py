@@ -79,6 +79,22 @@ class mb_star_cols(C.Structure):
                                           "discount", "extendedprice", "revenue", "supplycost", "suppcity")]
 
 
+MB_RECIPE_COLS = 4
+RECIPE_PERFECT, RECIPE_MANY_OR, RECIPE_CANDCHK = range(3)
+
+
+class mb_recipe(C.Structure):
+    _fields_ = [("factsz", C.c_uint64), ("nbit", C.c_uint32 * MB_RECIPE_COLS),
+                ("min", C.c_uint32 * MB_RECIPE_COLS), ("max", C.c_uint32 * MB_RECIPE_COLS),
+                ("dimsz", C.c_uint32 * MB_RECIPE_COLS), ("fk", C.c_void_p * MB_RECIPE_COLS),
+                ("attr", C.c_void_p * MB_RECIPE_COLS)]
+
+
+class mb_owned_vprg(C.Structure):
+    _fields_ = [("prg", mb_vprg), ("mid", (C.c_void_p * MB_MAXBINS) * MB_MAXCOLS),
+                ("owned", C.c_void_p * MB_MAXPTRS), ("nowned", C.c_uint32)]
+
+
 VOIDP = C.c_void_p
 U32 = C.c_uint32
 U64 = C.c_uint64
@@ -99,6 +115,12 @@ SIGNATURES: dict[str, tuple] = {
     "mb_vprg_grpby": (I32, [C.POINTER(mb_vprg), C.POINTER(mb_op), U32, VOIDP, VOIDP,
                             C.POINTER(mb_launch), VOIDP]),
     "mb_join_grpby": (I32, [U64, C.POINTER(mb_op), U32, VOIDP, VOIDP, VOIDP]),
+    "mb_col_from_bin": (I32, [U32, C.POINTER(C.c_void_p), C.POINTER(U64), U64, U64, C.POINTER(mb_col),
+                               C.POINTER(C.c_void_p)]),
+    "mb_col_from_bin2": (I32, [U32, C.POINTER(C.c_void_p), C.POINTER(U64), U32, C.POINTER(C.c_void_p),
+                                C.POINTER(U64), U64, U64, C.POINTER(mb_col), C.POINTER(C.c_void_p)]),
+    "mb_recipe_build": (I32, [C.POINTER(mb_recipe), I32, C.POINTER(mb_instr), C.POINTER(mb_owned_vprg), VOIDP]),
+    "mb_owned_vprg_release": (I32, [C.POINTER(mb_owned_vprg)]),
     "mb_gen_flat": (I32, [U64, U64, U64, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP]),
     "mb_gen_star": (I32, [U64, U32, U64, U64, I32, C.POINTER(mb_star_cols), VOIDP]),
     "mb_gen_star_dims": (I32, [U64, U32, VOIDP, VOIDP, VOIDP, VOIDP]),
