@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""bench.py - fact rows/s of the fused bitmap-index query path on B200.
+
+Workload (one GPU): the synthetic star schema at k=20 (120,000,000 fact rows,
+every fact column 4 bytes), its canonical 242-bitmap index resident in HBM,
+and a seeded 64-query mix of the four templates (s1op..s4op of the
+reference).  One step runs the 64 queries; fact rows/s = rows x queries /
+device time.  With N GPUs every rank holds its own 120M-row shard of an
+N x 120M-row table (weak scaling) and each step ends with one NCCL all-reduce
+of the int64 group tables (the only exchange step of a sharded query).
+
+  value     device-resident: queries enqueued back to back, results in HBM,
+            CUDA events on the engine stream around the timed steps
+  e2e       through the public C ABI (mb_engine_query): query descriptors from
+            host memory, int64 results read back to host every query
+  roofline  the fused kernel: algorithmic bytes (canonical bitmaps + touched
+            32-byte payload sectors + dimensions + outputs, computed by the
+            oracle on a host row sample) / its event-timed duration
+  cpu_baseline  the reference's own CPU oracle (ssb/cpuref.c s1ref..s4ref,
+            built from its sources into oracle/_ref) on a 24M-row sample, one
+            query per thread over all host cores (the ssb_cpujoin shape)
+
+`--impl reference` times that reference CPU path alone (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "fact rows/s + %HBM roofline, learned+batched vs plain plan; p50/p99 latency"
+UNIT = "fact rows/s"
+SEED_DATA, SEED_QUERIES = 2, 3
+CPU_SAMPLE_ROWS = 24_000_000
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--k", type=int, default=20)
+    ap.add_argument("--rows", type=int, default=0, help="rows per GPU (default 6M x k)")
+    ap.add_argument("--queries", type=int, default=64)
+    ap.add_argument("--narrow", type=float, default=0.3)
+    ap.add_argument("--width4", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.proc, self.f = gpu, None, None
+
+    def __enter__(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for ln in Path(self.f.name).read_text().splitlines():
+                x = [v.strip() for v in ln.split(",")]
+                if len(x) >= 9 and x[0] == str(self.gpu):
+                    rows.append(x)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+# ------------------------------------------------------- reference (CPU)
+def cpu_sample(k: int, nrows: int):
+    from oracle import oracle as O
+    return O.StarHost(SEED_DATA, k, nrows)
+
+
+def run_cpuref(ref, schema, n, qs, threads) -> float:
+    """One pass of the query mix through the reference's s1ref..s4ref, one
+    query per thread (ssb_cpujoin's shape, ssb/cpuref.c:244-302).  Seconds."""
+    import merle_b200
+    from merle_b200 import workload as WL
+
+    def one(q):
+        t, p = WL.as_tuple(q)
+        ng = int(max(1, merle_b200.lib().mb_query_ngroups(C.byref(q))))
+        out = np.zeros(ng + 1, np.uint32)
+        if t == 1:
+            ref.s1ref(C.byref(schema), n, *p)
+        elif t == 2:
+            ref.s2ref(C.byref(schema), n, *p, out.ctypes.data)
+        elif t == 3:
+            ref.s3ref(C.byref(schema), n, *p, out.ctypes.data)
+        else:
+            ref.s4ref(C.byref(schema), n, *p, out.ctypes.data)
+        return out
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(one, qs))
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(args, qs, steps: int = 1) -> dict:
+    from oracle import oracle as O
+    ref = O.ref()
+    if ref is None:
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    n = min(CPU_SAMPLE_ROWS, args.rows or 6_000_000 * args.k)
+    star = cpu_sample(args.k, n)
+    schema = star.ssb_schema()
+    threads = os.cpu_count() or 1
+    run_cpuref(ref, schema, n, qs[:4], threads)  # warm the pages
+    ts = [run_cpuref(ref, schema, n, qs, threads) for _ in range(steps)]
+    sec = float(np.median(ts))
+    return {"value": n * len(qs) / sec, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"the {len(qs)}-query mix over the first {n:,} rows of the k={args.k} table in ssb_schema "
+                      f"widths, reference s1ref..s4ref, one query per thread on {threads} threads",
+            "seconds_per_pass": sec}
+
+
+def reference_arm(args):
+    from merle_b200 import workload as WL
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    qs = WL.random_mix(SEED_QUERIES, args.queries, args.narrow)
+    from oracle import oracle as O
+    ref = O.ref()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's cpuref.c built from "
+                          "its sources) is missing"}))
+        return
+    n = min(CPU_SAMPLE_ROWS, args.rows or 6_000_000 * args.k)
+    star = cpu_sample(args.k, n)
+    schema = star.ssb_schema()
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        run_cpuref(ref, schema, n, qs, threads)
+    ts = [run_cpuref(ref, schema, n, qs, threads) for _ in range(args.steps)]
+    tot = sum(ts)
+    v = n * len(qs) * args.steps / tot
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic", "config": config_of(args, n),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{len(qs)}-query mix over the first {n:,} rows (ssb_schema widths), "
+                                       f"one query per thread"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def config_of(args, nrows_per_gpu):
+    return {"workload": f"star schema k={args.k}, {nrows_per_gpu:,} fact rows per GPU "
+                        f"({'4-byte' if args.width4 else 'ssb_schema-width'} fact columns), 242-bitmap index, "
+                        f"{args.queries}-query seeded mix of 4 templates",
+            "rows_per_gpu": nrows_per_gpu, "queries_per_step": args.queries, "k": args.k,
+            "l2": "inputs larger than L2 (each step reads several GB of bitmaps and payload)",
+            "parallelism": f"row shards x{args.gpus}"}
+
+
+# ------------------------------------------------------------- ours
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import merle_b200
+    from merle_b200 import abi, check, workload as WL
+    from merle_b200.engine import Engine
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    L = merle_b200.lib()
+    n = args.rows or 6_000_000 * args.k
+    eng = Engine(local)
+    eng.gen_star(SEED_DATA, args.k, n, width4=bool(args.width4), row0=rank * n)
+    eng.build_index()
+    info = eng.info()
+    qs = WL.random_mix(SEED_QUERIES, args.queries, args.narrow)
+    Q = len(qs)
+    qarr = (abi.mb_query * Q)(*qs)
+    total_g = int(L.mb_queries_layout(qarr, Q, None))
+    out = torch.zeros(total_g, dtype=torch.int64, device="cuda")
+    nq = torch.zeros(Q, dtype=torch.int64, device="cuda")
+    ext = torch.cuda.ExternalStream(int(L.mb_engine_stream(eng.handle) or 0))
+
+    def step(record=False):
+        check(L.mb_engine_enqueue(eng.handle, qarr, Q, None, out.data_ptr(), nq.data_ptr(), 1 if record else 0))
+        if world > 1:
+            with torch.cuda.stream(ext):
+                dist.all_reduce(out)
+
+    for _ in range(args.warmup):
+        step()
+    check(L.mb_engine_sync(eng.handle, None, 0))
+    if world > 1:
+        dist.barrier()
+    # ---- timed region: K steps, per-query events on the last one
+    times = np.zeros((args.steps, Q), np.float32)
+    with Clocks(local) as clk:
+        check(L.mb_engine_mark(eng.handle, 0))
+        for s in range(args.steps):
+            step(record=(s == args.steps - 1))
+        check(L.mb_engine_mark(eng.handle, 1))
+        tbuf = (C.c_float * Q)()
+        check(L.mb_engine_sync(eng.handle, tbuf, Q))
+        ms = C.c_float(0)
+        check(L.mb_engine_marks_ms(eng.handle, 0, 1, C.byref(ms)))
+    torch.cuda.synchronize()
+    ms_total = float(ms.value)
+    if world > 1:
+        t = torch.tensor([ms_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    qtimes = np.array(tbuf[:], np.float64)
+    rows_total = n * world
+    value = rows_total * Q * args.steps / (ms_total / 1e3)
+
+    # ---- per-query latency through the public API with host buffers (e2e)
+    lat = []
+    e2e_ms = 0.0
+    h2d = C.sizeof(abi.mb_query) * Q
+    d2h = 8 * total_g + 8 * Q
+    res_host = np.zeros(max(info["nbitmaps"], 8192), np.int64)
+    nqh = C.c_uint64(0)
+    for _ in range(1):
+        for q in qs:  # warm
+            check(L.mb_engine_query(eng.handle, C.byref(q), None, res_host.ctypes.data, C.addressof(nqh), None))
+    if world > 1:
+        dist.barrier()
+    check(L.mb_engine_mark(eng.handle, 2))
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        for q in qs:
+            t1 = time.perf_counter()
+            check(L.mb_engine_query(eng.handle, C.byref(q), None, res_host.ctypes.data, C.addressof(nqh), None))
+            lat.append((time.perf_counter() - t1) * 1e3)
+    check(L.mb_engine_mark(eng.handle, 3))
+    e2e_wall = time.perf_counter() - t0
+    ems = C.c_float(0)
+    check(L.mb_engine_marks_ms(eng.handle, 2, 3, C.byref(ems)))
+    e2e_ms = float(ems.value)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": rows_total * Q * args.e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "api": "mb_engine_query per query (host query descriptor in, host int64 results out)",
+           "wall_s": e2e_wall}
+
+    line = None
+    if rank == 0:
+        # ---- roofline of the fused kernel (algorithmic bytes from the oracle)
+        from oracle import oracle as O
+        peaks = {}
+        pk = ROOT / "MEASURED_PEAKS.json"
+        if pk.exists():
+            peaks = json.loads(pk.read_text())
+        peak = float(peaks.get("hbm_gbs", 6650.0))
+        sample_n = min(CPU_SAMPLE_ROWS, n)
+        star = cpu_sample(args.k, sample_n)
+        widths = {c: (4 if args.width4 else {"orderdate": 2, "discount": 1, "quantity": 1, "suppcity": 1}.get(c, 4))
+                  for c in ["extendedprice", "discount", "partkey", "orderdate", "revenue", "custkey", "suppcity",
+                            "supplycost", "quantity"]}
+        ab = []
+        for q in qs:
+            t, p = WL.as_tuple(q)
+            ab.append(O.algo_bytes(star, n / sample_n, n, t, p, Engine.ngroups(q), widths))
+        algo_total = sum(a["total"] for a in ab)
+        kern_s = qtimes.sum() / 1e3
+        achieved = algo_total / kern_s / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6.65 TB/s",
+                "kernel": "vbp_grpby_kernel (one launch per query)",
+                "algo_bytes_per_launch": algo_total / Q, "launch_ms_avg": float(qtimes.mean()),
+                "traffic": None, "traffic_note": "per-launch DRAM bytes in profiles/ (ncu)"}
+        cpu = None if args.no_cpu or world > 1 else cpu_baseline(args, qs)
+        lat_a = np.array(lat)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+                "config": config_of(args, n), "impl": "ours", "plan": "plain (rule planner, one launch per query)",
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "latency_ms": {"p50": float(np.percentile(lat_a, 50)), "p99": float(np.percentile(lat_a, 99)),
+                               "kernel_p50": float(np.percentile(qtimes, 50)),
+                               "kernel_p99": float(np.percentile(qtimes, 99))},
+                "gpu_launches": Q * args.steps,
+                "clocks": clk.summary(),
+                "index": {"bitmaps": info["nbitmaps"], "bytes": info["index_bytes"],
+                          "build_ms": info["index_build_ms"]},
+                "selected_rows_per_step": sum(a["rows"] for a in ab)}
+        print(json.dumps(line))
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

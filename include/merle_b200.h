@@ -325,6 +325,118 @@ MB_API mb_status mb_gen_star(uint64_t seed, uint32_t k, uint64_t row0, uint64_t 
 MB_API mb_status mb_gen_star_dims(uint64_t seed, uint32_t k, uint8_t *custcity,
                            uint8_t *suppcity, uint16_t *partmfgr, void *stream);
 
+/* ------------------------------------------------------------------------- */
+/* Engine: a resident star schema, its bitmap index, planners and queries    */
+/* ------------------------------------------------------------------------- */
+/* The engine keeps the fact columns, dimension arrays and the canonical
+ * bitmap index resident in HBM of one device and runs queries of the four
+ * star-schema templates (the SSB flights of ssb/cpuref.c:141-242, the op
+ * functors s1op..s4op of ssb/lambdas.cuh:19-152).  Calls on one engine are
+ * serialised by the caller; different engines are independent. */
+typedef struct mb_engine mb_engine;
+
+MB_API mb_status mb_engine_create(int device, mb_engine **out);
+MB_API mb_status mb_engine_destroy(mb_engine *e);
+
+/* Generates rows [row0, row0 + nrows) of the star schema at scale k on the
+ * device (a row shard when several engines split one table); width4 = 1
+ * stores every fact column in 4 bytes, 0 in the reference's ssb_schema widths. */
+MB_API mb_status mb_engine_gen_star(mb_engine *e, uint64_t seed, uint32_t k, uint64_t row0,
+                                    uint64_t nrows, int width4);
+
+/* Copies a host star schema into the engine (ssb_load's host->device step,
+ * ssb/cpuref.c:73-111).  Host columns in the reference's ssb_schema widths. */
+typedef struct mb_star_host {
+  uint64_t nrows, ncust, nsupp, npart;  /* dimension sizes include the pad key 0 */
+  const uint32_t *custkey, *partkey;
+  const uint16_t *orderdate;
+  const uint32_t *extendedprice, *revenue, *supplycost;
+  const uint8_t *quantity, *discount, *suppcity;
+  const uint8_t *custcity;
+  const uint16_t *partmfgr;
+} mb_star_host;
+MB_API mb_status mb_engine_load_star(mb_engine *e, const mb_star_host *h);
+
+/* Builds the canonical index: date (7 years, 84 months), discount (11),
+ * quantity (50), customer and supplier city (5 regions, 25 nations) and part
+ * mfgr (5 mfgrs, 25 categories): 242 bitmaps, one column pass per level. */
+MB_API mb_status mb_engine_build_index(mb_engine *e);
+
+typedef struct mb_engine_info {
+  uint64_t nrows, fact_bytes, dim_bytes, index_bytes;
+  uint32_t k, width4, nbitmaps, sms;
+  float index_build_ms;
+} mb_engine_info;
+MB_API mb_status mb_engine_get_info(mb_engine *e, mb_engine_info *out);
+
+/* A query of one of the four templates; bounds are half-open [min, max).
+ *  tmpl 1 (s1op): p = {dateMin, dateMax, discMin, discMax, qtyMin, qtyMax}
+ *  tmpl 2 (s2op): p = {pMfgrMin, pMfgrMax, sCityMin, sCityMax}
+ *  tmpl 3 (s3op): p = {cCityMin, cCityMax, sCityMin, sCityMax, dateMin, dateMax}
+ *  tmpl 4 (s4op): p = {cCityMin, cCityMax, sCityMin, sCityMax, pMfgrMin,
+ *                      pMfgrMax, dateMin, dateMax} */
+typedef struct mb_query {
+  uint32_t tmpl;
+  uint32_t p[8];
+} mb_query;
+
+/* Group count of a query (the reference's NGRP_* formula, ssb/ssbdemo.h:79-87). */
+MB_API uint32_t mb_query_ngroups(const mb_query *q);
+
+typedef enum mb_plan_kind {
+  MB_PLAN_FUSED = 0,        /* virtual program + fused join-probe + group-by */
+  MB_PLAN_SCAN = 1,         /* no index: every row through the op */
+  MB_PLAN_MATERIALISED = 2  /* stage 1 -> row list -> stage 3 */
+} mb_plan_kind;
+
+/* Per-query plan knobs.  The arithmetic never depends on them. */
+typedef struct mb_plan {
+  uint32_t kind;            /* mb_plan_kind */
+  uint32_t order_mode;      /* 0: most selective predicate first; 1: template order */
+  uint32_t materialise;     /* bit i: predicate i is evaluated into a bitmap first */
+  mb_launch launch;         /* group-by strategy and tile shape */
+} mb_plan;
+
+typedef struct mb_query_stats {
+  float ms;                 /* device time of the query's kernels */
+  uint32_t nbitmaps;        /* bitmaps the program reads */
+  uint32_t chk;             /* 1 if the program needs the candidate check */
+  uint64_t algo_bytes;      /* canonical bitmap bytes + touched payload sectors */
+} mb_query_stats;
+
+/* Plans a query with the rule planner; plan may be NULL for the default. */
+MB_API mb_status mb_engine_plan_rule(mb_engine *e, const mb_query *q, mb_plan *out);
+
+/* Runs one query: results (int64[ngroups]) and the qualifying-row count
+ * are copied to HOST memory before the call returns.  plan NULL = rule plan.
+ * stats may be NULL. */
+MB_API mb_status mb_engine_query(mb_engine *e, const mb_query *q, const mb_plan *plan,
+                                 int64_t *out_host, uint64_t *nqual_host, mb_query_stats *stats);
+
+/* Result layout of n queries: offsets[i] = sum of ngroups of queries < i;
+ * returns the total group count. */
+MB_API uint64_t mb_queries_layout(const mb_query *qs, uint32_t n, uint64_t *offsets);
+
+/* Enqueues n queries on the engine stream, one launch sequence per query (the
+ * plain path), without a host synchronisation.  Results go to DEVICE memory:
+ * query i's group sums at out_dev + offsets[i] (mb_queries_layout), its row
+ * count at nqual_dev[i].  plans: NULL = rule plan for every query.  With
+ * record_times, each query's device time is kept for mb_engine_sync. */
+MB_API mb_status mb_engine_enqueue(mb_engine *e, const mb_query *qs, uint32_t n,
+                                   const mb_plan *plans, int64_t *out_dev, uint64_t *nqual_dev,
+                                   int record_times);
+/* Waits for the engine stream; times_ms (n floats of the last enqueue with
+ * record_times, may be NULL) receives each query's device time. */
+MB_API mb_status mb_engine_sync(mb_engine *e, float *times_ms, uint32_t n);
+
+/* Device-time markers on the engine stream: mark records event `idx` (0..7);
+ * marks_ms gives the device time between two recorded markers. */
+MB_API mb_status mb_engine_mark(mb_engine *e, uint32_t idx);
+MB_API mb_status mb_engine_marks_ms(mb_engine *e, uint32_t a, uint32_t b, float *ms);
+
+/* The engine's stream (a cudaStream_t) for callers that order work after it. */
+MB_API void *mb_engine_stream(mb_engine *e);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -95,6 +95,42 @@ class mb_owned_vprg(C.Structure):
                 ("owned", C.c_void_p * MB_MAXPTRS), ("nowned", C.c_uint32)]
 
 
+class mb_star_host(C.Structure):
+    _fields_ = [("nrows", C.c_uint64), ("ncust", C.c_uint64), ("nsupp", C.c_uint64), ("npart", C.c_uint64)] + \
+        [(n, C.c_void_p) for n in ("custkey", "partkey", "orderdate", "extendedprice", "revenue", "supplycost",
+                                   "quantity", "discount", "suppcity", "custcity", "partmfgr")]
+
+
+class mb_engine_info(C.Structure):
+    _fields_ = [("nrows", C.c_uint64), ("fact_bytes", C.c_uint64), ("dim_bytes", C.c_uint64),
+                ("index_bytes", C.c_uint64), ("k", C.c_uint32), ("width4", C.c_uint32),
+                ("nbitmaps", C.c_uint32), ("sms", C.c_uint32), ("index_build_ms", C.c_float)]
+
+
+class mb_query(C.Structure):
+    _fields_ = [("tmpl", C.c_uint32), ("p", C.c_uint32 * 8)]
+
+
+PLAN_FUSED, PLAN_SCAN, PLAN_MATERIALISED = range(3)
+
+
+class mb_plan(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("order_mode", C.c_uint32), ("materialise", C.c_uint32),
+                ("launch", mb_launch)]
+
+
+class mb_query_stats(C.Structure):
+    _fields_ = [("ms", C.c_float), ("nbitmaps", C.c_uint32), ("chk", C.c_uint32), ("algo_bytes", C.c_uint64)]
+
+
+def query(tmpl: int, *p: int) -> mb_query:
+    q = mb_query()
+    q.tmpl = tmpl
+    for i, v in enumerate(p):
+        q.p[i] = v
+    return q
+
+
 VOIDP = C.c_void_p
 U32 = C.c_uint32
 U64 = C.c_uint64
@@ -121,6 +157,22 @@ SIGNATURES: dict[str, tuple] = {
                                 C.POINTER(U64), U64, U64, C.POINTER(mb_col), C.POINTER(C.c_void_p)]),
     "mb_recipe_build": (I32, [C.POINTER(mb_recipe), I32, C.POINTER(mb_instr), C.POINTER(mb_owned_vprg), VOIDP]),
     "mb_owned_vprg_release": (I32, [C.POINTER(mb_owned_vprg)]),
+    "mb_engine_create": (I32, [I32, C.POINTER(VOIDP)]),
+    "mb_engine_destroy": (I32, [VOIDP]),
+    "mb_engine_gen_star": (I32, [VOIDP, U64, U32, U64, U64, I32]),
+    "mb_engine_load_star": (I32, [VOIDP, C.POINTER(mb_star_host)]),
+    "mb_engine_build_index": (I32, [VOIDP]),
+    "mb_engine_get_info": (I32, [VOIDP, C.POINTER(mb_engine_info)]),
+    "mb_query_ngroups": (U32, [C.POINTER(mb_query)]),
+    "mb_engine_plan_rule": (I32, [VOIDP, C.POINTER(mb_query), C.POINTER(mb_plan)]),
+    "mb_engine_query": (I32, [VOIDP, C.POINTER(mb_query), C.POINTER(mb_plan), VOIDP, VOIDP,
+                              C.POINTER(mb_query_stats)]),
+    "mb_queries_layout": (U64, [C.POINTER(mb_query), U32, C.POINTER(U64)]),
+    "mb_engine_enqueue": (I32, [VOIDP, C.POINTER(mb_query), U32, C.POINTER(mb_plan), VOIDP, VOIDP, I32]),
+    "mb_engine_sync": (I32, [VOIDP, C.POINTER(C.c_float), U32]),
+    "mb_engine_mark": (I32, [VOIDP, U32]),
+    "mb_engine_marks_ms": (I32, [VOIDP, U32, U32, C.POINTER(C.c_float)]),
+    "mb_engine_stream": (VOIDP, [VOIDP]),
     "mb_gen_flat": (I32, [U64, U64, U64, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP]),
     "mb_gen_star": (I32, [U64, U32, U64, U64, I32, C.POINTER(mb_star_cols), VOIDP]),
     "mb_gen_star_dims": (I32, [U64, U32, VOIDP, VOIDP, VOIDP, VOIDP]),

@@ -1,0 +1,775 @@
+// engine.cu - resident star schema, canonical bitmap index, rule planner and
+// single-query execution (mb_engine_*).
+//
+// Reference: the SSB drivers (ssb/fixedlayout.cu:34-186 building programs
+// from a fixed index with col::from_bin / from_bin2, ssb/bmpidx-create.cu
+// building that index) and the op functors s1op..s4op (ssb/lambdas.cuh:19-152).
+// The planner generalises from_bin/from_bin2 (bmpidx_create.cu:138-226):
+//  - an exact multi-level cover (coarsest bins first, e.g. years then months),
+//  - the complement of an exact cover taken with NOT when it needs fewer bins
+//    (the reference's Q3 date trick, ssb/fixedlayout.cu:93-98),
+//  - otherwise edge bins with the candidate check (leftmost / rightmost),
+// choosing by the bytes each option reads.
+#include <string.h>
+#include <algorithm>
+#include "engine.h"
+
+namespace mb {
+
+// ------------------------------------------------------------ lifetime
+Engine::~Engine() {
+  if (device >= 0) cudaSetDevice(device);
+  for (void *p : allocs) cudaFree(p);
+  allocs.clear();
+  if (h_out) cudaFreeHost(h_out);
+  if (h_nqual) cudaFreeHost(h_nqual);
+  for (cudaEvent_t ev : qev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : marks)
+    if (ev) cudaEventDestroy(ev);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+mb_status Engine::alloc(void **p, size_t bytes) {
+  MB_CUDA(cudaMalloc(p, bytes < 256 ? 256 : bytes));
+  allocs.push_back(*p);
+  return MB_OK;
+}
+
+static void free_one(std::vector<void *> &allocs, void *p) {
+  if (!p) return;
+  auto it = std::find(allocs.begin(), allocs.end(), p);
+  if (it != allocs.end()) allocs.erase(it);
+  cudaFree(p);
+}
+
+void Engine::free_star() {
+  void **cols[] = {&custkey, &partkey, &suppkey, &orderdate, &quantity, &discount, &extendedprice,
+                   &revenue, &supplycost, &suppcity};
+  for (void **c : cols) {
+    free_one(allocs, *c);
+    *c = nullptr;
+  }
+  free_one(allocs, custcity);
+  free_one(allocs, suppcity_dim);
+  free_one(allocs, partmfgr);
+  custcity = suppcity_dim = nullptr;
+  partmfgr = nullptr;
+  for (auto &c : idx)
+    for (auto &l : c.levels) free_one(allocs, l.slab);
+  for (auto &c : idx) c.levels.clear();
+  indexed = false;
+}
+
+mb_status Engine::ensure_out(uint32_t n) {
+  if (n <= out_cap) return MB_OK;
+  uint32_t cap = std::max<uint32_t>(n, 8192);
+  free_one(allocs, d_out);
+  free_one(allocs, d_nqual);
+  if (h_out) cudaFreeHost(h_out);
+  if (h_nqual) cudaFreeHost(h_nqual);
+  h_out = nullptr;
+  h_nqual = nullptr;
+  MB_CHECK(alloc((void **)&d_out, (size_t)cap * 8));
+  MB_CHECK(alloc((void **)&d_nqual, 64 * 8));
+  MB_CUDA(cudaMallocHost(&h_out, (size_t)cap * 8));
+  MB_CUDA(cudaMallocHost(&h_nqual, 64 * 8));
+  out_cap = cap;
+  return MB_OK;
+}
+
+mb_status Engine::ensure_tmp(uint64_t words) {
+  if (words <= tmp_words) return MB_OK;
+  free_one(allocs, tmp_bits);
+  tmp_bits = nullptr;
+  MB_CHECK(alloc((void **)&tmp_bits, words * 4));
+  tmp_words = words;
+  return MB_OK;
+}
+
+mb_status Engine::ensure_rows(uint64_t n) {
+  if (n <= rows_cap) return MB_OK;
+  free_one(allocs, rows);
+  rows = nullptr;
+  MB_CHECK(alloc((void **)&rows, n * 4));
+  rows_cap = n;
+  return MB_OK;
+}
+
+uint32_t Engine::fact_width(const char *col) const {
+  if (width4) return 4;
+  if (!strcmp(col, "orderdate")) return 2;
+  if (!strcmp(col, "quantity") || !strcmp(col, "discount") || !strcmp(col, "suppcity")) return 1;
+  return 4;
+}
+
+// ------------------------------------------------------------ index layout
+static std::vector<uint64_t> range_bounds(uint64_t lo, uint64_t hi, uint64_t step) {
+  std::vector<uint64_t> b;
+  for (uint64_t x = lo; x < hi; x += step) b.push_back(x);
+  b.push_back(hi);
+  return b;
+}
+
+static std::vector<uint64_t> year_bounds() { return {0, 366, 731, 1096, 1461, 1827, 2192, 2557}; }
+
+static std::vector<uint64_t> month_bounds() {
+  static const int dm[12] = {31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31};
+  std::vector<uint64_t> b;
+  uint64_t d = 0;
+  for (int y = 1992; y < 1999; ++y)
+    for (int m = 0; m < 12; ++m) {
+      b.push_back(d);
+      d += dm[m] + ((m == 1 && y % 4 == 0) ? 1 : 0);
+    }
+  b.push_back(d);  // 2557 = 1999-01-01
+  return b;
+}
+
+static mb_src fact_src(const void *col, uint32_t w) {
+  mb_src s;
+  memset(&s, 0, sizeof(s));
+  s.col = col;
+  s.width = w;
+  return s;
+}
+
+static mb_src join_src(const void *dim, const void *fk, uint64_t dimsz, uint32_t w) {
+  mb_src s;
+  memset(&s, 0, sizeof(s));
+  s.col = dim;
+  s.fk = reinterpret_cast<const uint32_t *>(fk);
+  s.dimsz = dimsz;
+  s.width = w;
+  return s;
+}
+
+mb_status Engine::setup_index_cols() {
+  auto lv = [](std::vector<uint64_t> b) {
+    Level l;
+    l.bounds = std::move(b);
+    return l;
+  };
+  IdxCol &d = idx[IC_DATE];
+  d.name = "date";
+  d.src = fact_src(orderdate, fact_width("orderdate"));
+  d.dom_lo = 0, d.dom_hi = 2557;
+  d.levels = {lv(year_bounds()), lv(month_bounds())};
+  IdxCol &di = idx[IC_DISC];
+  di.name = "discount";
+  di.src = fact_src(discount, fact_width("discount"));
+  di.dom_lo = 0, di.dom_hi = 11;
+  di.levels = {lv(range_bounds(0, 11, 1))};
+  IdxCol &q = idx[IC_QTY];
+  q.name = "quantity";
+  q.src = fact_src(quantity, fact_width("quantity"));
+  q.dom_lo = 1, q.dom_hi = 51;
+  q.levels = {lv(range_bounds(1, 51, 1))};
+  IdxCol &cc = idx[IC_CCITY];
+  cc.name = "custcity";
+  cc.src = join_src(custcity, custkey, ncust + 1, 1);
+  cc.dom_lo = 0, cc.dom_hi = 250;
+  cc.levels = {lv(range_bounds(0, 250, 50)), lv(range_bounds(0, 250, 10))};
+  IdxCol &sc = idx[IC_SCITY];
+  sc.name = "suppcity";
+  sc.src = fact_src(suppcity, fact_width("suppcity"));
+  sc.dom_lo = 0, sc.dom_hi = 250;
+  sc.levels = {lv(range_bounds(0, 250, 50)), lv(range_bounds(0, 250, 10))};
+  IdxCol &m = idx[IC_MFGR];
+  m.name = "partmfgr";
+  m.src = join_src(partmfgr, partkey, npart + 1, 2);
+  m.dom_lo = 0, m.dom_hi = 1000;
+  m.levels = {lv(range_bounds(0, 1000, 200)), lv(range_bounds(0, 1000, 40))};
+  return MB_OK;
+}
+
+// ------------------------------------------------------------ planner
+// Level l's bin j starting exactly at x, or -1.
+static int bin_at(const Level &L, uint64_t x) {
+  auto it = std::lower_bound(L.bounds.begin(), L.bounds.end() - 1, x);
+  if (it == L.bounds.end() - 1 || *it != x) return -1;
+  return (int)(it - L.bounds.begin());
+}
+
+static const uint32_t *bin_ptr(const Level &L, int j, uint64_t stride) {
+  return L.slab + (uint64_t)j * stride;
+}
+
+// Exact cover of [lo, hi) with the coarsest bins that fit (levels nest).
+static bool exact_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t stride,
+                        std::vector<const uint32_t *> &out, uint64_t &rows) {
+  uint64_t x = lo;
+  while (x < hi) {
+    bool found = false;
+    for (const Level &L : c.levels) {
+      int j = bin_at(L, x);
+      if (j >= 0 && L.bounds[j + 1] <= hi) {
+        out.push_back(bin_ptr(L, j, stride));
+        rows += L.pop.empty() ? 0 : L.pop[j];
+        x = L.bounds[j + 1];
+        found = true;
+        break;
+      }
+    }
+    if (!found) return false;
+  }
+  return true;
+}
+
+Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t stride, int nchk_sources) {
+  Cover best;
+  lo = std::max(lo, c.dom_lo);
+  hi = std::min(hi, c.dom_hi);
+  if (lo >= hi) {
+    best.empty = true;
+    return best;
+  }
+  if (lo == c.dom_lo && hi == c.dom_hi) {
+    best.full = true;
+    return best;
+  }
+  const uint64_t W = stride;  // bytes of one bitmap / 4 (padding is negligible)
+  uint64_t best_cost = UINT64_MAX;
+  // (a) exact direct cover
+  {
+    Cover cv;
+    if (exact_cover(c, lo, hi, stride, cv.mid, cv.est_rows)) {
+      uint64_t cost = (uint64_t)cv.nb() * W * 4;
+      if (cost < best_cost) best = cv, best_cost = cost;
+    }
+  }
+  // (b) complement: NOT of the exact cover of [dom_lo, lo) u [hi, dom_hi)
+  {
+    Cover cv;
+    uint64_t rows = 0;
+    bool ok = true;
+    if (c.dom_lo < lo) ok = exact_cover(c, c.dom_lo, lo, stride, cv.mid, rows);
+    if (ok && hi < c.dom_hi) ok = exact_cover(c, hi, c.dom_hi, stride, cv.mid, rows);
+    if (ok && !cv.mid.empty()) {
+      cv.complement = true;
+      uint64_t total = 0;
+      for (uint64_t p : c.levels[0].pop) total += p;
+      cv.est_rows = total > rows ? total - rows : 0;
+      uint64_t cost = (uint64_t)cv.nb() * W * 4;
+      if (cost < best_cost) best = cv, best_cost = cost;
+    }
+  }
+  // (c) edge bins on the finest level around an exact inner cover (from_bin /
+  // from_bin2 generalised); edge rows pay the candidate check
+  {
+    const Level &F = c.levels.back();
+    const uint64_t *b = F.bounds.data();
+    const int nb = (int)F.nbins();
+    int l = (int)(std::upper_bound(b, b + nb + 1, lo) - b) - 1;      // bin holding lo
+    int r = (int)(std::lower_bound(b, b + nb + 1, hi) - b) - 1;      // bin holding hi-1
+    if (l >= 0 && r < nb && l <= r) {
+      Cover cv;
+      uint64_t ilo = b[l] == lo ? lo : b[l + 1];
+      uint64_t ihi = b[r + 1] == hi ? hi : b[r];
+      bool ok = true;
+      if (l == r && (b[l] != lo || b[r + 1] != hi)) {
+        cv.left = bin_ptr(F, l, stride);
+        cv.edge_rows += F.pop.empty() ? 0 : F.pop[l];
+      } else {
+        if (b[l] != lo) {
+          cv.left = bin_ptr(F, l, stride);
+          cv.edge_rows += F.pop.empty() ? 0 : F.pop[l];
+        }
+        if (b[r + 1] != hi) {
+          cv.right = bin_ptr(F, r, stride);
+          cv.edge_rows += F.pop.empty() ? 0 : F.pop[r];
+        }
+        if (ilo < ihi) ok = exact_cover(c, ilo, ihi, stride, cv.mid, cv.est_rows);
+      }
+      if (ok && cv.nb() > 0) {
+        // the check gathers ~one 32-byte sector per filter source per edge row
+        uint64_t cost = (uint64_t)cv.nb() * W * 4 + cv.edge_rows * 32ull * (uint64_t)nchk_sources;
+        cv.est_rows += cv.edge_rows / 2;
+        if (cost < best_cost) best = cv, best_cost = cost;
+      }
+    }
+  }
+  return best;
+}
+
+uint32_t query_ngroups(const mb_query &q) {
+  const uint32_t *p = q.p;
+  auto years = [](uint32_t dmin, uint32_t dmax) -> uint32_t {
+    if (dmax <= dmin) return 1;
+    return date_to_year(dmax - 1) - date_to_year(dmin) + 1;
+  };
+  switch (q.tmpl) {
+  case 1: return 1;
+  case 2: return p[1] > p[0] ? 7 * (p[1] - p[0]) : 1;
+  case 3: {
+    uint32_t a = p[1] - p[0], b = p[3] - p[2];
+    if (p[1] - p[0] >= 50) a = p[1] / 10 - p[0] / 10, b = p[3] / 10 - p[2] / 10;
+    uint32_t g = a * b * years(p[4], p[5]);
+    return g ? g : 1;
+  }
+  case 4: {
+    uint32_t a = p[3] - p[2], b = p[5] - p[4];
+    if (p[3] - p[2] >= 50) a = p[3] / 10 - p[2] / 10;
+    if (p[5] - p[4] >= 200) b = p[5] / 40 - p[4] / 40;
+    uint32_t g = a * b * years(p[6], p[7]);
+    return g ? g : 1;
+  }
+  default: return 0;
+  }
+}
+
+// The op functors s1op..s4op (ssb/lambdas.cuh:19-152) as mb_op.
+struct OpB {
+  mb_op o;
+  uint32_t nt = 0;
+  OpB() { memset(&o, 0, sizeof(o)); }
+  uint32_t src(const mb_src &s) {
+    o.src[o.nsrc] = s;
+    return o.nsrc++;
+  }
+  void clause1(uint32_t s, uint64_t lo, uint64_t hi) {
+    o.clause_len[o.nclause++] = 1;
+    o.terms[nt].src = s, o.terms[nt].lo = lo, o.terms[nt].hi = hi;
+    ++nt;
+  }
+  void key(uint32_t s, uint32_t xf, uint32_t div, uint32_t base, uint32_t mul) {
+    mb_key &k = o.keys[o.nkey++];
+    k.src = s, k.xform = xf, k.div = div, k.base = base, k.mul = mul;
+  }
+};
+
+static void build_op(const Engine &E, const mb_query &q, mb_op &out) {
+  OpB b;
+  const uint32_t *p = q.p;
+  const mb_src date = fact_src(E.orderdate, E.fact_width("orderdate"));
+  const mb_src scity = fact_src(E.suppcity, E.fact_width("suppcity"));
+  const mb_src ccity = join_src(E.custcity, E.custkey, E.ncust + 1, 1);
+  const mb_src mfgr = join_src(E.partmfgr, E.partkey, E.npart + 1, 2);
+  const mb_src rev = fact_src(E.revenue, 4);
+  if (q.tmpl == 1) {
+    uint32_t sd = b.src(date), sdi = b.src(fact_src(E.discount, E.fact_width("discount")));
+    uint32_t sq = b.src(fact_src(E.quantity, E.fact_width("quantity")));
+    uint32_t se = b.src(fact_src(E.extendedprice, 4));
+    b.clause1(sd, p[0], p[1]), b.clause1(sdi, p[2], p[3]), b.clause1(sq, p[4], p[5]);
+    b.o.vkind = MB_V_MUL, b.o.va = se, b.o.vb = sdi;
+  } else if (q.tmpl == 2) {
+    uint32_t ss = b.src(scity), sm = b.src(mfgr), sd = b.src(date), sr = b.src(rev);
+    b.clause1(ss, p[2], p[3]), b.clause1(sm, p[0], p[1]);
+    b.key(sm, MB_X_ID, 1, p[0], 1);
+    b.key(sd, MB_X_YEAR, 1, 0, p[1] - p[0]);
+    b.o.vkind = MB_V_COL, b.o.va = sr;
+  } else if (q.tmpl == 3) {
+    uint32_t ss = b.src(scity), sd = b.src(date), sc = b.src(ccity), sr = b.src(rev);
+    b.clause1(ss, p[2], p[3]), b.clause1(sd, p[4], p[5]), b.clause1(sc, p[0], p[1]);
+    uint32_t cmn = p[0], cmx = p[1], smn = p[2], smx = p[3], xf = MB_X_ID, dv = 1;
+    if (p[1] - p[0] >= 50) cmn /= 10, cmx /= 10, smn /= 10, smx /= 10, xf = MB_X_DIV, dv = 10;
+    const uint32_t a = cmx - cmn, bb = smx - smn;
+    b.key(sd, MB_X_YEAR, 1, date_to_year(p[4]), a * bb);
+    b.key(sc, xf, dv, cmn, a);
+    b.key(ss, xf, dv, smn, 1);
+    b.o.vkind = MB_V_COL, b.o.va = sr;
+  } else {
+    uint32_t ss = b.src(scity), sd = b.src(date), sc = b.src(ccity), sm = b.src(mfgr), sr = b.src(rev);
+    uint32_t sk = b.src(fact_src(E.supplycost, 4));
+    b.clause1(ss, p[2], p[3]), b.clause1(sd, p[6], p[7]), b.clause1(sc, p[0], p[1]), b.clause1(sm, p[4], p[5]);
+    uint32_t smn = p[2], smx = p[3], sxf = MB_X_ID, sdv = 1;
+    if (p[3] - p[2] >= 50) smn /= 10, smx /= 10, sxf = MB_X_DIV, sdv = 10;
+    uint32_t pmn = p[4], pmx = p[5], pxf = MB_X_ID, pdv = 1;
+    if (p[5] - p[4] >= 200) pmn /= 40, pmx /= 40, pxf = MB_X_DIV, pdv = 40;
+    const uint32_t a = smx - smn, bb = pmx - pmn;
+    b.key(sd, MB_X_YEAR, 1, date_to_year(p[6]), a * bb);
+    b.key(ss, sxf, sdv, smn, a);
+    b.key(sm, pxf, pdv, pmn, 1);
+    b.o.vkind = MB_V_SUB, b.o.va = sr, b.o.vb = sk;
+  }
+  out = b.o;
+}
+
+static void query_preds(const mb_query &q, std::vector<Pred> &preds) {
+  const uint32_t *p = q.p;
+  switch (q.tmpl) {
+  case 1: preds = {{IC_DATE, p[0], p[1]}, {IC_DISC, p[2], p[3]}, {IC_QTY, p[4], p[5]}}; break;
+  case 2: preds = {{IC_MFGR, p[0], p[1]}, {IC_SCITY, p[2], p[3]}}; break;
+  case 3: preds = {{IC_CCITY, p[0], p[1]}, {IC_SCITY, p[2], p[3]}, {IC_DATE, p[4], p[5]}}; break;
+  default: preds = {{IC_CCITY, p[0], p[1]}, {IC_SCITY, p[2], p[3]}, {IC_MFGR, p[4], p[5]}, {IC_DATE, p[6], p[7]}};
+  }
+}
+
+mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered &L) {
+  if (q.tmpl < 1 || q.tmpl > 4) return fail(MB_ERR_INVALID, "query: template %u not in 1..4", q.tmpl);
+  if (!E.indexed) return fail(MB_ERR_INVALID, "query: the engine has no index (mb_engine_build_index)");
+  L = Lowered();
+  L.ngroups = query_ngroups(q);
+  build_op(E, q, L.op);
+  query_preds(q, L.preds);
+  const int nchk = (int)L.op.nclause;
+  L.covers.resize(L.preds.size());
+  for (size_t i = 0; i < L.preds.size(); ++i) {
+    const Pred &pr = L.preds[i];
+    L.covers[i] = plan_cover(E.idx[pr.col], pr.lo, pr.hi, E.stride, nchk);
+    if (L.covers[i].empty) L.empty = true;
+    // plan-independent canonical count: the fewer of direct and complement exact covers
+    Cover d = plan_cover(E.idx[pr.col], pr.lo, pr.hi, E.stride, 1 << 20);  // edges priced out
+    L.canonical_bitmaps += d.full || d.empty ? 0 : d.nb();
+  }
+  // predicate order: most selective first (ANDM skips loads under zero words)
+  std::vector<int> order;
+  for (size_t i = 0; i < L.preds.size(); ++i)
+    if (!L.covers[i].full) order.push_back((int)i);
+  if (plan.order_mode == 0)
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return L.covers[a].est_rows < L.covers[b].est_rows; });
+  mb_vprg &P = L.prg;
+  memset(&P, 0, sizeof(P));
+  P.factsz = E.nrows;
+  for (int c = 0; c < MB_MAXCOLS; ++c) P.cols[c].middle = L.mids[c];
+  uint32_t ni = 0, nc = 0;
+  auto ins = [&](uint8_t op, uint8_t d, uint8_t s) {
+    P.instrs[ni].opcode = op, P.instrs[ni].dstreg = d, P.instrs[ni].src1 = s, P.instrs[ni].src2 = 0;
+    ++ni;
+  };
+  if (L.empty) return MB_OK;
+  if (order.empty()) {  // every predicate is full: all rows (NOT of the zero register)
+    ins(MB_NOT, 0, 3);
+    return MB_OK;
+  }
+  bool first = true;
+  for (int i : order) {
+    const Cover &cv = L.covers[i];
+    mb_col &col = P.cols[nc];
+    if (cv.mid.size() > MB_MAXBINS) return fail(MB_ERR_INVALID, "query: predicate needs %zu bins", cv.mid.size());
+    col.nmiddle = (uint32_t)cv.mid.size();
+    for (size_t k = 0; k < cv.mid.size(); ++k) L.mids[nc][k] = cv.mid[k];
+    col.leftmost = cv.left;
+    col.rightmost = cv.right;
+    L.col_pred[nc] = i;
+    L.nbitmaps += cv.nb();
+    L.chk |= cv.chk();
+    if (!cv.complement) {
+      ins(first ? MB_ORM : MB_ANDM, 0, (uint8_t)nc);
+    } else if (first) {
+      ins(MB_ORM, 1, (uint8_t)nc);
+      ins(MB_NOT, 0, 1);
+    } else {
+      ins(MB_AND, 1, 2);  // r2 is never written: clears r1
+      ins(MB_ORM, 1, (uint8_t)nc);
+      ins(MB_NOT, 1, 1);
+      ins(MB_AND, 0, 1);
+    }
+    first = false;
+    ++nc;
+  }
+  P.ncols = nc;
+  return MB_OK;
+}
+
+}  // namespace mb
+
+using namespace mb;
+
+// ------------------------------------------------------------------ C ABI
+extern "C" mb_status mb_engine_create(int device, mb_engine **out) {
+  if (!out) return fail(MB_ERR_INVALID, "mb_engine_create: out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  MB_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(MB_ERR_INVALID, "mb_engine_create: device %d of %d", device, ndev);
+  MB_CUDA(cudaSetDevice(device));
+  mb_engine *e = new (std::nothrow) mb_engine();
+  if (!e) return fail(MB_ERR_OOM, "mb_engine_create: host allocation");
+  e->E.device = device;
+  cudaError_t r = cudaStreamCreateWithFlags(&e->E.stream, cudaStreamNonBlocking);
+  if (r == cudaSuccess) r = cudaEventCreate(&e->E.ev0);
+  if (r == cudaSuccess) r = cudaEventCreate(&e->E.ev1);
+  if (r != cudaSuccess) {
+    delete e;
+    return cuda_fail(r, "mb_engine_create");
+  }
+  *out = e;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_engine_destroy(mb_engine *e) {
+  if (e) {
+    cudaSetDevice(e->E.device);
+    cudaStreamSynchronize(e->E.stream);
+    delete e;
+  }
+  return MB_OK;
+}
+
+extern "C" mb_status mb_engine_gen_star(mb_engine *e, uint64_t seed, uint32_t k, uint64_t row0, uint64_t nrows,
+                                        int width4) {
+  if (!e || k == 0) return fail(MB_ERR_INVALID, "mb_engine_gen_star: engine NULL or k == 0");
+  if (nrows >= (1ull << 31)) return fail(MB_ERR_INVALID, "mb_engine_gen_star: rows must be < 2^31");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  E.free_star();
+  E.nrows = nrows, E.k = k, E.width4 = width4 ? 1 : 0;
+  E.stride = mb_bitmap_stride(nrows);
+  uint32_t lg = 0;
+  while ((2u << lg) <= k) ++lg;
+  E.ncust = 30000ull * k, E.nsupp = 2000ull * k, E.npart = 200000ull * (1 + lg);
+  const char *names[] = {"custkey", "partkey", "suppkey", "orderdate", "quantity", "discount",
+                         "extendedprice", "revenue", "supplycost", "suppcity"};
+  void **cols[] = {&E.custkey, &E.partkey, &E.suppkey, &E.orderdate, &E.quantity, &E.discount,
+                   &E.extendedprice, &E.revenue, &E.supplycost, &E.suppcity};
+  for (int i = 0; i < 10; ++i) MB_CHECK(E.alloc(cols[i], nrows * E.fact_width(names[i])));
+  MB_CHECK(E.alloc((void **)&E.custcity, E.ncust + 1));
+  MB_CHECK(E.alloc((void **)&E.suppcity_dim, E.nsupp + 1));
+  MB_CHECK(E.alloc((void **)&E.partmfgr, (E.npart + 1) * 2));
+  mb_star_cols sc = {E.custkey, E.partkey, E.suppkey, E.orderdate, E.quantity, E.discount,
+                     E.extendedprice, E.revenue, E.supplycost, E.suppcity};
+  MB_CHECK(mb_gen_star(seed, k, row0, nrows, E.width4, &sc, E.stream));
+  MB_CHECK(mb_gen_star_dims(seed, k, E.custcity, E.suppcity_dim, E.partmfgr, E.stream));
+  MB_CUDA(cudaStreamSynchronize(E.stream));
+  return E.setup_index_cols();
+}
+
+extern "C" mb_status mb_engine_load_star(mb_engine *e, const mb_star_host *h) {
+  if (!e || !h) return fail(MB_ERR_INVALID, "mb_engine_load_star: NULL argument");
+  if (h->nrows >= (1ull << 31)) return fail(MB_ERR_INVALID, "mb_engine_load_star: rows must be < 2^31");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  E.free_star();
+  E.nrows = h->nrows, E.k = 0, E.width4 = 0;
+  E.stride = mb_bitmap_stride(h->nrows);
+  E.ncust = h->ncust ? h->ncust - 1 : 0, E.nsupp = h->nsupp ? h->nsupp - 1 : 0, E.npart = h->npart ? h->npart - 1 : 0;
+  struct {
+    void **d;
+    const void *s;
+    size_t bytes;
+  } cp[] = {{&E.custkey, h->custkey, h->nrows * 4},          {&E.partkey, h->partkey, h->nrows * 4},
+            {&E.orderdate, h->orderdate, h->nrows * 2},      {&E.extendedprice, h->extendedprice, h->nrows * 4},
+            {&E.revenue, h->revenue, h->nrows * 4},          {&E.supplycost, h->supplycost, h->nrows * 4},
+            {&E.quantity, h->quantity, h->nrows},            {&E.discount, h->discount, h->nrows},
+            {&E.suppcity, h->suppcity, h->nrows},            {(void **)&E.custcity, h->custcity, h->ncust},
+            {(void **)&E.partmfgr, h->partmfgr, h->npart * 2}};
+  for (auto &c : cp) {
+    if (!c.s) return fail(MB_ERR_INVALID, "mb_engine_load_star: a host column is NULL");
+    MB_CHECK(E.alloc(c.d, c.bytes));
+    MB_CUDA(cudaMemcpyAsync(*c.d, c.s, c.bytes, cudaMemcpyHostToDevice, E.stream));
+  }
+  MB_CUDA(cudaStreamSynchronize(E.stream));
+  return E.setup_index_cols();
+}
+
+extern "C" mb_status mb_engine_build_index(mb_engine *e) {
+  if (!e) return fail(MB_ERR_INVALID, "mb_engine_build_index: NULL engine");
+  Engine &E = e->E;
+  if (!E.custkey) return fail(MB_ERR_INVALID, "mb_engine_build_index: no table");
+  MB_CUDA(cudaSetDevice(E.device));
+  for (auto &c : E.idx)
+    for (auto &l : c.levels) {
+      free_one(E.allocs, l.slab);
+      l.slab = nullptr;
+    }
+  uint64_t *d_pop = nullptr;
+  MB_CHECK(E.alloc((void **)&d_pop, 1024 * 8));
+  MB_CUDA(cudaEventRecord(E.ev0, E.stream));
+  for (auto &c : E.idx) {
+    for (auto &l : c.levels) {
+      const uint32_t nb = l.nbins();
+      MB_CHECK(E.alloc((void **)&l.slab, (size_t)nb * E.stride * 4));
+      MB_CUDA(cudaMemsetAsync(l.slab, 0, (size_t)nb * E.stride * 4, E.stream));
+      MB_CUDA(cudaMemsetAsync(d_pop, 0, nb * 8, E.stream));
+      std::vector<uint64_t> lo(l.bounds.begin(), l.bounds.end() - 1), hi(l.bounds.begin() + 1, l.bounds.end());
+      MB_CHECK(mb_bitmap_create(&c.src, E.nrows, lo.data(), hi.data(), nb, l.slab, E.stride, d_pop, E.stream));
+      l.pop.assign(nb, 0);
+      MB_CUDA(cudaMemcpyAsync(l.pop.data(), d_pop, nb * 8, cudaMemcpyDeviceToHost, E.stream));
+    }
+  }
+  MB_CUDA(cudaEventRecord(E.ev1, E.stream));
+  MB_CUDA(cudaStreamSynchronize(E.stream));
+  MB_CHECK(check_device_error(E.stream));
+  cudaEventElapsedTime(&E.index_build_ms, E.ev0, E.ev1);
+  free_one(E.allocs, d_pop);
+  E.indexed = true;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_engine_get_info(mb_engine *e, mb_engine_info *o) {
+  if (!e || !o) return fail(MB_ERR_INVALID, "mb_engine_get_info: NULL argument");
+  Engine &E = e->E;
+  memset(o, 0, sizeof(*o));
+  o->nrows = E.nrows, o->k = E.k, o->width4 = E.width4;
+  const char *names[] = {"custkey", "partkey", "suppkey", "orderdate", "quantity", "discount",
+                         "extendedprice", "revenue", "supplycost", "suppcity"};
+  for (const char *n : names) o->fact_bytes += E.nrows * E.fact_width(n);
+  o->dim_bytes = (E.ncust + 1) + (E.nsupp + 1) + (E.npart + 1) * 2;
+  for (auto &c : E.idx)
+    for (auto &l : c.levels) {
+      o->nbitmaps += l.nbins();
+      if (E.indexed) o->index_bytes += (uint64_t)l.nbins() * E.stride * 4;
+    }
+  o->sms = (uint32_t)dev_info().sms;
+  o->index_build_ms = E.index_build_ms;
+  return MB_OK;
+}
+
+extern "C" uint32_t mb_query_ngroups(const mb_query *q) { return q ? query_ngroups(*q) : 0; }
+
+extern "C" mb_status mb_engine_plan_rule(mb_engine *e, const mb_query *q, mb_plan *out) {
+  if (!e || !q || !out) return fail(MB_ERR_INVALID, "mb_engine_plan_rule: NULL argument");
+  memset(out, 0, sizeof(*out));
+  out->kind = MB_PLAN_FUSED;
+  out->order_mode = 0;
+  out->launch.grp_strategy = MB_GRP_AUTO;
+  return MB_OK;
+}
+
+namespace mb {
+// Runs a lowered query on the engine stream; results stay on the device.
+// Materialised predicates (plan.materialise, template order) are evaluated
+// into a (certain, uncertain) bitmap pair first and read as one operand.
+mb_status run_lowered(Engine &E, Lowered &L, const mb_plan &plan, int64_t *d_out, uint64_t *d_nq, bool zero) {
+  cudaStream_t st = E.stream;
+  if (L.empty) {
+    if (!zero) return MB_OK;
+    MB_CUDA(cudaMemsetAsync(d_out, 0, (size_t)L.ngroups * 8, st));
+    MB_CUDA(cudaMemsetAsync(d_nq, 0, 8, st));
+    return MB_OK;
+  }
+  if (plan.kind == MB_PLAN_SCAN) return mb_join_grpby(E.nrows, &L.op, L.ngroups, d_out, d_nq, st);
+  // materialise predicates whose bit is set: their operand becomes one
+  // (certain, uncertain) bitmap pair evaluated up front
+  const uint64_t W = E.stride;
+  uint32_t nmat = 0;
+  for (uint32_t c = 0; c < L.prg.ncols; ++c)
+    if (plan.materialise & (1u << L.col_pred[c])) ++nmat;
+  if (plan.kind == MB_PLAN_MATERIALISED || nmat) MB_CHECK(E.ensure_tmp(W * (2 * nmat + 2)));
+  uint32_t used = 0;
+  for (uint32_t c = 0; c < L.prg.ncols && nmat; ++c) {
+    if (!(plan.materialise & (1u << L.col_pred[c]))) continue;
+    mb_col &col = L.prg.cols[c];
+    mb_vprg one;
+    memset(&one, 0, sizeof(one));
+    one.factsz = E.nrows;
+    one.ncols = 1;
+    one.cols[0] = col;
+    one.instrs[0].opcode = MB_ORM;
+    const bool chk = col.leftmost || col.rightmost;
+    uint32_t *pc = E.tmp_bits + W * used++, *pu = chk ? E.tmp_bits + W * used++ : nullptr;
+    MB_CHECK(mb_vprg_eval(&one, chk ? 1 : 0, pc, pu, nullptr, st));
+    if (chk) MB_CHECK(certain_of(pc, pu, E.nrows, st));
+    L.mids[c][0] = pc;
+    col.nmiddle = 1;
+    col.leftmost = pu;
+    col.rightmost = nullptr;
+  }
+  if (plan.kind == MB_PLAN_MATERIALISED) {
+    uint32_t *poss = E.tmp_bits + W * used, *unc = E.tmp_bits + W * (used + 1);
+    const int chk = !mb_vprg_is_nochk(&L.prg);
+    MB_CHECK(mb_vprg_eval(&L.prg, chk, poss, chk ? unc : nullptr, nullptr, st));
+    MB_CHECK(E.ensure_rows(E.nrows + 1));
+    if (!E.d_rowcnt) MB_CHECK(E.alloc((void **)&E.d_rowcnt, 8));
+    MB_CHECK(mb_bitmap_to_rows(poss, chk ? unc : nullptr, E.nrows, E.rows, E.d_rowcnt, st));
+    return mb_rows_grpby(E.rows, E.d_rowcnt, E.rows_cap, &L.op, L.ngroups, d_out, d_nq, st);
+  }
+  return fused_grpby(&L.prg, &L.op, L.ngroups, d_out, d_nq, &plan.launch, st, zero);
+}
+}  // namespace mb
+
+extern "C" mb_status mb_engine_query(mb_engine *e, const mb_query *q, const mb_plan *plan, int64_t *out_host,
+                                     uint64_t *nqual_host, mb_query_stats *stats) {
+  if (!e || !q || !out_host) return fail(MB_ERR_INVALID, "mb_engine_query: NULL argument");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  mb_plan pl;
+  if (plan) pl = *plan;
+  else MB_CHECK(mb_engine_plan_rule(e, q, &pl));
+  Lowered L;
+  MB_CHECK(lower_query(E, *q, pl, L));
+  MB_CHECK(E.ensure_out(L.ngroups));
+  MB_CUDA(cudaEventRecord(E.ev0, E.stream));
+  MB_CHECK(run_lowered(E, L, pl, E.d_out, E.d_nqual, true));
+  MB_CUDA(cudaEventRecord(E.ev1, E.stream));
+  MB_CUDA(cudaMemcpyAsync(E.h_out, E.d_out, (size_t)L.ngroups * 8, cudaMemcpyDeviceToHost, E.stream));
+  MB_CUDA(cudaMemcpyAsync(E.h_nqual, E.d_nqual, 8, cudaMemcpyDeviceToHost, E.stream));
+  MB_CUDA(cudaStreamSynchronize(E.stream));
+  memcpy(out_host, E.h_out, (size_t)L.ngroups * 8);
+  if (nqual_host) *nqual_host = E.h_nqual[0];
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    cudaEventElapsedTime(&stats->ms, E.ev0, E.ev1);
+    stats->nbitmaps = L.nbitmaps;
+    stats->chk = L.chk ? 1 : 0;
+    stats->algo_bytes = L.canonical_bitmaps * mb_bitmap_words(E.nrows) * 4;
+  }
+  return MB_OK;
+}
+
+extern "C" uint64_t mb_queries_layout(const mb_query *qs, uint32_t n, uint64_t *offsets) {
+  uint64_t off = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (offsets) offsets[i] = off;
+    off += query_ngroups(qs[i]);
+  }
+  return off;
+}
+
+extern "C" mb_status mb_engine_enqueue(mb_engine *e, const mb_query *qs, uint32_t n, const mb_plan *plans,
+                                       int64_t *out_dev, uint64_t *nqual_dev, int record_times) {
+  if (!e || (!qs && n) || !out_dev || !nqual_dev) return fail(MB_ERR_INVALID, "mb_engine_enqueue: NULL argument");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  if (record_times) {
+    while (E.qev.size() < 2ull * n) {
+      cudaEvent_t ev;
+      MB_CUDA(cudaEventCreate(&ev));
+      E.qev.push_back(ev);
+    }
+  }
+  E.qev_used = record_times ? n : 0;
+  // one memset zeroes every query's outputs; the per-query events then
+  // bracket the query kernels only
+  const uint64_t total = mb_queries_layout(qs, n, nullptr);
+  MB_CUDA(cudaMemsetAsync(out_dev, 0, total * 8, E.stream));
+  MB_CUDA(cudaMemsetAsync(nqual_dev, 0, (size_t)n * 8, E.stream));
+  uint64_t off = 0;
+  Lowered L;
+  for (uint32_t i = 0; i < n; ++i) {
+    mb_plan pl;
+    if (plans) pl = plans[i];
+    else MB_CHECK(mb_engine_plan_rule(e, &qs[i], &pl));
+    MB_CHECK(lower_query(E, qs[i], pl, L));
+    if (record_times) MB_CUDA(cudaEventRecord(E.qev[2 * i], E.stream));
+    MB_CHECK(run_lowered(E, L, pl, out_dev + off, nqual_dev + i, false));
+    if (record_times) MB_CUDA(cudaEventRecord(E.qev[2 * i + 1], E.stream));
+    off += L.ngroups;
+  }
+  return MB_OK;
+}
+
+extern "C" mb_status mb_engine_sync(mb_engine *e, float *times_ms, uint32_t n) {
+  if (!e) return fail(MB_ERR_INVALID, "mb_engine_sync: NULL engine");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  MB_CUDA(cudaStreamSynchronize(E.stream));
+  if (times_ms) {
+    if (n > E.qev_used) return fail(MB_ERR_INVALID, "mb_engine_sync: %u times requested, %u recorded", n, E.qev_used);
+    for (uint32_t i = 0; i < n; ++i) MB_CUDA(cudaEventElapsedTime(&times_ms[i], E.qev[2 * i], E.qev[2 * i + 1]));
+  }
+  return MB_OK;
+}
+
+extern "C" mb_status mb_engine_mark(mb_engine *e, uint32_t idx) {
+  if (!e || idx >= 8) return fail(MB_ERR_INVALID, "mb_engine_mark: engine NULL or marker >= 8");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  if (!E.marks[idx]) MB_CUDA(cudaEventCreate(&E.marks[idx]));
+  MB_CUDA(cudaEventRecord(E.marks[idx], E.stream));
+  return MB_OK;
+}
+
+extern "C" mb_status mb_engine_marks_ms(mb_engine *e, uint32_t a, uint32_t b, float *ms) {
+  if (!e || a >= 8 || b >= 8 || !ms) return fail(MB_ERR_INVALID, "mb_engine_marks_ms: bad argument");
+  Engine &E = e->E;
+  if (!E.marks[a] || !E.marks[b]) return fail(MB_ERR_INVALID, "mb_engine_marks_ms: marker not recorded");
+  MB_CUDA(cudaEventSynchronize(E.marks[b]));
+  MB_CUDA(cudaEventElapsedTime(ms, E.marks[a], E.marks[b]));
+  return MB_OK;
+}
+
+extern "C" void *mb_engine_stream(mb_engine *e) { return e ? (void *)e->E.stream : nullptr; }

@@ -1,0 +1,123 @@
+// engine.h - internal C++ view of mb_engine: resident star schema, canonical
+// bitmap index, the rule planner and query execution.
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+#include "common.cuh"
+
+namespace mb {
+
+// One partition of an indexed column's value domain into bins.
+struct Level {
+  std::vector<uint64_t> bounds;  // nbins + 1 ascending boundaries
+  uint32_t *slab = nullptr;      // nbins bitmaps at `stride` words
+  std::vector<uint64_t> pop;     // rows per bin
+  uint32_t nbins() const { return (uint32_t)bounds.size() - 1; }
+};
+
+// An indexed column: its value source and levels, coarse to fine (every
+// coarse boundary is also a fine boundary).
+struct IdxCol {
+  const char *name = "";
+  mb_src src{};
+  uint64_t dom_lo = 0, dom_hi = 0;
+  std::vector<Level> levels;
+};
+
+enum { IC_DATE = 0, IC_DISC, IC_QTY, IC_CCITY, IC_SCITY, IC_MFGR, IC_N };
+
+// A predicate lo <= value < hi on an indexed column.
+struct Pred {
+  int col;
+  uint64_t lo, hi;
+};
+
+// The bitmaps that answer one predicate.
+struct Cover {
+  std::vector<const uint32_t *> mid;
+  const uint32_t *left = nullptr, *right = nullptr;
+  bool complement = false;  // the program takes NOT of the (exact) cover
+  bool empty = false;       // no row qualifies
+  bool full = false;        // every row qualifies: no operand needed
+  uint64_t est_rows = 0;    // rows the predicate selects (from bin popcounts)
+  uint64_t edge_rows = 0;   // rows in edge bins (candidate check)
+  uint32_t nb() const { return (uint32_t)mid.size() + (left ? 1 : 0) + (right ? 1 : 0); }
+  bool chk() const { return left || right; }
+};
+
+// A query lowered to the C ABI's program + op.
+struct Lowered {
+  mb_vprg prg{};
+  const uint32_t *mids[MB_MAXCOLS][MB_MAXBINS] = {};
+  mb_op op{};
+  uint32_t ngroups = 1;
+  bool empty = false;
+  uint32_t nbitmaps = 0;
+  bool chk = false;
+  std::vector<Pred> preds;
+  std::vector<Cover> covers;
+  int col_pred[MB_MAXCOLS] = {};   // predicate (template order) of each program operand
+  uint64_t canonical_bitmaps = 0;  // plan-independent: min(direct, complement) exact cover
+};
+
+struct Engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // star schema
+  uint64_t nrows = 0, stride = 0;
+  uint32_t k = 0, width4 = 0;
+  uint64_t ncust = 0, nsupp = 0, npart = 0;  // without the pad key
+  void *custkey = nullptr, *partkey = nullptr, *suppkey = nullptr, *orderdate = nullptr,
+       *quantity = nullptr, *discount = nullptr, *extendedprice = nullptr, *revenue = nullptr,
+       *supplycost = nullptr, *suppcity = nullptr;
+  uint8_t *custcity = nullptr, *suppcity_dim = nullptr;
+  uint16_t *partmfgr = nullptr;
+  IdxCol idx[IC_N];
+  bool indexed = false;
+  float index_build_ms = 0;
+  // query scratch
+  int64_t *d_out = nullptr;
+  uint64_t *d_nqual = nullptr;
+  int64_t *h_out = nullptr;  // pinned
+  uint64_t *h_nqual = nullptr;
+  uint32_t out_cap = 0;
+  uint32_t *tmp_bits = nullptr;  // materialisation / row-list scratch
+  uint64_t tmp_words = 0;
+  uint32_t *rows = nullptr;
+  uint64_t rows_cap = 0;
+  uint64_t *d_rowcnt = nullptr;  // row count of the materialised plan
+  std::vector<void *> allocs;
+  // timing: per-query event pairs of the last enqueue, and markers
+  std::vector<cudaEvent_t> qev;
+  uint32_t qev_used = 0;
+  cudaEvent_t marks[8] = {};
+
+  ~Engine();
+  uint32_t fact_width(const char *col) const;
+  mb_status ensure_out(uint32_t ngroups);
+  mb_status ensure_tmp(uint64_t words);
+  mb_status ensure_rows(uint64_t n);
+  mb_status alloc(void **p, size_t bytes);
+  void free_star();
+  mb_status setup_index_cols();
+};
+
+// Planner and lowering (engine.cu).
+Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t W, int nchk_sources);
+mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered &L);
+uint32_t query_ngroups(const mb_query &q);
+mb_status run_lowered(Engine &E, Lowered &L, const mb_plan &plan, int64_t *d_out, uint64_t *d_nq, bool zero);
+
+// p &= ~u over the words of an nrows bitmap (grpby.cu).
+mb_status certain_of(uint32_t *p, const uint32_t *u, uint64_t nrows, cudaStream_t st);
+// mb_vprg_grpby with the output zeroing optional (grpby.cu).
+mb_status fused_grpby(const mb_vprg *p, const mb_op *op, uint32_t nr_grp, int64_t *out, uint64_t *nqual,
+                      const mb_launch *launch, cudaStream_t st, bool zero);
+
+}  // namespace mb
+
+struct mb_engine {
+  mb::Engine E;
+};

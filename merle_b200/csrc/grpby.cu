@@ -350,6 +350,20 @@ rows_grpby_kernel(const uint32_t *__restrict__ rows, const unsigned long long *_
   grp_flush<GS>(G, nr_grp, acc, cnt, nqual, red);
 }
 
+__global__ void certain_kernel(uint32_t *__restrict__ p, const uint32_t *__restrict__ u, uint64_t W) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < W; i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] &= ~u[i];
+}
+
+mb_status certain_of(uint32_t *p, const uint32_t *u, uint64_t nrows, cudaStream_t st) {
+  const uint64_t W = (nrows + 31) / 32;
+  if (W == 0) return MB_OK;
+  uint64_t grid = (W + 255) / 256, cap = (uint64_t)dev_info().sms * 8;
+  certain_kernel<<<(unsigned)(grid < cap ? grid : cap), 256, 0, st>>>(p, u, W);
+  MB_LAUNCH_CHECK("certain_kernel");
+  return MB_OK;
+}
+
 // ------------------------------------------------------------------ host
 constexpr uint32_t DEFAULT_HCAP = 4096;
 constexpr uint32_t SHARED_MAX_GROUPS = 8192;
@@ -419,8 +433,9 @@ static mb_status fused_gs(int gs, const DevPrg &P, const mb_op &O, uint32_t nr_g
 
 using namespace mb;
 
-extern "C" mb_status mb_vprg_grpby(const mb_vprg *p, const mb_op *op, uint32_t nr_grp, int64_t *out,
-                                   uint64_t *nqual, const mb_launch *launch, void *stream) {
+namespace mb {
+mb_status fused_grpby(const mb_vprg *p, const mb_op *op, uint32_t nr_grp, int64_t *out, uint64_t *nqual,
+                      const mb_launch *launch, cudaStream_t st, bool zero) {
   if (!out || !nqual) return fail(MB_ERR_INVALID, "mb_vprg_grpby: NULL output");
   if (nr_grp == 0) return fail(MB_ERR_INVALID, "mb_vprg_grpby: nr_grp == 0");
   const int chk = !mb_vprg_is_nochk(p);
@@ -429,9 +444,10 @@ extern "C" mb_status mb_vprg_grpby(const mb_vprg *p, const mb_op *op, uint32_t n
   MB_CHECK(flatten_prg(p, chk, &P, &v4));
   MB_CHECK(validate_op(op));
   if (P.nrows >= (1ull << 32)) return fail(MB_ERR_INVALID, "mb_vprg_grpby: %llu rows >= 2^32", (unsigned long long)P.nrows);
-  cudaStream_t st = as_stream(stream);
-  MB_CUDA(cudaMemsetAsync(out, 0, (size_t)nr_grp * sizeof(int64_t), st));
-  MB_CUDA(cudaMemsetAsync(nqual, 0, sizeof(uint64_t), st));
+  if (zero) {
+    MB_CUDA(cudaMemsetAsync(out, 0, (size_t)nr_grp * sizeof(int64_t), st));
+    MB_CUDA(cudaMemsetAsync(nqual, 0, sizeof(uint64_t), st));
+  }
   if (P.nrows == 0) return MB_OK;
   mb_launch L = launch ? *launch : mb_launch{0, 0, 0, 0};
   const int gs = pick_gs(nr_grp, L.grp_strategy);
@@ -439,8 +455,7 @@ extern "C" mb_status mb_vprg_grpby(const mb_vprg *p, const mb_op *op, uint32_t n
   if (warps > 16 || warps == 0) return fail(MB_ERR_INVALID, "mb_vprg_grpby: warps_per_cta %u", warps);
   uint32_t V = L.words_per_lane ? L.words_per_lane : 4;
   if (V != 1 && V != 2 && V != 4) return fail(MB_ERR_INVALID, "mb_vprg_grpby: words_per_lane %u", V);
-  if (!v4 && V == 4) V = 2;  // 8-byte aligned pairs still vectorise poorly: use scalar loads
-  if (!v4) V = 1;
+  if (!v4) V = 1;  // unaligned bitmaps: scalar loads
   const uint32_t hcap = DEFAULT_HCAP;
   if (V == 4) return chk ? fused_gs<4, true>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st)
                          : fused_gs<4, false>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st);
@@ -448,6 +463,12 @@ extern "C" mb_status mb_vprg_grpby(const mb_vprg *p, const mb_op *op, uint32_t n
                          : fused_gs<2, false>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st);
   return chk ? fused_gs<1, true>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st)
              : fused_gs<1, false>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st);
+}
+}  // namespace mb
+
+extern "C" mb_status mb_vprg_grpby(const mb_vprg *p, const mb_op *op, uint32_t nr_grp, int64_t *out,
+                                   uint64_t *nqual, const mb_launch *launch, void *stream) {
+  return fused_grpby(p, op, nr_grp, out, nqual, launch, as_stream(stream), true);
 }
 
 template <int GS>

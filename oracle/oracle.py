@@ -221,3 +221,109 @@ def bitmap_to_rows(poss: np.ndarray, unc: np.ndarray | None, n: int) -> np.ndarr
 
 def sector_count(rowbits: np.ndarray, n: int, width: int) -> int:
     return int(lib().orc_sector_count(ptr(rowbits), n, width))
+
+
+# ------------------------------------------------- algorithmic bytes (roofline)
+# The canonical index of the star schema (levels coarse to fine) and, per
+# template, the columns a plan must gather for every qualifying row (the key
+# and value sources of s1op..s4op, ssb/lambdas.cuh:19-152) and the dimension
+# arrays it probes.
+_YEARS = [0, 366, 731, 1096, 1461, 1827, 2192, 2557]
+_DM = [31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31]
+_MONTHS = []
+_d = 0
+for _y in range(1992, 1999):
+    for _m in range(12):
+        _MONTHS.append(_d)
+        _d += _DM[_m] + (1 if (_m == 1 and _y % 4 == 0) else 0)
+_MONTHS.append(_d)
+INDEX_LEVELS = {
+    "date": (0, 2557, [_YEARS, _MONTHS]),
+    "discount": (0, 11, [list(range(0, 12))]),
+    "quantity": (1, 51, [list(range(1, 52))]),
+    "custcity": (0, 250, [list(range(0, 251, 50)), list(range(0, 251, 10))]),
+    "suppcity": (0, 250, [list(range(0, 251, 50)), list(range(0, 251, 10))]),
+    "partmfgr": (0, 1000, [list(range(0, 1001, 200)), list(range(0, 1001, 40))]),
+}
+PREDS = {1: [("date", 0, 1), ("discount", 2, 3), ("quantity", 4, 5)],
+         2: [("partmfgr", 0, 1), ("suppcity", 2, 3)],
+         3: [("custcity", 0, 1), ("suppcity", 2, 3), ("date", 4, 5)],
+         4: [("custcity", 0, 1), ("suppcity", 2, 3), ("partmfgr", 4, 5), ("date", 6, 7)]}
+GATHER = {1: ["extendedprice", "discount"], 2: ["partkey", "orderdate", "revenue"],
+          3: ["custkey", "suppcity", "orderdate", "revenue"],
+          4: ["suppcity", "orderdate", "partkey", "revenue", "supplycost"]}
+DIMS = {1: [], 2: ["partmfgr"], 3: ["custcity"], 4: ["partmfgr"]}
+
+
+def _exact_bins(levels, lo, hi):
+    """Bins of the coarsest-first exact cover of [lo, hi), or None."""
+    x, n = lo, 0
+    while x < hi:
+        for b in levels:
+            if x in b:
+                j = b.index(x)
+                if j + 1 < len(b) and b[j + 1] <= hi:
+                    x, n = b[j + 1], n + 1
+                    break
+        else:
+            return None
+    return n
+
+
+def canonical_bitmaps(tmpl: int, p) -> int:
+    """Per predicate the fewer of (bins covering the range) and (bins covering
+    its complement); a range no exact cover reaches counts its finest-level
+    bins, edge bins included.  Full ranges read nothing."""
+    total = 0
+    for col, a, b in PREDS[tmpl]:
+        dlo, dhi, levels = INDEX_LEVELS[col]
+        lo, hi = max(p[a], dlo), min(p[b], dhi)
+        if lo >= hi or (lo == dlo and hi == dhi):
+            continue
+        cands = []
+        d = _exact_bins(levels, lo, hi)
+        if d is not None:
+            cands.append(d)
+        c1 = _exact_bins(levels, dlo, lo) if dlo < lo else 0
+        c2 = _exact_bins(levels, hi, dhi) if hi < dhi else 0
+        if c1 is not None and c2 is not None:
+            cands.append(c1 + c2)
+        if not cands:
+            f = levels[-1]
+            cands.append(sum(1 for j in range(len(f) - 1) if f[j + 1] > lo and f[j] < hi))
+        total += min(cands)
+    return total
+
+
+def qualifying_mask(star: "StarHost", tmpl: int, p) -> np.ndarray:
+    """Rows that satisfy every predicate of the query (numpy, vectorised)."""
+    c = star.cols
+    vals = getattr(star, "_joined", None)
+    if vals is None:
+        vals = {"date": c["orderdate"], "discount": c["discount"], "quantity": c["quantity"],
+                "suppcity": c["suppcity"], "custcity": star.custcity[c["custkey"]],
+                "partmfgr": star.partmfgr[c["partkey"]]}
+        star._joined = vals
+    m = np.ones(star.n, bool)
+    for col, a, b in PREDS[tmpl]:
+        v = vals[col]
+        m &= (v >= p[a]) & (v < p[b])
+    return m
+
+
+def algo_bytes(star: "StarHost", scale: float, nrows: int, tmpl: int, p, ngroups: int, widths: dict) -> dict:
+    """Plan-independent algorithmic bytes of one query over `nrows` rows:
+    canonical bitmaps + the 32-byte sectors of every gathered column that hold
+    a qualifying row (counted exactly on the host sample `star`, scaled by
+    `scale`) + probed dimension arrays + the int64 group outputs."""
+    W = (nrows + 31) // 32
+    bm = canonical_bitmaps(tmpl, p) * W * 4
+    m = qualifying_mask(star, tmpl, p)
+    rows = np.flatnonzero(m)
+    sec = 0
+    for col in GATHER[tmpl]:
+        w = widths[col]
+        sec += len(np.unique(rows // (32 // w))) * 32
+    dims = sum(len(getattr(star, d)) * getattr(star, d).dtype.itemsize for d in DIMS[tmpl])
+    return {"bitmap": bm, "gather": int(sec * scale), "dims": dims, "out": 8 * ngroups,
+            "total": int(bm + sec * scale + dims + 8 * ngroups), "rows": int(len(rows) * scale)}
