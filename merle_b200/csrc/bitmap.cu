@@ -41,21 +41,26 @@ struct BinSpec {
   uint64_t lo[BC_MAXBINS], hi[BC_MAXBINS];
 };
 
+// Bin of v: BC_EQUAL by arithmetic, BC_SORTED by binary search over the lower
+// bounds staged in shared memory (divergent lanes read shared memory at bank
+// speed; the same search over the kernel-parameter array serialises per
+// distinct address in the constant cache).
 template <int MODE>
-__device__ __forceinline__ uint32_t find_bin(const BinSpec &S, uint64_t v) {
+__device__ __forceinline__ uint32_t find_bin(const BinSpec &S, const uint64_t *slo, const uint64_t *shi,
+                                             uint64_t v) {
   if (MODE == BC_EQUAL) {
     if (v < S.lo0) return BC_NOBIN;
     uint64_t d = v - S.lo0;
     uint64_t b = S.width == 1 ? d : d / S.width;
     return b < S.nbins ? (uint32_t)b : BC_NOBIN;
   } else {  // BC_SORTED: last bin with lo <= v, then v < hi
-    if (v < S.lo[0]) return BC_NOBIN;
+    if (v < slo[0]) return BC_NOBIN;
     uint32_t lo = 0, hi = S.nbins - 1;
     while (lo < hi) {
       uint32_t mid = (lo + hi + 1) >> 1;
-      if (S.lo[mid] <= v) lo = mid; else hi = mid - 1;
+      if (slo[mid] <= v) lo = mid; else hi = mid - 1;
     }
-    return v < S.hi[lo] ? lo : BC_NOBIN;
+    return v < shi[lo] ? lo : BC_NOBIN;
   }
 }
 
@@ -65,6 +70,13 @@ __device__ __forceinline__ uint64_t ld_smem_w(const uint8_t *p, uint32_t i) {
   if (W == 2) return reinterpret_cast<const uint16_t *>(p)[i];
   if (W == 4) return reinterpret_cast<const uint32_t *>(p)[i];
   return reinterpret_cast<const unsigned long long *>(p)[i];
+}
+
+// Word wi of bin b in the shared tile: groups of 4 words are XOR-swizzled by
+// the bin so that leaders of different bins storing the same word index hit
+// different banks, while each bin's 4-word groups stay contiguous.
+__device__ __forceinline__ uint32_t tile_word(uint32_t b, uint32_t wi) {
+  return b * BC_TILE_WORDS + ((((wi >> 2) ^ b) & 31u) << 2) + (wi & 3u);
 }
 
 // W: bytes of the staged column element (4 for join: the foreign key);
@@ -81,14 +93,19 @@ bitmap_create_kernel(const __grid_constant__ BinSpec S, const void *__restrict__
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + BC_STAGES * STAGE_BYTES);
   uint32_t *obuf = reinterpret_cast<uint32_t *>(smem + BC_STAGES * STAGE_BYTES + 128);
   unsigned long long *cnt = reinterpret_cast<unsigned long long *>(obuf + S.nbins * BC_TILE_WORDS);
+  uint64_t *slo = reinterpret_cast<uint64_t *>(cnt + S.nbins);
+  uint64_t *shi = slo + S.nbins;
 
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint64_t nwords = (n + 31) / 32;
   const uint64_t ntiles = (n + BC_TILE_ROWS - 1) / BC_TILE_ROWS;
   const uint8_t *colb = reinterpret_cast<const uint8_t *>(col);
 
-  if (pop)
-    for (uint32_t b = tid; b < S.nbins; b += BC_THREADS) cnt[b] = 0;
+  for (uint32_t b = tid; b < S.nbins; b += BC_THREADS) {
+    cnt[b] = 0;
+    slo[b] = S.lo[b];
+    shi[b] = S.hi[b];
+  }
   if (MODE != BC_BALLOT)
     for (uint32_t i = tid; i < S.nbins * BC_TILE_WORDS; i += BC_THREADS) obuf[i] = 0;
   if (tid == 0) {
@@ -146,14 +163,13 @@ bitmap_create_kernel(const __grid_constant__ BinSpec S, const void *__restrict__
       }
       if (MODE == BC_BALLOT) {
         for (uint32_t b = 0; b < S.nbins; ++b) {
-          uint32_t m = __ballot_sync(0xffffffffu, valid && v >= S.lo[b] && v < S.hi[b]);
-          if (lane == (b & 31)) obuf[b * BC_TILE_WORDS + wi] = m;
+          uint32_t m = __ballot_sync(0xffffffffu, valid && v >= slo[b] && v < shi[b]);
+          if (lane == (b & 31)) obuf[tile_word(b, wi)] = m;
         }
       } else {
-        uint32_t bin = valid ? find_bin<MODE>(S, v) : BC_NOBIN;
+        uint32_t bin = valid ? find_bin<MODE>(S, slo, shi, v) : BC_NOBIN;
         uint32_t peers = __match_any_sync(0xffffffffu, bin);
-        if (bin != BC_NOBIN && lane == (uint32_t)(__ffs(peers) - 1))
-          obuf[bin * BC_TILE_WORDS + wi] = peers;
+        if (bin != BC_NOBIN && lane == (uint32_t)(__ffs(peers) - 1)) obuf[tile_word(bin, wi)] = peers;
       }
     }
     __syncthreads();  // stage s fully read, obuf complete
@@ -161,26 +177,30 @@ bitmap_create_kernel(const __grid_constant__ BinSpec S, const void *__restrict__
     if (tid == 0 && t + (uint64_t)BC_STAGES * gridDim.x < ntiles)
       issue(t + (uint64_t)BC_STAGES * gridDim.x, s);
 
-    // Coalesced write-out: per bin 128 consecutive words = 32 x uint4.
+    // Coalesced write-out: per bin 128 consecutive words = 32 x uint4.  A
+    // warp covers exactly one bin per iteration (i / 32 is warp-uniform).
     const uint64_t w0 = t * BC_TILE_WORDS;
     for (uint32_t i = tid; i < S.nbins * (BC_TILE_WORDS / 4); i += BC_THREADS) {
       const uint32_t b = i / (BC_TILE_WORDS / 4), q = i % (BC_TILE_WORDS / 4);
       const uint64_t w = w0 + q * 4;
-      if (w >= nwords) continue;  // obuf beyond the last word is never written
-      uint4 v4 = *reinterpret_cast<const uint4 *>(&obuf[b * BC_TILE_WORDS + q * 4]);
-      if (MODE != BC_BALLOT)  // leave the tile zeroed for the next one
-        *reinterpret_cast<uint4 *>(&obuf[b * BC_TILE_WORDS + q * 4]) = make_uint4(0, 0, 0, 0);
-      uint32_t *dst = out + b * stride + w;
-      if (w + 4 <= nwords) {
-        *reinterpret_cast<uint4 *>(dst) = v4;
-      } else {
-        dst[0] = v4.x;
-        if (w + 1 < nwords) dst[1] = v4.y;
-        if (w + 2 < nwords) dst[2] = v4.z;
+      uint32_t c = 0;
+      if (w < nwords) {  // obuf beyond the last word is never written
+        uint4 *src = reinterpret_cast<uint4 *>(&obuf[tile_word(b, q * 4)]);
+        const uint4 v4 = *src;
+        if (MODE != BC_BALLOT) *src = make_uint4(0, 0, 0, 0);  // zeroed for the next tile
+        uint32_t *dst = out + b * stride + w;
+        if (w + 4 <= nwords) {
+          *reinterpret_cast<uint4 *>(dst) = v4;
+        } else {
+          dst[0] = v4.x;
+          if (w + 1 < nwords) dst[1] = v4.y;
+          if (w + 2 < nwords) dst[2] = v4.z;
+        }
+        c = __popc(v4.x) + __popc(v4.y) + __popc(v4.z) + __popc(v4.w);
       }
       if (pop) {
-        uint32_t c = __popc(v4.x) + __popc(v4.y) + __popc(v4.z) + __popc(v4.w);
-        if (c) atomicAdd(&cnt[b], (unsigned long long)c);
+        c = __reduce_add_sync(0xffffffffu, c);
+        if (lane == 0 && c) atomicAdd(&cnt[b], (unsigned long long)c);
       }
     }
     __syncthreads();  // obuf reused by the next tile
@@ -198,7 +218,7 @@ static mb_status launch_bc(const BinSpec &S, const mb_src *src, uint64_t n, uint
                            uint64_t stride, uint64_t *pop, cudaStream_t st) {
   auto kern = bitmap_create_kernel<W, JOIN, DW, MODE>;
   size_t smem = (size_t)BC_STAGES * BC_TILE_ROWS * W + 128 +
-                (size_t)S.nbins * BC_TILE_WORDS * 4 + (size_t)S.nbins * 8;
+                (size_t)S.nbins * BC_TILE_WORDS * 4 + (size_t)S.nbins * 24;
   MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
   MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, BC_THREADS, smem));
@@ -282,8 +302,10 @@ extern "C" mb_status mb_bitmap_create(const mb_src *src, uint64_t nrows, const u
   if (nrows == 0) return MB_OK;
   cudaStream_t st = as_stream(stream);
   // More bins than one shared-memory tile holds: split into passes.
-  for (uint32_t b0 = 0; b0 < nbins; b0 += BC_MAXBINS) {
-    uint32_t nb = nbins - b0 < (uint32_t)BC_MAXBINS ? nbins - b0 : (uint32_t)BC_MAXBINS;
+  // 8-byte staged columns leave room for 224 bins next to the 3 stages
+  const uint32_t maxb = (w == 8 && src->fk == nullptr) ? 224u : (uint32_t)BC_MAXBINS;
+  for (uint32_t b0 = 0; b0 < nbins; b0 += maxb) {
+    uint32_t nb = nbins - b0 < maxb ? nbins - b0 : maxb;
     BinSpec S;
     memset(&S, 0, sizeof(S));
     S.nbins = nb;
