@@ -224,6 +224,30 @@ MB_API mb_status mb_bitmap_to_rows(const uint32_t *possible, const uint32_t *unc
                             uint64_t nrows, uint32_t *rows, uint64_t *count,
                             void *stream);
 
+/* No-allocation variant of mb_bitmap_to_rows.  It has no counterpart in the
+ * reference.  Some callers cannot let a library allocate device memory during
+ * a query: hosts that hand the whole device to their own memory pool (where a
+ * cudaMalloc from a plugin fails or fragments the pool), and latency-critical
+ * callers for whom the device-wide synchronisation that cudaMalloc and
+ * cudaFree may cause is not acceptable.  This entry point calls no cudaMalloc,
+ * cudaFree or other allocating routine: its only scratch (the per-segment row
+ * offsets, one 32-bit word per 65,536 rows) is a fixed 64 KiB array compiled
+ * into the library, which every device that loads the library holds until the
+ * process exits.  The caller still provides `rows` and `count`.
+ *  - Limit: nrows <= MB_NOALLOC_MAX_ROWS (2^30); larger inputs are rejected
+ *    with MB_ERR_INVALID before any device work.
+ *  - The first call on each device looks up the array's device address with
+ *    that device current; make that first call before capturing the stream
+ *    into a CUDA graph.
+ *  - Every call on a device shares the one array.  Calls that may overlap on
+ *    the GPU (different streams, or different host threads without ordering)
+ *    race on it and corrupt each other's results; order them on one stream.
+ * Output is identical to mb_bitmap_to_rows. */
+#define MB_NOALLOC_MAX_ROWS 1073741824ull
+MB_API mb_status mb_bitmap_to_rows_noalloc(const uint32_t *possible, const uint32_t *uncertain,
+                                           uint64_t nrows, uint32_t *rows, uint64_t *count,
+                                           void *stream);
+
 /* Materialised stage 3 (abla::_stg3, primitive_abla.cuh:356-394): applies the
  * op to a row list and aggregates.  The row count is read on the device (no
  * host round trip, unlike primitive_abla.cuh:437).  out: device int64[nr_grp]

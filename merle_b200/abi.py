@@ -147,6 +147,7 @@ SIGNATURES: dict[str, tuple] = {
                                VOIDP, VOIDP]),
     "mb_vprg_eval": (I32, [C.POINTER(mb_vprg), I32, VOIDP, VOIDP, VOIDP, VOIDP]),
     "mb_bitmap_to_rows": (I32, [VOIDP, VOIDP, U64, VOIDP, VOIDP, VOIDP]),
+    "mb_bitmap_to_rows_noalloc": (I32, [VOIDP, VOIDP, U64, VOIDP, VOIDP, VOIDP]),
     "mb_rows_grpby": (I32, [VOIDP, VOIDP, U64, C.POINTER(mb_op), U32, VOIDP, VOIDP, VOIDP]),
     "mb_vprg_grpby": (I32, [C.POINTER(mb_vprg), C.POINTER(mb_op), U32, VOIDP, VOIDP,
                             C.POINTER(mb_launch), VOIDP]),

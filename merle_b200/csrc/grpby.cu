@@ -19,6 +19,7 @@
 //    global atomics (GS_GLOBAL), a shared-memory hash table (GS_HASH), or a
 //    register accumulator when there is one group (GS_SCALAR).
 #include <string.h>
+#include <mutex>
 #include "common.cuh"
 #include "opeval.cuh"
 #include "vbp.cuh"
@@ -600,4 +601,60 @@ extern "C" mb_status mb_rows_grpby(const uint32_t *rows, const uint64_t *count, 
   case GS_SHARED: return launch_rows<GS_SHARED>(rows, count, capacity, *op, nr_grp, DEFAULT_HCAP, out, nqual, st);
   default: return launch_rows<GS_GLOBAL>(rows, count, capacity, *op, nr_grp, DEFAULT_HCAP, out, nqual, st);
   }
+}
+
+// ------------------------------------------- row list without allocation
+// mb_bitmap_to_rows keeps its per-segment offsets in a library-allocated
+// buffer.  This variant keeps them in a fixed array compiled into the
+// library, for callers that must not allocate device memory.  The array is
+// shared by every call on a device and keeps whatever the previous call left
+// in it; the count kernel overwrites every entry the scan and write kernels
+// later read, so nothing has to be cleared between calls.
+namespace mb {
+constexpr uint64_t NOALLOC_MAX_SEGMENTS = MB_NOALLOC_MAX_ROWS / (RL_SEG_WORDS * 32ull);
+static __device__ __align__(256) uint32_t g_noalloc_seg[NOALLOC_MAX_SEGMENTS];
+
+// Device address of g_noalloc_seg on the current device, looked up once per
+// device.  The name g_noalloc_seg in host code is only a host-side handle,
+// never a device address, so it is never passed to a kernel directly.
+static mb_status noalloc_scratch(uint32_t **out) {
+  static std::mutex mu;
+  static uint32_t *addr[64] = {nullptr};
+  int dev = 0;
+  MB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(MB_ERR_INVALID, "mb_bitmap_to_rows_noalloc: device %d out of range", dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_seg);
+    if (e != cudaSuccess) return cuda_fail(e, "mb_bitmap_to_rows_noalloc: cudaGetSymbolAddress");
+    addr[dev] = static_cast<uint32_t *>(p);
+  }
+  *out = addr[dev];
+  return MB_OK;
+}
+}  // namespace mb
+
+extern "C" mb_status mb_bitmap_to_rows_noalloc(const uint32_t *possible, const uint32_t *uncertain,
+                                               uint64_t nrows, uint32_t *rows, uint64_t *count, void *stream) {
+  if (!possible || !rows || !count) return fail(MB_ERR_INVALID, "mb_bitmap_to_rows_noalloc: NULL argument");
+  if (nrows > MB_NOALLOC_MAX_ROWS)
+    return fail(MB_ERR_INVALID, "mb_bitmap_to_rows_noalloc: %llu rows exceed the fixed limit of %llu rows",
+                (unsigned long long)nrows, (unsigned long long)MB_NOALLOC_MAX_ROWS);
+  uint32_t *seg = nullptr;
+  MB_CHECK(noalloc_scratch(&seg));
+  cudaStream_t st = as_stream(stream);
+  if (nrows == 0) {
+    MB_CUDA(cudaMemsetAsync(count, 0, sizeof(uint64_t), st));
+    return MB_OK;
+  }
+  const uint64_t nwords = (nrows + 31) / 32;
+  const uint64_t nseg = (nwords + RL_SEG_WORDS - 1) / RL_SEG_WORDS;
+  rows_count_kernel<<<(unsigned)nseg, RL_THREADS, 0, st>>>(possible, nrows, seg);
+  MB_LAUNCH_CHECK("rows_count_kernel");
+  rows_scan_kernel<<<1, 1024, 0, st>>>(seg, nseg, reinterpret_cast<unsigned long long *>(count));
+  MB_LAUNCH_CHECK("rows_scan_kernel");
+  rows_write_kernel<<<(unsigned)nseg, RL_THREADS, 0, st>>>(possible, uncertain, nrows, seg, rows);
+  MB_LAUNCH_CHECK("rows_write_kernel");
+  return MB_OK;
 }
