@@ -193,7 +193,16 @@ typedef struct mb_launch {
   uint32_t warps_per_cta; /* 0 = auto (4 / 8 / 16) */
   uint32_t ctas_per_sm;   /* 0 = auto (occupancy) */
   uint32_t words_per_lane;/* 0 = auto; 1, 2 or 4 bitmap words per lane */
+  uint32_t staging;       /* mb_staging: how operand bitmaps reach the program */
 } mb_launch;
+
+typedef enum mb_staging {
+  MB_STAGE_AUTO = 0,    /* conjunctive programs: warp-independent tiles with all
+                           operand loads batched; others: MB_STAGE_DIRECT */
+  MB_STAGE_DIRECT = 1,  /* the instruction interpreter with per-thread loads */
+  MB_STAGE_TMA = 2      /* every operand tile staged in shared memory by TMA
+                           bulk copies, double-buffered per CTA */
+} mb_staging;
 
 /* ------------------------------------------------------------------------- */
 /* L2 kernels over raw device buffers                                        */

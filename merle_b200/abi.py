@@ -71,7 +71,7 @@ class mb_op(C.Structure):
 
 class mb_launch(C.Structure):
     _fields_ = [("grp_strategy", C.c_uint32), ("warps_per_cta", C.c_uint32),
-                ("ctas_per_sm", C.c_uint32), ("words_per_lane", C.c_uint32)]
+                ("ctas_per_sm", C.c_uint32), ("words_per_lane", C.c_uint32), ("staging", C.c_uint32)]
 
 
 class mb_star_cols(C.Structure):

@@ -69,7 +69,74 @@ mb_status flatten_prg(const mb_vprg *p, int chk, DevPrg *o, bool *vec4) {
   }
   o->ninstr = n;
   *vec4 = v4;
+  detect_cnf(o);
   return MB_OK;
+}
+
+// Recognises the conjunctive chain the planner emits (every conjunct a
+// distinct operand; r2 and r3 never written):
+//   first conjunct:  ORM r0,c            | ORM r1,c; NOT r0,r1    | NOT r0,r3 (all rows)
+//   next conjuncts:  ANDM r0,c           | AND r1,r2; ORM r1,c; NOT r1,r1; AND r0,r1
+// On every row the chain selects, its (possible, uncertain) result equals
+// p = AND_c (m_c or ~m_c), u = (OR of the positive conjuncts' edge bins) & p,
+// with m_c = middle | edge bins of operand c: a negated conjunct contributes
+// no uncertain bit (its edge bits lie outside ~m_c), and the zero-word skip of
+// ANDM only changes uncertain bits of unselected words (primitive.cuh:292).
+void detect_cnf(DevPrg *o) {
+  o->cnf = 0;
+  o->cmask = 0;
+  o->neg = 0;
+  const uint32_t n = o->ninstr;
+  auto is = [&](uint32_t i, uint8_t op, uint8_t d, int s) {
+    return i < n && o->ins[i].opcode == op && o->ins[i].dstreg == d && (s < 0 || o->ins[i].src1 == (uint8_t)s);
+  };
+  uint32_t i = 0;
+  uint8_t used = 0, neg = 0;
+  auto add = [&](uint8_t c, bool ng) -> bool {
+    if (c >= MB_MAXCOLS || (used >> c) & 1u) return false;
+    used |= (uint8_t)(1u << c);
+    if (ng) neg |= (uint8_t)(1u << c);
+    return true;
+  };
+  if (is(i, MB_ORM, 0, -1)) {
+    if (!add(o->ins[i].src1, false)) return;
+    i += 1;
+  } else if (is(i, MB_ORM, 1, -1) && is(i + 1, MB_NOT, 0, 1)) {
+    if (!add(o->ins[i].src1, true)) return;
+    i += 2;
+  } else if (is(i, MB_NOT, 0, 3)) {
+    i += 1;
+  } else {
+    return;
+  }
+  while (i < n) {
+    if (is(i, MB_ANDM, 0, -1)) {
+      if (!add(o->ins[i].src1, false)) return;
+      i += 1;
+    } else if (is(i, MB_AND, 1, 2) && is(i + 1, MB_ORM, 1, -1) && is(i + 2, MB_NOT, 1, 1) && is(i + 3, MB_AND, 0, 1)) {
+      if (!add(o->ins[i + 1].src1, true)) return;
+      i += 4;
+    } else {
+      return;
+    }
+  }
+  // flatten the chain: bins of each conjunct, the last one flagged CNF_END
+  uint32_t k = 0;
+  for (uint32_t c = 0; c < MB_MAXCOLS; ++c) {
+    if (!((used >> c) & 1u)) continue;
+    const uint32_t nb = o->nmid[c] + o->nedge[c];
+    for (uint32_t b = 0; b < nb; ++b, ++k) {
+      o->cnf_ptr[k] = o->ptr[o->off[c] + b];
+      uint8_t f = (uint8_t)((b >= o->nmid[c] ? CNF_EDGE : 0) | (b + 1 == nb ? CNF_END : 0) |
+                            (((neg >> c) & 1u) ? CNF_NEG : 0));
+      o->cnf_flag[k] = f;
+    }
+    if (nb == 0) return;  // a conjunct without bitmaps: keep the interpreter
+  }
+  o->ncnf = (uint8_t)k;
+  o->cnf = 1;
+  o->cmask = used;
+  o->neg = neg;
 }
 
 static mb_status validate_op(const mb_op *op) {
@@ -450,14 +517,21 @@ mb_status fused_grpby(const mb_vprg *p, const mb_op *op, uint32_t nr_grp, int64_
     MB_CUDA(cudaMemsetAsync(nqual, 0, sizeof(uint64_t), st));
   }
   if (P.nrows == 0) return MB_OK;
-  mb_launch L = launch ? *launch : mb_launch{0, 0, 0, 0};
+  mb_launch L = launch ? *launch : mb_launch{0, 0, 0, 0, 0};
   const int gs = pick_gs(nr_grp, L.grp_strategy);
   const uint32_t warps = L.warps_per_cta ? L.warps_per_cta : 8;
   if (warps > 16 || warps == 0) return fail(MB_ERR_INVALID, "mb_vprg_grpby: warps_per_cta %u", warps);
-  uint32_t V = L.words_per_lane ? L.words_per_lane : 4;
-  if (V != 1 && V != 2 && V != 4) return fail(MB_ERR_INVALID, "mb_vprg_grpby: words_per_lane %u", V);
-  if (!v4) V = 1;  // unaligned bitmaps: scalar loads
+  if (L.words_per_lane != 0 && L.words_per_lane != 1 && L.words_per_lane != 2 && L.words_per_lane != 4)
+    return fail(MB_ERR_INVALID, "mb_vprg_grpby: words_per_lane %u", L.words_per_lane);
   const uint32_t hcap = DEFAULT_HCAP;
+  if (L.staging == MB_STAGE_AUTO && fused_warp_applies(P, *op))
+    return fused_warp(P, *op, nr_grp, gs, hcap, L.words_per_lane, L.warps_per_cta, out, nqual, L.ctas_per_sm, st);
+  if (L.staging == MB_STAGE_TMA && fused_tma_applies(P, v4, *op)) {
+    const mb_status r = fused_tma(P, *op, nr_grp, gs, hcap, L.words_per_lane, out, nqual, L.ctas_per_sm, st);
+    if (r != MB_ERR_UNSUPPORTED) return r;  // else: too many bitmaps to stage, load directly
+  }
+  uint32_t V = L.words_per_lane ? L.words_per_lane : 4;
+  if (!v4) V = 1;  // unaligned bitmaps: scalar loads
   if (V == 4) return chk ? fused_gs<4, true>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st)
                          : fused_gs<4, false>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st);
   if (V == 2) return chk ? fused_gs<2, true>(gs, P, *op, nr_grp, hcap, out, nqual, warps, L.ctas_per_sm, st)

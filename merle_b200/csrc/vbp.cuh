@@ -21,13 +21,27 @@ struct DevPrg {
   uint8_t off[MB_MAXCOLS];    // first pointer of operand c in ptr[]
   uint8_t nmid[MB_MAXCOLS];   // middle bins of operand c
   uint8_t nedge[MB_MAXCOLS];  // edge bins of operand c (after the middles)
-  uint8_t pad_[8];
+  // Conjunctive form, when the program is a chain of conjuncts over distinct
+  // operands (see flatten_prg): p = AND over operands of m_c or ~m_c (neg bit
+  // c), u = OR of the edge bins of the positive operands, masked by p.
+  uint8_t cnf;                // 1 if the conjunctive form applies
+  uint8_t cmask;              // bit c: operand c is a conjunct
+  uint8_t neg;                // bit c: operand c enters negated
+  uint8_t ncnf;               // bitmaps in cnf_ptr
+  uint8_t pad_[4];
   const uint32_t *ptr[MB_MAXPTRS];
+  // The conjunctive chain flattened conjunct by conjunct: bitmap i of the
+  // chain is cnf_ptr[i] with flags cnf_flag[i] (CNF_EDGE, CNF_END, CNF_NEG).
+  const uint32_t *cnf_ptr[MB_MAXPTRS];
+  uint8_t cnf_flag[MB_MAXPTRS];
 };
+enum { CNF_EDGE = 1, CNF_END = 2, CNF_NEG = 4 };
 
 // Host: validates and flattens an mb_vprg.  vec4 = every bitmap pointer is
 // 16-byte aligned (128-bit loads allowed).
 mb_status flatten_prg(const mb_vprg *p, int chk, DevPrg *out, bool *vec4);
+// Host: sets cnf / cmask / neg when the program is a conjunctive chain.
+void detect_cnf(DevPrg *o);
 
 template <int V>
 __device__ __forceinline__ void vload(const uint32_t *p, uint64_t w0, uint64_t nwords, uint32_t (&o)[V]) {
@@ -189,4 +203,18 @@ __device__ __forceinline__ void vbp_eval(const DevPrg &P, uint64_t w0, uint32_t 
   }
 }
 
+}  // namespace mb
+
+namespace mb {
+// The TMA-staged fused kernel (fused.cu).
+bool fused_tma_applies(const DevPrg &P, bool vec4, const mb_op &O);
+mb_status fused_tma(const DevPrg &P, const mb_op &O, uint32_t nr_grp, int gs, uint32_t hcap, uint32_t V,
+                    int64_t *out, uint64_t *nq, uint32_t cps, cudaStream_t st);
+}  // namespace mb
+
+namespace mb {
+// The warp-independent kernel for conjunctive programs (fused.cu).
+bool fused_warp_applies(const DevPrg &P, const mb_op &O);
+mb_status fused_warp(const DevPrg &P, const mb_op &O, uint32_t nr_grp, int gs, uint32_t hcap, uint32_t V,
+                     uint32_t warps, int64_t *out, uint64_t *nq, uint32_t cps, cudaStream_t st);
 }  // namespace mb

@@ -65,8 +65,9 @@ PLANS = [
     dict(kind=abi.PLAN_MATERIALISED),
     dict(kind=abi.PLAN_FUSED, materialise=0b1011),
     dict(kind=abi.PLAN_MATERIALISED, materialise=0b0101),
-    dict(kind=abi.PLAN_FUSED, order_mode=1, launch=(abi.GRP_GLOBAL, 4, 0, 2)),
-    dict(kind=abi.PLAN_FUSED, launch=(abi.GRP_HASH, 16, 1, 1)),
+    dict(kind=abi.PLAN_FUSED, order_mode=1, launch=(abi.GRP_GLOBAL, 4, 0, 2, 1)),
+    dict(kind=abi.PLAN_FUSED, launch=(abi.GRP_HASH, 16, 1, 1, 1)),
+    dict(kind=abi.PLAN_FUSED, launch=(abi.GRP_GLOBAL, 8, 0, 1, 0)),
 ]
 
 

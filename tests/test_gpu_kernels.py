@@ -139,8 +139,11 @@ def _device_recipe(mb, dev, kind, preds, instrs, n):
     return o
 
 
-LAUNCHES = [None, (abi.GRP_SHARED, 4, 0, 4), (abi.GRP_GLOBAL, 8, 1, 2), (abi.GRP_HASH, 16, 0, 1),
-            (abi.GRP_GLOBAL, 8, 0, 4)]
+# (group strategy, warps per CTA, CTAs per SM, words per lane, staging): staging 0 runs the
+# TMA-staged kernel, 1 the direct-load kernel
+LAUNCHES = [None, (abi.GRP_SHARED, 4, 0, 4, 1), (abi.GRP_GLOBAL, 8, 1, 2, 1), (abi.GRP_HASH, 16, 0, 1, 1),
+            (abi.GRP_GLOBAL, 8, 0, 4, 0), (abi.GRP_SHARED, 8, 0, 1, 0), (abi.GRP_HASH, 8, 2, 2, 0),
+            (abi.GRP_AUTO, 8, 0, 4, 0)]
 
 
 @pytest.mark.parametrize("kind", ["perfect", "many_or", "candchk"])
