@@ -392,13 +392,22 @@ MB_API mb_status mb_engine_load_star(mb_engine *e, const mb_star_host *h);
 
 /* Builds the canonical index: date (7 years, 84 months), discount (11),
  * quantity (50), customer and supplier city (5 regions, 25 nations) and part
- * mfgr (5 mfgrs, 25 categories): 242 bitmaps, one column pass per level. */
+ * mfgr (5 mfgrs, 25 categories): 242 bitmaps, one column pass per level.
+ * It also denormalises the customer city and part mfgr into one value per
+ * fact row (custcity[custkey], partmfgr[partkey]: 3 bytes a row), which the
+ * index build and the queries then read instead of probing the dimensions
+ * through the foreign keys; a table with a foreign key outside its dimension
+ * keeps the probes.  Results are the same either way. */
 MB_API mb_status mb_engine_build_index(mb_engine *e);
+#define MB_INDEX_PROBE_DIMS 1u  /* keep probing the dimensions (no denormalised columns) */
+MB_API mb_status mb_engine_build_index_ex(mb_engine *e, uint32_t flags);
 
 typedef struct mb_engine_info {
   uint64_t nrows, fact_bytes, dim_bytes, index_bytes;
   uint32_t k, width4, nbitmaps, sms;
   float index_build_ms;
+  uint32_t denorm;          /* 1 if the denormalised dimension columns are in use */
+  uint64_t denorm_bytes;    /* their bytes */
 } mb_engine_info;
 MB_API mb_status mb_engine_get_info(mb_engine *e, mb_engine_info *out);
 
@@ -469,6 +478,43 @@ MB_API mb_status mb_engine_marks_ms(mb_engine *e, uint32_t a, uint32_t b, float 
 
 /* The engine's stream (a cudaStream_t) for callers that order work after it. */
 MB_API void *mb_engine_stream(mb_engine *e);
+
+/* Batched execution: one persistent launch walks the rows once for a whole
+ * batch of queries.  Per row tile it stages the union of the batch's bitmaps
+ * in shared memory (each word read from HBM once per batch, not once per
+ * query) and prefetches the tile's payload columns into L2; the selected rows
+ * of all the batch's queries then share one row list per tile, so the ops run
+ * on full warps and gather from the same lines.  No counterpart in the
+ * reference, which runs one query per launch (ssb/fixedlayout.cu:34-186).
+ * A launch takes up to MB_BATCH_MAX queries (and up to 256 distinct bitmaps);
+ * longer batches are split.  A query the batch kernel cannot take (an op
+ * source wider than 4 bytes, a clause of several terms) runs through the
+ * single-query path on the same stream.  Each query's results equal what it
+ * gets alone.  Results as mb_engine_enqueue (device memory, layout of
+ * mb_queries_layout). */
+#define MB_BATCH_MAX 128
+typedef enum mb_prefetch {
+  MB_PREFETCH_AUTO = 0,     /* columns the batch's selected rows hit densely */
+  MB_PREFETCH_NONE = 1,
+  MB_PREFETCH_ALL = 2       /* every column an op reads for every selected row */
+} mb_prefetch;
+typedef struct mb_batch_opts {
+  uint32_t words_per_lane;  /* 1, 2 or 4 (0 = auto): a tile is 1024 * words_per_lane rows */
+  uint32_t warps;           /* warps per CTA, 1..16 (0 = 16) */
+  uint32_t stages;          /* staged tiles in flight per CTA, 1..4 (0 = as many as fit) */
+  uint32_t ctas_per_sm;     /* 0 = occupancy */
+  uint32_t prefetch;        /* mb_prefetch */
+  uint32_t pad_[3];
+} mb_batch_opts;
+MB_API mb_status mb_engine_enqueue_batch(mb_engine *e, const mb_query *qs, uint32_t n,
+                                         const mb_batch_opts *opts, int64_t *out_dev,
+                                         uint64_t *nqual_dev);
+/* The same with host buffers: results (layout of mb_queries_layout) are
+ * copied to out_host / nqual_host (may be NULL), and the call returns when
+ * they are there. */
+MB_API mb_status mb_engine_query_batch(mb_engine *e, const mb_query *qs, uint32_t n,
+                                       const mb_batch_opts *opts, int64_t *out_host,
+                                       uint64_t *nqual_host);
 
 #ifdef __cplusplus
 } /* extern "C" */

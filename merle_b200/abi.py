@@ -104,7 +104,8 @@ class mb_star_host(C.Structure):
 class mb_engine_info(C.Structure):
     _fields_ = [("nrows", C.c_uint64), ("fact_bytes", C.c_uint64), ("dim_bytes", C.c_uint64),
                 ("index_bytes", C.c_uint64), ("k", C.c_uint32), ("width4", C.c_uint32),
-                ("nbitmaps", C.c_uint32), ("sms", C.c_uint32), ("index_build_ms", C.c_float)]
+                ("nbitmaps", C.c_uint32), ("sms", C.c_uint32), ("index_build_ms", C.c_float),
+                ("denorm", C.c_uint32), ("denorm_bytes", C.c_uint64)]
 
 
 class mb_query(C.Structure):
@@ -112,6 +113,14 @@ class mb_query(C.Structure):
 
 
 PLAN_FUSED, PLAN_SCAN, PLAN_MATERIALISED = range(3)
+MB_INDEX_PROBE_DIMS = 1
+MB_BATCH_MAX = 128
+PREFETCH_AUTO, PREFETCH_NONE, PREFETCH_ALL = range(3)
+
+
+class mb_batch_opts(C.Structure):
+    _fields_ = [("words_per_lane", C.c_uint32), ("warps", C.c_uint32), ("stages", C.c_uint32),
+                ("ctas_per_sm", C.c_uint32), ("prefetch", C.c_uint32), ("pad_", C.c_uint32 * 3)]
 
 
 class mb_plan(C.Structure):
@@ -163,6 +172,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_engine_gen_star": (I32, [VOIDP, U64, U32, U64, U64, I32]),
     "mb_engine_load_star": (I32, [VOIDP, C.POINTER(mb_star_host)]),
     "mb_engine_build_index": (I32, [VOIDP]),
+    "mb_engine_build_index_ex": (I32, [VOIDP, U32]),
     "mb_engine_get_info": (I32, [VOIDP, C.POINTER(mb_engine_info)]),
     "mb_query_ngroups": (U32, [C.POINTER(mb_query)]),
     "mb_engine_plan_rule": (I32, [VOIDP, C.POINTER(mb_query), C.POINTER(mb_plan)]),
@@ -174,6 +184,8 @@ SIGNATURES: dict[str, tuple] = {
     "mb_engine_mark": (I32, [VOIDP, U32]),
     "mb_engine_marks_ms": (I32, [VOIDP, U32, U32, C.POINTER(C.c_float)]),
     "mb_engine_stream": (VOIDP, [VOIDP]),
+    "mb_engine_enqueue_batch": (I32, [VOIDP, C.POINTER(mb_query), U32, C.POINTER(mb_batch_opts), VOIDP, VOIDP]),
+    "mb_engine_query_batch": (I32, [VOIDP, C.POINTER(mb_query), U32, C.POINTER(mb_batch_opts), VOIDP, VOIDP]),
     "mb_gen_flat": (I32, [U64, U64, U64, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP]),
     "mb_gen_star": (I32, [U64, U32, U64, U64, I32, C.POINTER(mb_star_cols), VOIDP]),
     "mb_gen_star_dims": (I32, [U64, U32, VOIDP, VOIDP, VOIDP, VOIDP]),

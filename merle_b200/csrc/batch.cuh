@@ -1,0 +1,108 @@
+// batch.cuh - the batched scan: one persistent launch evaluates a batch of
+// conjunctive queries over the resident bitmap index and shares every HBM
+// read between them.
+//
+// Per row tile (T = 32 * V words = 1024 * V rows) a CTA stages the tile of
+// every DISTINCT bitmap the batch reads (the union: each word fetched from
+// HBM once per batch instead of once per query) and prefetches into L2 the
+// tile's rows of every payload column the batch's ops read densely.  The
+// CTA's warps then take the batch's queries off a counter, costliest first,
+// evaluate each query's conjunctive chain from shared memory and append the
+// selected rows of all queries to one tile-wide row list; the ops then run
+// over that list in 64-row chunks, so every query of the batch gathers from
+// the same prefetched payload lines.
+//
+// The op of a batch query is its mb_op restated per source slot: the
+// intersected bounds of the single-term clauses on the slot (re-checked for
+// uncertain rows only), the slot's group-key transform (divisions by
+// multiplication with a precomputed magic number), and the slots of the
+// value.  Ops outside that form (a clause with several terms, a source in two
+// keys, sources wider than 4 bytes) run through the single-query path.
+#pragma once
+#include "common.cuh"
+
+namespace mb {
+
+constexpr uint32_t BQ_MAX = 128;   // queries per launch (7-bit query field of a row entry)
+constexpr uint32_t BU_MAX = 256;   // distinct bitmaps per launch (8-bit index)
+constexpr uint32_t BS_MAX = 16;    // distinct op sources per launch
+constexpr uint32_t BC_MAX = 4096;  // chain entries per launch
+constexpr uint32_t BW_MAX = 16;    // warps per CTA
+constexpr uint32_t BSLOT = MB_MAXSRC;
+
+// One op source of the batch: a column read by row or through a foreign key.
+struct BatchSrc {
+  const void *col;
+  const uint32_t *fk;
+  uint32_t dimsz;  // keys >= dimsz make the source invalid (0: unchecked)
+  uint32_t width;  // 1, 2 or 4 bytes
+};
+
+// Query descriptor: BQD_WORDS 32-bit words.
+//   [0] nslot | single group << 8 | vkind << 16 | va << 20 | vb << 24
+//   [1] groups   [2] first output slot   [3] row-count slot
+//   [4] first chain entry | entries << 16
+//   [5] kv mask | filt mask << 8 | key mask << 16 | term mask << 24 (bit s: slot s)
+//   [6], [7] unused
+//   slot s at 8 + 7 * s:
+//     [0] source index | width << 8 | key xform << 16 | division shifts << 24
+//     [1] term lo  [2] term hi (inclusive)  [3] division magic  [4] key base
+//     [5] key multiplier  [6] divisor
+enum : uint32_t { BQD_SLOT0 = 8, BQD_SLOTW = 7, BQD_WORDS = 8 + 7 * BSLOT };
+
+struct BatchHdr {
+  uint64_t nrows, nwords;
+  uint64_t stride;       // allocated words per bitmap: a multiple of 32, >= nwords
+  uint32_t nq, nu, nsrc, nchain;
+  uint32_t pf_mask;      // bit i: prefetch source i's row-indexed column into L2
+  uint32_t pad_[3];
+  BatchSrc src[BS_MAX];
+  const uint32_t *ubmp[BU_MAX];
+  uint32_t Qd[BQ_MAX * BQD_WORDS];
+  uint16_t chain[BC_MAX];  // union bitmap index | CNF_* flags << 8
+  uint8_t order[BQ_MAX];   // the order in which warps take the queries (costliest first)
+};
+
+// Launch shape of the batched scan.
+struct BatchCfg {
+  uint32_t V;       // words per lane: tile = 32 * V words
+  uint32_t warps;   // warps per CTA
+  uint32_t stages;  // staged tiles in flight per CTA
+  uint32_t cps;     // CTAs per SM (0: as many as fit)
+};
+
+// Launches the batched scan over the header at dh (device copy of h, which
+// the host keeps for the sizes); out / nqual are zeroed by the caller.
+mb_status batch_scan(const BatchHdr &h, const BatchHdr *dh, const BatchCfg &cfg, int64_t *out, uint64_t *nqual,
+                     cudaStream_t st);
+
+// Shared-memory bytes of a launch (0 if the configuration is invalid).
+size_t batch_smem(const BatchHdr &h, const BatchCfg &cfg);
+
+// Unsigned 32-bit division by an invariant divisor d >= 1 as a multiply-high
+// and shifts (Granlund and Montgomery, "Division by Invariant Integers using
+// Multiplication", PLDI 1994, figure 4.1): with l = ceil(log2 d),
+// m = floor(2^32 * (2^l - d) / d) + 1, sh1 = min(l, 1), sh2 = max(l - 1, 0),
+// x / d = (t + ((x - t) >> sh1)) >> sh2 where t = mulhi(m, x).
+struct DivMagic {
+  uint32_t m, sh1, sh2;
+};
+inline DivMagic div_magic(uint32_t d) {
+  uint32_t l = 0;
+  while (l < 32 && (1ull << l) < d) ++l;
+  DivMagic r;
+  r.m = (uint32_t)((((1ull << l) - d) << 32) / d + 1);
+  r.sh1 = l < 1 ? l : 1;
+  r.sh2 = l > 0 ? l - 1 : 0;
+  return r;
+}
+__host__ __device__ inline uint32_t div_by_magic(uint32_t x, uint32_t m, uint32_t sh1, uint32_t sh2) {
+#ifdef __CUDA_ARCH__
+  const uint32_t t = __umulhi(m, x);
+#else
+  const uint32_t t = (uint32_t)(((uint64_t)m * x) >> 32);
+#endif
+  return (t + ((x - t) >> sh1)) >> sh2;
+}
+
+}  // namespace mb

@@ -12,7 +12,10 @@
 // choosing by the bytes each option reads.
 #include <string.h>
 #include <algorithm>
+#include <unordered_map>
+#include "batch.cuh"
 #include "engine.h"
+#include "vbp.cuh"
 
 namespace mb {
 
@@ -23,6 +26,10 @@ Engine::~Engine() {
   allocs.clear();
   if (h_out) cudaFreeHost(h_out);
   if (h_nqual) cudaFreeHost(h_nqual);
+  for (int i = 0; i < BQ_RING; ++i) {
+    if (bq_host[i]) cudaFreeHost(bq_host[i]);
+    if (bq_copied[i]) cudaEventDestroy(bq_copied[i]);
+  }
   for (cudaEvent_t ev : qev) cudaEventDestroy(ev);
   for (cudaEvent_t ev : marks)
     if (ev) cudaEventDestroy(ev);
@@ -56,6 +63,7 @@ void Engine::free_star() {
   free_one(allocs, partmfgr);
   custcity = suppcity_dim = nullptr;
   partmfgr = nullptr;
+  free_denorm();
   for (auto &c : idx)
     for (auto &l : c.levels) free_one(allocs, l.slab);
   for (auto &c : idx) c.levels.clear();
@@ -145,6 +153,69 @@ static mb_src join_src(const void *dim, const void *fk, uint64_t dimsz, uint32_t
   return s;
 }
 
+mb_src Engine::ccity_src() const {
+  return custcity_row ? fact_src(custcity_row, 1) : join_src(custcity, custkey, ncust + 1, 1);
+}
+
+mb_src Engine::mfgr_src() const {
+  return partmfgr_row ? fact_src(partmfgr_row, 2) : join_src(partmfgr, partkey, npart + 1, 2);
+}
+
+void Engine::free_denorm() {
+  free_one(allocs, custcity_row);
+  free_one(allocs, partmfgr_row);
+  custcity_row = nullptr;
+  partmfgr_row = nullptr;
+}
+
+// out[r] = dim[fk[r]]; counts the rows whose key lies outside the dimension.
+template <typename D>
+__global__ void denorm_kernel(const uint32_t *__restrict__ fk, const D *__restrict__ dim, uint64_t dimsz,
+                              D *__restrict__ out, uint64_t n, unsigned long long *bad) {
+  uint32_t nbad = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = __ldcs(fk + i);
+    D v = 0;
+    if (k < dimsz) v = __ldg(dim + k);
+    else ++nbad;
+    out[i] = v;
+  }
+  nbad = __reduce_add_sync(0xffffffffu, nbad);
+  if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad, (unsigned long long)nbad);
+}
+
+// Builds custcity_row and partmfgr_row; a column whose foreign keys leave
+// their dimension is dropped again (its queries keep the probe, which
+// treats such rows as the op semantics say).
+mb_status Engine::build_denorm() {
+  free_denorm();
+  unsigned long long *d_bad = nullptr;
+  MB_CHECK(alloc((void **)&d_bad, 16));
+  MB_CUDA(cudaMemsetAsync(d_bad, 0, 16, stream));
+  MB_CHECK(alloc((void **)&custcity_row, nrows));
+  MB_CHECK(alloc((void **)&partmfgr_row, nrows * 2));
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(nrows, 256), 148ull * 8));
+  denorm_kernel<uint8_t><<<grid, 256, 0, stream>>>(reinterpret_cast<const uint32_t *>(custkey), custcity,
+                                                    ncust + 1, custcity_row, nrows, d_bad);
+  MB_LAUNCH_CHECK("denorm_kernel");
+  denorm_kernel<uint16_t><<<grid, 256, 0, stream>>>(reinterpret_cast<const uint32_t *>(partkey), partmfgr,
+                                                     npart + 1, partmfgr_row, nrows, d_bad + 1);
+  MB_LAUNCH_CHECK("denorm_kernel");
+  unsigned long long bad[2] = {0, 0};
+  MB_CUDA(cudaMemcpyAsync(bad, d_bad, 16, cudaMemcpyDeviceToHost, stream));
+  MB_CUDA(cudaStreamSynchronize(stream));
+  free_one(allocs, d_bad);
+  if (bad[0]) {
+    free_one(allocs, custcity_row);
+    custcity_row = nullptr;
+  }
+  if (bad[1]) {
+    free_one(allocs, partmfgr_row);
+    partmfgr_row = nullptr;
+  }
+  return MB_OK;
+}
+
 mb_status Engine::setup_index_cols() {
   auto lv = [](std::vector<uint64_t> b) {
     Level l;
@@ -168,7 +239,7 @@ mb_status Engine::setup_index_cols() {
   q.levels = {lv(range_bounds(1, 51, 1))};
   IdxCol &cc = idx[IC_CCITY];
   cc.name = "custcity";
-  cc.src = join_src(custcity, custkey, ncust + 1, 1);
+  cc.src = ccity_src();
   cc.dom_lo = 0, cc.dom_hi = 250;
   cc.levels = {lv(range_bounds(0, 250, 50)), lv(range_bounds(0, 250, 10))};
   IdxCol &sc = idx[IC_SCITY];
@@ -178,7 +249,7 @@ mb_status Engine::setup_index_cols() {
   sc.levels = {lv(range_bounds(0, 250, 50)), lv(range_bounds(0, 250, 10))};
   IdxCol &m = idx[IC_MFGR];
   m.name = "partmfgr";
-  m.src = join_src(partmfgr, partkey, npart + 1, 2);
+  m.src = mfgr_src();
   m.dom_lo = 0, m.dom_hi = 1000;
   m.levels = {lv(range_bounds(0, 1000, 200)), lv(range_bounds(0, 1000, 40))};
   return MB_OK;
@@ -344,8 +415,7 @@ static void build_op(const Engine &E, const mb_query &q, mb_op &out) {
   const uint32_t *p = q.p;
   const mb_src date = fact_src(E.orderdate, E.fact_width("orderdate"));
   const mb_src scity = fact_src(E.suppcity, E.fact_width("suppcity"));
-  const mb_src ccity = join_src(E.custcity, E.custkey, E.ncust + 1, 1);
-  const mb_src mfgr = join_src(E.partmfgr, E.partkey, E.npart + 1, 2);
+  const mb_src ccity = E.ccity_src(), mfgr = E.mfgr_src();
   const mb_src rev = fact_src(E.revenue, 4);
   if (q.tmpl == 1) {
     uint32_t sd = b.src(date), sdi = b.src(fact_src(E.discount, E.fact_width("discount")));
@@ -555,8 +625,11 @@ extern "C" mb_status mb_engine_load_star(mb_engine *e, const mb_star_host *h) {
   return E.setup_index_cols();
 }
 
-extern "C" mb_status mb_engine_build_index(mb_engine *e) {
+extern "C" mb_status mb_engine_build_index(mb_engine *e) { return mb_engine_build_index_ex(e, 0); }
+
+extern "C" mb_status mb_engine_build_index_ex(mb_engine *e, uint32_t flags) {
   if (!e) return fail(MB_ERR_INVALID, "mb_engine_build_index: NULL engine");
+  if (flags & ~MB_INDEX_PROBE_DIMS) return fail(MB_ERR_INVALID, "mb_engine_build_index_ex: flags 0x%x", flags);
   Engine &E = e->E;
   if (!E.custkey) return fail(MB_ERR_INVALID, "mb_engine_build_index: no table");
   MB_CUDA(cudaSetDevice(E.device));
@@ -565,9 +638,13 @@ extern "C" mb_status mb_engine_build_index(mb_engine *e) {
       free_one(E.allocs, l.slab);
       l.slab = nullptr;
     }
+  E.indexed = false;
+  MB_CUDA(cudaEventRecord(E.ev0, E.stream));
+  if (flags & MB_INDEX_PROBE_DIMS) E.free_denorm();
+  else MB_CHECK(E.build_denorm());
+  MB_CHECK(E.setup_index_cols());
   uint64_t *d_pop = nullptr;
   MB_CHECK(E.alloc((void **)&d_pop, 1024 * 8));
-  MB_CUDA(cudaEventRecord(E.ev0, E.stream));
   for (auto &c : E.idx) {
     for (auto &l : c.levels) {
       const uint32_t nb = l.nbins();
@@ -605,6 +682,8 @@ extern "C" mb_status mb_engine_get_info(mb_engine *e, mb_engine_info *o) {
     }
   o->sms = (uint32_t)dev_info().sms;
   o->index_build_ms = E.index_build_ms;
+  o->denorm = (E.custcity_row || E.partmfgr_row) ? 1u : 0u;
+  o->denorm_bytes = (E.custcity_row ? E.nrows : 0) + (E.partmfgr_row ? E.nrows * 2 : 0);
   return MB_OK;
 }
 
@@ -773,3 +852,299 @@ extern "C" mb_status mb_engine_marks_ms(mb_engine *e, uint32_t a, uint32_t b, fl
 }
 
 extern "C" void *mb_engine_stream(mb_engine *e) { return e ? (void *)e->E.stream : nullptr; }
+
+// ------------------------------------------------------------------ batches
+namespace mb {
+
+// Inclusive 32-bit form of a half-open 64-bit term [lo, hi) over values that
+// fit 32 bits; an empty term becomes lo = 1, hi = 0.
+static void term32(uint64_t lo, uint64_t hi, uint32_t &l, uint32_t &h) {
+  if (lo >= hi || lo > 0xffffffffull) {
+    l = 1, h = 0;
+    return;
+  }
+  l = (uint32_t)lo;
+  h = (uint32_t)((hi > 0x100000000ull ? 0x100000000ull : hi) - 1);
+}
+
+enum { BADD_OK = 0, BADD_FULL = 1, BADD_ALONE = 2 };
+
+// Batch under construction: the staging header and its lookup tables.
+struct BatchBuild {
+  BatchHdr *h = nullptr;
+  std::unordered_map<const uint32_t *, uint32_t> umap;
+  std::vector<double> cost;        // estimated cost of each query (per bitmap word)
+  double src_weight[BS_MAX] = {};  // selected-row fraction reading each source
+
+  void reset(BatchHdr *hh, uint64_t nrows, uint64_t stride) {
+    h = hh;
+    memset(h, 0, sizeof(*h));
+    h->nrows = nrows;
+    h->nwords = (nrows + 31) / 32;
+    h->stride = stride;
+    umap.clear();
+    cost.clear();
+    for (double &w : src_weight) w = 0;
+  }
+};
+
+static bool same_src(const mb_src &a, const mb_src &b) {
+  return a.col == b.col && a.fk == b.fk && a.width == b.width && a.dimsz == b.dimsz;
+}
+
+static int src_slot(const BatchHdr &h, const mb_src &s) {
+  for (uint32_t i = 0; i < h.nsrc; ++i) {
+    const BatchSrc &b = h.src[i];
+    if (b.col == s.col && b.fk == s.fk && b.width == s.width && b.dimsz == (uint32_t)s.dimsz) return (int)i;
+  }
+  return -1;
+}
+
+// The op as the batch kernel's per-slot descriptor (batch.cuh); false if it
+// is outside that form.
+static bool slot_plan(const mb_op &O, uint32_t *d) {
+  if (O.nsrc > BSLOT) return false;
+  for (uint32_t s = 0; s < O.nsrc; ++s)
+    if (O.src[s].width > 4 || O.src[s].width == 3 || O.src[s].dimsz > 0xffffffffull) return false;
+  const OpNeeds N = op_needs(O);
+  uint32_t termm = 0, keym = 0;
+  uint32_t lo[BSLOT], hi[BSLOT];
+  for (uint32_t s = 0; s < BSLOT; ++s) lo[s] = 0, hi[s] = 0xffffffffu;
+  for (uint32_t c = 0; c < O.nclause; ++c) {
+    if (O.clause_len[c] != 1) return false;  // OR clauses: single-query path
+    const mb_term &t = O.terms[c];
+    uint32_t l, h;
+    term32(t.lo, t.hi, l, h);
+    const uint32_t s = t.src;
+    termm |= 1u << s;
+    lo[s] = std::max(lo[s], l);
+    hi[s] = std::min(hi[s], h);
+  }
+  for (uint32_t k = 0; k < O.nkey; ++k) {
+    const mb_key &kk = O.keys[k];
+    if ((keym >> kk.src) & 1u) return false;  // a source in two keys
+    keym |= 1u << kk.src;
+    uint32_t *sl = d + BQD_SLOT0 + BQD_SLOTW * kk.src;
+    uint32_t sh = 0;
+    if (kk.xform == MB_X_DIV) {
+      const DivMagic m = div_magic(kk.div);
+      for (uint32_t x : {0u, 1u, kk.div - 1, kk.div, kk.div + 1, 12345u, 0x7fffffffu, 0xfffffffeu, 0xffffffffu})
+        if (div_by_magic(x, m.m, m.sh1, m.sh2) != x / kk.div) return false;
+      sl[3] = m.m;
+      sh = m.sh1 | (m.sh2 << 4);
+    }
+    sl[0] |= (kk.xform << 16) | (sh << 24);
+    sl[4] = kk.base;
+    sl[5] = kk.mul;
+    sl[6] = kk.div;
+  }
+  for (uint32_t s = 0; s < O.nsrc; ++s) {
+    uint32_t *sl = d + BQD_SLOT0 + BQD_SLOTW * s;
+    sl[0] |= O.src[s].width << 8;
+    if ((termm >> s) & 1u) {
+      if (lo[s] > hi[s]) lo[s] = 1, hi[s] = 0;
+      sl[1] = lo[s];
+      sl[2] = hi[s];
+    }
+  }
+  d[0] = O.nsrc | (O.vkind << 16) | (O.va << 20) | (O.vb << 24);
+  d[5] = (N.kv_mask & 0xffu) | ((N.filt_mask & 0xffu) << 8) | (keym << 16) | (termm << 24);
+  return true;
+}
+
+// Adds a lowered query (its conjunctive program P) as the next query of the
+// batch.  BADD_FULL: a limit of this launch is reached (flush and retry);
+// BADD_ALONE: the batch kernel cannot run the query.
+static int batch_add(BatchBuild &B, const Lowered &L, const DevPrg &P, uint64_t out_off, uint32_t nq_slot,
+                     double sel) {
+  BatchHdr &h = *B.h;
+  const mb_op &O = L.op;
+  if (!P.cnf) return BADD_ALONE;
+  if (out_off + L.ngroups >= 0x80000000ull) return BADD_ALONE;
+  uint32_t d[BQD_WORDS];
+  memset(d, 0, sizeof(d));
+  if (!slot_plan(O, d)) return BADD_ALONE;
+  // bitmaps and sources this query adds to the batch
+  std::vector<const uint32_t *> fresh;
+  for (uint32_t i = 0; i < P.ncnf; ++i) {
+    const uint32_t *p = P.cnf_ptr[i];
+    if (((uintptr_t)p & 15) != 0) return BADD_ALONE;
+    if (!B.umap.count(p) && std::find(fresh.begin(), fresh.end(), p) == fresh.end()) fresh.push_back(p);
+  }
+  uint32_t newsrc = 0;
+  for (uint32_t s = 0; s < O.nsrc; ++s) {
+    bool seen = src_slot(h, O.src[s]) >= 0;
+    for (uint32_t t = 0; t < s && !seen; ++t) seen = same_src(O.src[t], O.src[s]);
+    if (!seen) ++newsrc;
+  }
+  if (fresh.size() > BU_MAX || newsrc > BS_MAX || P.ncnf > BC_MAX) return BADD_ALONE;
+  if (h.nq + 1 > BQ_MAX || h.nu + fresh.size() > BU_MAX || h.nsrc + newsrc > BS_MAX || h.nchain + P.ncnf > BC_MAX)
+    return BADD_FULL;
+  // commit
+  const uint32_t q = h.nq++;
+  for (const uint32_t *p : fresh) {
+    B.umap[p] = h.nu;
+    h.ubmp[h.nu++] = p;
+  }
+  const OpNeeds N = op_needs(O);
+  for (uint32_t s = 0; s < O.nsrc; ++s) {
+    int t = src_slot(h, O.src[s]);
+    if (t < 0) {
+      t = (int)h.nsrc++;
+      BatchSrc &b = h.src[t];
+      b.col = O.src[s].col;
+      b.fk = O.src[s].fk;
+      b.dimsz = (uint32_t)O.src[s].dimsz;
+      b.width = O.src[s].width;
+    }
+    d[BQD_SLOT0 + BQD_SLOTW * s] |= (uint32_t)t;
+    if ((N.kv_mask >> s) & 1u) B.src_weight[t] += sel;
+  }
+  d[0] |= (L.ngroups == 1 ? 1u : 0u) << 8;
+  d[1] = L.ngroups;
+  d[2] = (uint32_t)out_off;
+  d[3] = nq_slot;
+  d[4] = h.nchain | ((uint32_t)P.ncnf << 16);
+  memcpy(h.Qd + (size_t)q * BQD_WORDS, d, sizeof(d));
+  for (uint32_t i = 0; i < P.ncnf; ++i)
+    h.chain[h.nchain++] = (uint16_t)(B.umap[P.cnf_ptr[i]] | ((uint32_t)P.cnf_flag[i] << 8));
+  // cost per bitmap word of a tile: the chain entries, the compaction, and
+  // the ops of the selected rows (about 2 chain entries' worth per row)
+  B.cost.push_back((double)P.ncnf + 2.0 + 64.0 * sel);
+  return BADD_OK;
+}
+
+// Selected-row fraction of a lowered query: the product of its predicates'
+// estimated fractions (bin popcounts, predicates taken as independent).
+static double est_selectivity(const Engine &E, const Lowered &L) {
+  if (E.nrows == 0) return 0;
+  double f = 1;
+  for (const Cover &c : L.covers)
+    if (!c.full) f *= std::min(1.0, (double)c.est_rows / (double)E.nrows);
+  return f;
+}
+
+// The launch shape: the options given, and for stages left at 0 the most
+// (up to 4) that fit in shared memory, narrowing the tile if not even two do.
+static BatchCfg batch_cfg(const BatchHdr &h, const mb_batch_opts &o) {
+  BatchCfg c;
+  c.V = o.words_per_lane ? o.words_per_lane : 2;
+  c.warps = o.warps ? std::min<uint32_t>(o.warps, BW_MAX) : BW_MAX;
+  c.cps = o.ctas_per_sm;
+  c.stages = o.stages;
+  const size_t cap = (size_t)dev_info().max_smem_optin;
+  if (!c.stages) {
+    while (true) {
+      for (c.stages = 4; c.stages > 1; --c.stages)
+        if (batch_smem(h, c) && batch_smem(h, c) <= cap) break;
+      if (c.stages > 1 || c.V == 1 || o.words_per_lane) break;
+      c.V >>= 1;
+    }
+  }
+  return c;
+}
+
+// Orders the batch's queries, copies its header to the device and launches
+// the scan.
+static mb_status batch_flush(Engine &E, BatchBuild &B, const mb_batch_opts &o, int64_t *out, uint64_t *nq,
+                             uint32_t slot) {
+  BatchHdr &h = *B.h;
+  if (h.nq == 0) return MB_OK;
+  std::vector<uint32_t> order(h.nq);
+  for (uint32_t q = 0; q < h.nq; ++q) order[q] = q;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return B.cost[a] > B.cost[b]; });
+  for (uint32_t i = 0; i < h.nq; ++i) h.order[i] = (uint8_t)order[i];
+  h.pf_mask = 0;
+  for (uint32_t i = 0; i < h.nsrc; ++i) {
+    const void *base = h.src[i].fk ? (const void *)h.src[i].fk : h.src[i].col;
+    const bool aligned = ((uintptr_t)base & 15) == 0;
+    const bool dense = o.prefetch == MB_PREFETCH_ALL || (o.prefetch == MB_PREFETCH_AUTO && B.src_weight[i] >= 0.02);
+    if (aligned && dense && B.src_weight[i] > 0) h.pf_mask |= 1u << i;
+  }
+  const BatchCfg c = batch_cfg(h, o);
+  MB_CUDA(cudaMemcpyAsync(E.bq_dev, &h, sizeof(BatchHdr), cudaMemcpyHostToDevice, E.stream));
+  MB_CUDA(cudaEventRecord(E.bq_copied[slot], E.stream));
+  return batch_scan(h, static_cast<const BatchHdr *>(E.bq_dev), c, out, nq, E.stream);
+}
+
+// The next staging header of the ring, once its previous copy is done.
+static mb_status batch_staging(Engine &E, BatchHdr **out, uint32_t *slot) {
+  if (!E.bq_dev) {
+    for (int i = 0; i < Engine::BQ_RING; ++i) {
+      MB_CUDA(cudaMallocHost(&E.bq_host[i], sizeof(BatchHdr)));
+      MB_CUDA(cudaEventCreateWithFlags(&E.bq_copied[i], cudaEventDisableTiming));
+    }
+    MB_CHECK(E.alloc(&E.bq_dev, sizeof(BatchHdr)));
+  }
+  const uint32_t i = E.bq_next;
+  E.bq_next = (E.bq_next + 1) % Engine::BQ_RING;
+  MB_CUDA(cudaEventSynchronize(E.bq_copied[i]));  // an unrecorded event counts as complete
+  *out = static_cast<BatchHdr *>(E.bq_host[i]);
+  *slot = i;
+  return MB_OK;
+}
+
+}  // namespace mb
+
+extern "C" mb_status mb_engine_enqueue_batch(mb_engine *e, const mb_query *qs, uint32_t n, const mb_batch_opts *opts,
+                                             int64_t *out_dev, uint64_t *nqual_dev) {
+  if (!e || (!qs && n) || !out_dev || !nqual_dev) return fail(MB_ERR_INVALID, "mb_engine_enqueue_batch: NULL argument");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  mb_batch_opts o;
+  if (opts) o = *opts;
+  else memset(&o, 0, sizeof(o));
+  if ((o.words_per_lane && o.words_per_lane != 1 && o.words_per_lane != 2 && o.words_per_lane != 4) ||
+      o.warps > 16 || o.stages > 4 || o.prefetch > MB_PREFETCH_ALL)
+    return fail(MB_ERR_INVALID, "mb_engine_enqueue_batch: options out of range");
+  std::vector<uint64_t> offs(n);
+  const uint64_t total = mb_queries_layout(qs, n, offs.data());
+  MB_CUDA(cudaMemsetAsync(out_dev, 0, total * 8, E.stream));
+  MB_CUDA(cudaMemsetAsync(nqual_dev, 0, (size_t)n * 8, E.stream));
+  mb_plan pl;  // the rule plan (queries the batch kernel cannot take run with it alone)
+  memset(&pl, 0, sizeof(pl));
+  pl.kind = MB_PLAN_FUSED;
+  pl.launch.grp_strategy = MB_GRP_AUTO;
+  BatchBuild B;
+  BatchHdr *h = nullptr;
+  uint32_t slot = 0;
+  MB_CHECK(batch_staging(E, &h, &slot));
+  B.reset(h, E.nrows, E.stride);
+  Lowered L;
+  DevPrg P;
+  for (uint32_t i = 0; i < n; ++i) {
+    MB_CHECK(lower_query(E, qs[i], pl, L));
+    if (L.empty) continue;  // outputs stay zero
+    bool v4 = false;
+    MB_CHECK(flatten_prg(&L.prg, L.chk ? 1 : 0, &P, &v4));
+    const double sel = est_selectivity(E, L);
+    int r = batch_add(B, L, P, offs[i], i, sel);
+    if (r == BADD_FULL) {
+      MB_CHECK(batch_flush(E, B, o, out_dev, nqual_dev, slot));
+      MB_CHECK(batch_staging(E, &h, &slot));
+      B.reset(h, E.nrows, E.stride);
+      r = batch_add(B, L, P, offs[i], i, sel);
+    }
+    if (r != BADD_OK) MB_CHECK(run_lowered(E, L, pl, out_dev + offs[i], nqual_dev + i, false));
+  }
+  return batch_flush(E, B, o, out_dev, nqual_dev, slot);
+}
+
+extern "C" mb_status mb_engine_query_batch(mb_engine *e, const mb_query *qs, uint32_t n, const mb_batch_opts *opts,
+                                           int64_t *out_host, uint64_t *nqual_host) {
+  if (!e || (!qs && n) || !out_host) return fail(MB_ERR_INVALID, "mb_engine_query_batch: NULL argument");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  const uint64_t total = mb_queries_layout(qs, n, nullptr);
+  if (E.bout_cap < total + n) {
+    free_one(E.allocs, E.bout);
+    E.bout = nullptr;
+    MB_CHECK(E.alloc((void **)&E.bout, (total + n) * 8));
+    E.bout_cap = total + n;
+  }
+  MB_CHECK(mb_engine_enqueue_batch(e, qs, n, opts, E.bout, reinterpret_cast<uint64_t *>(E.bout + total)));
+  MB_CUDA(cudaMemcpyAsync(out_host, E.bout, total * 8, cudaMemcpyDeviceToHost, E.stream));
+  if (nqual_host) MB_CUDA(cudaMemcpyAsync(nqual_host, E.bout + total, (size_t)n * 8, cudaMemcpyDeviceToHost, E.stream));
+  MB_CUDA(cudaStreamSynchronize(E.stream));
+  return check_device_error(E.stream);
+}

@@ -74,6 +74,11 @@ struct Engine {
        *supplycost = nullptr, *suppcity = nullptr;
   uint8_t *custcity = nullptr, *suppcity_dim = nullptr;
   uint16_t *partmfgr = nullptr;
+  // Denormalised dimension attributes, one per fact row (custcity[custkey],
+  // partmfgr[partkey]), built with the index: the ops and the index build
+  // read them directly instead of probing through the foreign key.
+  uint8_t *custcity_row = nullptr;
+  uint16_t *partmfgr_row = nullptr;
   IdxCol idx[IC_N];
   bool indexed = false;
   float index_build_ms = 0;
@@ -89,6 +94,14 @@ struct Engine {
   uint64_t rows_cap = 0;
   uint64_t *d_rowcnt = nullptr;  // row count of the materialised plan
   std::vector<void *> allocs;
+  // batch descriptors: a ring of pinned host staging headers (each reusable
+  // once its copy event completed) and the device copy
+  static constexpr int BQ_RING = 4;
+  void *bq_host[BQ_RING] = {}, *bq_dev = nullptr;
+  cudaEvent_t bq_copied[BQ_RING] = {};
+  uint32_t bq_next = 0;
+  int64_t *bout = nullptr;  // device results of mb_engine_query_batch
+  uint64_t bout_cap = 0;
   // timing: per-query event pairs of the last enqueue, and markers
   std::vector<cudaEvent_t> qev;
   uint32_t qev_used = 0;
@@ -101,7 +114,13 @@ struct Engine {
   mb_status ensure_rows(uint64_t n);
   mb_status alloc(void **p, size_t bytes);
   void free_star();
+  void free_denorm();
   mb_status setup_index_cols();
+  // Customer city / part mfgr of a row: the denormalised column when built,
+  // else a probe of the dimension through the foreign key.
+  mb_src ccity_src() const;
+  mb_src mfgr_src() const;
+  mb_status build_denorm();
 };
 
 // Planner and lowering (engine.cu).

@@ -34,12 +34,6 @@ namespace mb {
 constexpr uint32_t FT_THREADS = 256;
 constexpr uint32_t FT_WARPS = FT_THREADS / 32;
 
-// Which op sources every row needs (keys, value) and which only uncertain
-// rows need (filter terms).
-struct OpNeeds {
-  uint32_t kv_mask, filt_mask;
-};
-
 OpNeeds op_needs(const mb_op &O) {
   OpNeeds n{0, 0};
   for (uint32_t k = 0; k < O.nkey; ++k) n.kv_mask |= 1u << O.keys[k].src;

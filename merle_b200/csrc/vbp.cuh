@@ -215,6 +215,12 @@ mb_status fused_tma(const DevPrg &P, const mb_op &O, uint32_t nr_grp, int gs, ui
 namespace mb {
 // The warp-independent kernel for conjunctive programs (fused.cu).
 bool fused_warp_applies(const DevPrg &P, const mb_op &O);
+// Which op sources every row needs (keys, value) and which only uncertain
+// rows need (filter terms).
+struct OpNeeds {
+  uint32_t kv_mask, filt_mask;
+};
+OpNeeds op_needs(const mb_op &O);
 mb_status fused_warp(const DevPrg &P, const mb_op &O, uint32_t nr_grp, int gs, uint32_t hcap, uint32_t V,
                      uint32_t warps, int64_t *out, uint64_t *nq, uint32_t cps, cudaStream_t st);
 }  // namespace mb

@@ -36,8 +36,10 @@ class Engine:
     def load_star(self, h: abi.mb_star_host) -> None:
         check(lib().mb_engine_load_star(self._e, C.byref(h)))
 
-    def build_index(self) -> None:
-        check(lib().mb_engine_build_index(self._e))
+    def build_index(self, probe_dims: bool = False) -> None:
+        """Canonical index; probe_dims keeps the dimension probes through the
+        foreign keys instead of the denormalised per-row columns."""
+        check(lib().mb_engine_build_index_ex(self._e, abi.MB_INDEX_PROBE_DIMS if probe_dims else 0))
 
     def info(self) -> dict:
         i = abi.mb_engine_info()
@@ -62,3 +64,15 @@ class Engine:
         check(lib().mb_engine_query(self._e, C.byref(q), C.byref(plan) if plan is not None else None,
                                     out.ctypes.data, C.addressof(nq), C.byref(st)))
         return out[:ng], nq.value, st
+
+    def query_batch(self, qs: list[abi.mb_query], opts: abi.mb_batch_opts | None = None):
+        """Results of a batch through the batched scan (host buffers): the
+        concatenated group sums (layout of mb_queries_layout) and row counts."""
+        n = len(qs)
+        qarr = (abi.mb_query * max(n, 1))(*qs)
+        total = int(lib().mb_queries_layout(qarr, n, None))
+        out = np.zeros(max(total, 1), np.int64)
+        nq = np.zeros(max(n, 1), np.uint64)
+        check(lib().mb_engine_query_batch(self._e, qarr, n, C.byref(opts) if opts is not None else None,
+                                          out.ctypes.data, nq.ctypes.data))
+        return out[:total], nq[:n]

@@ -147,3 +147,112 @@ def test_engine_errors(eng, mb):
     q = abi.query(1, 0, 10, 0, 1, 1, 2)
     assert mb.lib().mb_engine_query(e.handle, C.byref(q), None, out.ctypes.data, None, None) == abi.MB_ERR_INVALID
     e.close()
+
+
+def _batch_oracle(orc, star, qs):
+    outs, nqs = [], []
+    for q in qs:
+        o, n = oracle_query(orc, star, q)
+        outs.append(o)
+        nqs.append(n)
+    return np.concatenate(outs) if outs else np.zeros(0, np.int64), np.array(nqs, np.uint64)
+
+
+BATCH_OPTS = [
+    (0, 0, 0, 0, abi.PREFETCH_AUTO),
+    (1, 8, 2, 0, abi.PREFETCH_NONE),
+    (2, 16, 3, 0, abi.PREFETCH_ALL),
+    (4, 16, 0, 0, abi.PREFETCH_AUTO),
+    (2, 4, 1, 2, abi.PREFETCH_AUTO),
+]
+
+
+def _mix_with_edges():
+    return WL.ssb13() + WL.random_mix(21, 40, narrow=0.4) + [
+        abi.query(1, 100, 100, 0, 11, 1, 51), abi.query(1, 0, 2557, 0, 11, 1, 51), abi.query(2, 37, 41, 3, 4),
+        abi.query(3, 13, 17, 201, 205, 59, 1500), abi.query(4, 0, 50, 0, 50, 0, 1000, 366, 2557)]
+
+
+@pytest.mark.parametrize("opts", BATCH_OPTS)
+def test_engine_batch_matches_oracle(eng, star, orc, mb, opts):
+    """The batched scan through the device-memory entry point, on every
+    launch shape, against the oracle (edge cases: empty, full, candidate
+    checks on both sides)."""
+    import torch
+    L = mb.lib()
+    qs = _mix_with_edges()
+    want, wn = _batch_oracle(orc, star, qs)
+    n = len(qs)
+    qarr = (abi.mb_query * n)(*qs)
+    total = int(L.mb_queries_layout(qarr, n, None))
+    assert total == len(want)
+    out = torch.zeros(total, dtype=torch.int64, device="cuda")
+    nq = torch.zeros(n, dtype=torch.int64, device="cuda")
+    o = abi.mb_batch_opts(*opts)
+    mb.check(L.mb_engine_enqueue_batch(eng.handle, qarr, n, C.byref(o), out.data_ptr(), nq.data_ptr()))
+    mb.check(L.mb_engine_sync(eng.handle, None, 0))
+    np.testing.assert_array_equal(out.cpu().numpy(), want)
+    np.testing.assert_array_equal(nq.cpu().numpy().astype(np.uint64), wn)
+
+
+def test_engine_batch_host_api_and_split(eng, star, orc):
+    qs = WL.random_mix(33, 300, narrow=0.3)  # > MB_BATCH_MAX: three launches
+    want, wn = _batch_oracle(orc, star, qs)
+    out, nq = eng.query_batch(qs)
+    np.testing.assert_array_equal(out, want)
+    np.testing.assert_array_equal(nq, wn)
+
+
+def test_engine_batch_alone_equals_in_mix(eng):
+    """Every query's results are the same alone (a batch of one, and the
+    single-query path) as inside a mix of 64."""
+    qs = WL.random_mix(3, 64, narrow=0.3)
+    out, nq = eng.query_batch(qs)
+    offs = np.concatenate([[0], np.cumsum([Engine.ngroups(q) for q in qs])])
+    for i in range(0, 64, 7):
+        a, an = eng.query_batch([qs[i]])
+        np.testing.assert_array_equal(a, out[offs[i]:offs[i + 1]])
+        assert an[0] == nq[i]
+        b, bn, _ = eng.query(qs[i])
+        np.testing.assert_array_equal(b, a)
+        assert bn == an[0]
+
+
+def test_engine_batch_invalid_options(eng, mb):
+    L = mb.lib()
+    qs = WL.random_mix(4, 2)
+    qarr = (abi.mb_query * 2)(*qs)
+    out = np.zeros(4096, np.int64)
+    for bad in [(3, 0, 0, 0, 0), (0, 17, 0, 0, 0), (0, 0, 5, 0, 0), (0, 0, 0, 0, 3)]:
+        o = abi.mb_batch_opts(*bad)
+        assert L.mb_engine_query_batch(eng.handle, qarr, 2, C.byref(o), out.ctypes.data, None) == abi.MB_ERR_INVALID
+
+
+def test_engine_denormalised_equals_probe(cuda, star, orc):
+    """The index over denormalised dimension columns and the one that probes
+    the dimensions through the foreign keys give the same results, on the
+    plan kinds and through the batch."""
+    g = G["ssb13"]
+    ep = Engine(0)
+    ep.gen_star(g["seed"], g["k"], g["n"])
+    ep.build_index(probe_dims=True)
+    ed = Engine(0)
+    ed.gen_star(g["seed"], g["k"], g["n"])
+    ed.build_index()
+    assert ep.info()["denorm"] == 0 and ed.info()["denorm"] == 1
+    assert ed.info()["denorm_bytes"] == 3 * g["n"]
+    qs = WL.ssb13() + WL.random_mix(8, 24, narrow=0.4)
+    for q in qs:
+        want, nqw = oracle_query(orc, star, q)
+        for e in (ep, ed):
+            for d in PLANS[:3]:
+                out, nq, _ = e.query(q, mkplan(d))
+                np.testing.assert_array_equal(out, want, err_msg=f"{WL.as_tuple(q)} {d}")
+                assert nq == nqw
+    want, wn = _batch_oracle(orc, star, qs)
+    for e in (ep, ed):
+        out, nq = e.query_batch(qs)
+        np.testing.assert_array_equal(out, want)
+        np.testing.assert_array_equal(nq, wn)
+    ep.close()
+    ed.close()
