@@ -120,7 +120,8 @@ PREFETCH_AUTO, PREFETCH_NONE, PREFETCH_ALL = range(3)
 
 class mb_batch_opts(C.Structure):
     _fields_ = [("words_per_lane", C.c_uint32), ("warps", C.c_uint32), ("stages", C.c_uint32),
-                ("ctas_per_sm", C.c_uint32), ("prefetch", C.c_uint32), ("pad_", C.c_uint32 * 3)]
+                ("ctas_per_sm", C.c_uint32), ("prefetch", C.c_uint32), ("drain_warps", C.c_uint32),
+                ("pad_", C.c_uint32 * 2)]
 
 
 class mb_plan(C.Structure):

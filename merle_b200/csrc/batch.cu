@@ -6,29 +6,34 @@
 // candidate-check semantics, so every query's groups and row count equal what
 // it gets alone.
 //
-// A CTA walks its row tiles (T = 32 * V words); per tile, with S stages of
-// the union bitmaps in flight:
-//   phase A  warps take the batch's queries off a counter (costliest first),
-//            evaluate each query's conjunctive chain on the staged words and
-//            append its selected rows - entry = row in tile << 8 | uncertain
-//            << 7 | query - to one tile-wide row list in shared memory, each
-//            query's rows reserved as one contiguous run;
-//   barrier  the stage is consumed: its refill with tile j + S starts (every
-//            thread issues its share of 16-byte cp.async copies, completing
-//            on the stage's mbarrier), plus an L2 prefetch of the tile's
-//            payload rows;
-//   phase B  warps take 64-entry chunks of the row list and run the ops, two
-//            rows per lane, each lane reading its own row's query descriptor
-//            (a chunk spans few queries, so most reads are broadcasts); the
-//            payload rows of the tile were prefetched into L2, and every
-//            query of the batch gathers from the same lines;
-//   barrier  the list is consumed.
-// 1-group sums and row counts accumulate per warp (plain adds by one leader
-// lane per query, no shared-memory atomics) and are folded at the end.  A
-// query whose rows do not fit the list (a dense query on a full list) runs
-// them through the warp's own 64-row queue instead.  Every wait is bounded: a
-// stage that does not arrive records the block in the device error word, and
-// the block stops walking and waits for its own copies before exiting.
+// A CTA's warps split into producers and consumers.
+//
+// Producers walk the CTA's row tiles (T = 32 * V words), S tiles of the
+// bitmaps in flight: the index is one slab of bitmap rows, so one thread
+// stages a tile of the whole run of rows the batch reads with a single 2-D
+// tensor copy (TMA, box = rows x T words, completing on the stage's
+// mbarrier) and prefetches the tile's payload rows into L2.  On a tile,
+// producers take the batch's queries off a counter, costliest first; for its
+// query a producer evaluates the conjunctive chain on the staged words and
+// appends the selected rows to the query's own row queue.  Every 64 queued
+// rows become a job in a ring in shared memory.  A producer barrier closes
+// the tile (then its stage is refilled), so a query is on one producer at a
+// time and its queue, which outlives the tile, needs no atomics.
+//
+// Consumers take jobs off the ring and run the op on their 64 rows: one
+// query per job, so every descriptor read is a broadcast and every branch on
+// the descriptor uniform (a compiled drain for the engine's op shapes, the
+// generic one otherwise).  Drains wait on payload gathers; on their own
+// warps that latency overlaps the producers' bitmap work instead of stalling
+// the tile.  A producer that finds the ring full runs the drain itself.
+// 1-group sums and row counts accumulate per warp (plain adds) and are
+// folded at the end.
+//
+// Job states move FREE -> FILL -> READY -> RUN -> FREE by compare-and-swap.
+// Every wait is bounded: a stage that does not arrive, or consumers idle for
+// too long, record the block in the device error word; the block then stops
+// and lets its copies land before exiting.
+#include <cudaTypedefs.h>
 #include <string.h>
 #include "batch.cuh"
 #include "opeval.cuh"
@@ -40,13 +45,18 @@ namespace mb {
 namespace {
 
 constexpr uint32_t BT_THREADS_MAX = BW_MAX * 32;
-constexpr uint32_t BL_CAP = 4096;  // entries of the tile row list
-constexpr uint32_t BWQ = 96;       // a warp's own queue: < 64 pending + one 32-entry round
+constexpr uint32_t BQQ = 96;  // a query's queue: < 64 pending + one 32-entry round
+constexpr uint32_t BJ = 64;   // jobs in the ring
+constexpr uint32_t CONSUMER_IDLE_TRIES = 1u << 24;  // x 128 ns sleeps, about two seconds
+enum : uint32_t { JOB_FREE = 0, JOB_FILL = 1, JOB_READY = 2, JOB_RUN = 3 };
+struct Job {
+  uint32_t state, q, n, pad_;
+  uint32_t rows[64];
+};
 
 // Shared-memory layout of one launch (identical on host and device).
 struct BLayout {
-  uint32_t nqs;  // query stride of the per-warp accumulators
-  uint32_t off_Q, off_src, off_ubmp, off_sum, off_cnt, off_bar, off_ctr, off_order, off_chain, off_list, off_wq,
+  uint32_t off_Q, off_src, off_sum, off_cnt, off_len, off_bar, off_ctr, off_order, off_chain, off_qbuf, off_jobs,
       off_stage, total;
 };
 
@@ -56,29 +66,28 @@ __host__ __device__ inline BLayout blayout(uint32_t nq, uint32_t nchain, uint32_
                                            uint32_t T) {
   BLayout L;
   uint32_t o = 0;
-  L.nqs = align_up(nq, 2);
   L.off_Q = o;
   o += nq * BQD_WORDS * 4;
   L.off_src = o = align_up(o, 16);
   o += BS_MAX * 24;  // col[] and fk[] (8 bytes), dimsz[] and width[] (4 bytes)
-  L.off_ubmp = o;
-  o += nu * 8;
   L.off_sum = o = align_up(o, 16);
-  o += warps * L.nqs * 8;  // per warp and query: 1-group sum
+  o += warps * nq * 8;  // per warp and query: 1-group sum
   L.off_cnt = o;
-  o += warps * L.nqs * 4;  // per warp and query: kept rows
+  o += warps * nq * 4;  // per warp and query: kept rows
+  L.off_len = o;
+  o += nq * 4;  // per query: rows queued
   L.off_bar = o = align_up(o, 8);
   o += 8 * S;
   L.off_ctr = o;
-  o += 4 * 8;  // qctr[2], lcnt[2], cctr[2]
+  o += 6 * 4;  // qctr[2], tiles issued, producers done, producer error, consumer error
   L.off_order = o;
   o += nq;
   L.off_chain = o = align_up(o, 16);
   o += align_up(nchain * 2, 16);
-  L.off_list = o;
-  o += BL_CAP * 4;
-  L.off_wq = o;
-  o += warps * BWQ * 4;
+  L.off_qbuf = o;
+  o += nq * BQQ * 4;
+  L.off_jobs = o = align_up(o, 16);
+  o += BJ * (uint32_t)sizeof(Job);
   L.off_stage = o = align_up(o, 128);
   o += S * nu * T * 4;
   L.total = o;
@@ -86,8 +95,8 @@ __host__ __device__ inline BLayout blayout(uint32_t nq, uint32_t nchain, uint32_
 }
 
 struct BParams {
-  uint64_t nrows, nwords, stride;
-  uint32_t nq, nu, nsrc, nchain, pf_mask, S;
+  uint64_t nrows, nwords;
+  uint32_t nq, nu, urow0, nsrc, nchain, pf_mask, S, np;  // np: producer warps
   BLayout L;
 };
 
@@ -97,8 +106,9 @@ struct BCtx {
   const unsigned long long *scol, *sfk;
   const uint32_t *sdim;
   unsigned long long *out;
-  unsigned long long *wsum;  // this warp's 1-group sums, per query
-  uint32_t *wcnt;            // this warp's kept rows, per query
+  unsigned long long *usum;  // this warp's 1-group sums, per query
+  uint32_t *ucnt;            // this warp's kept rows, per query
+  Job *jobs;
 };
 
 // Value of a 1-, 2- or 4-byte element without a branch on the width: the
@@ -112,134 +122,317 @@ __device__ __forceinline__ uint32_t b_ldw(const void *col, uint32_t i, uint32_t 
   return (word >> sh) & mask;
 }
 
-// One row's share of the op: everything per lane (the row's own query).
-struct BRow {
-  bool ok, chk;
-  uint32_t q, row;
-  const uint32_t *d;
-};
-
-// Runs the ops of the first n (<= 64) entries of ents, two rows per lane;
-// each lane reads its own row's query descriptor.  Accumulates 1-group sums
-// and kept rows into the warp's own slots (plain adds by one leader lane per
-// query), group sums by warp-aggregated global atomics.  All 32 lanes call it.
-__device__ __forceinline__ void b_drain(const BCtx &C, const uint32_t *ents, uint32_t n, uint32_t row0) {
+// Runs query q's op on the first n (<= 64) entries of qe (row | uncertain
+// << 31), two rows per lane, and accumulates them: 1-group sums and kept
+// rows into the query's slots (its warp's alone while it holds the query),
+// group sums by warp-aggregated global atomics.  q is warp-uniform: descriptor reads are broadcasts, branches on
+// the descriptor uniform, and the slots unrolled, so no value is picked by
+// a run-time index.  All 32 lanes call it.
+__device__ __forceinline__ void b_drain(const BCtx &C, uint32_t q, const uint32_t *qe, uint32_t n) {
   const uint32_t lane = threadIdx.x & 31;
-  BRow R[2];
+  const uint32_t *d = C.Qd + q * BQD_WORDS;
+  const uint32_t h0 = d[0], roles = d[5];
+  const uint32_t nslot = h0 & 0xffu, kv = roles & 0xffu, filt = (roles >> 8) & 0xffu, keym = (roles >> 16) & 0xffu,
+                 termm = roles >> 24;
+  const bool ok0 = lane < n, ok1 = lane + 32 < n;
+  const uint32_t e0 = ok0 ? qe[lane] : 0u, e1 = ok1 ? qe[lane + 32] : 0u;
+  const bool c0 = ok0 && (e0 >> 31), c1 = ok1 && (e1 >> 31);
+  const uint32_t r0 = e0 & 0x7fffffffu, r1 = e1 & 0x7fffffffu;
+  uint32_t v0[BSLOT], v1[BSLOT], bad0 = 0, bad1 = 0;
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const uint32_t i = lane + 32 * h;
-    R[h].ok = i < n;
-    const uint32_t e = R[h].ok ? ents[i] : 0u;
-    R[h].q = e & 0x7fu;
-    R[h].chk = R[h].ok && ((e >> 7) & 1u);
-    R[h].row = row0 + (e >> 8);
-    R[h].d = C.Qd + R[h].q * BQD_WORDS;
-  }
-  // loads: foreign keys, then values, of every slot of both rows
-  uint32_t key[2][BSLOT], v[2][BSLOT], bad[2] = {0, 0};
-  bool ld[2][BSLOT];
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const uint32_t h0 = R[h].d[0], roles = R[h].d[5];
-    const uint32_t nslot = h0 & 0xffu, kv = roles & 0xffu, filt = (roles >> 8) & 0xffu;
-#pragma unroll
-    for (uint32_t s = 0; s < BSLOT; ++s) {
-      key[h][s] = R[h].row;
-      ld[h][s] = R[h].ok && s < nslot && (((kv >> s) & 1u) || (R[h].chk && ((filt >> s) & 1u)));
-      if (ld[h][s]) {
-        const uint32_t t = R[h].d[BQD_SLOT0 + BQD_SLOTW * s] & 0xffu;
-        const uint32_t *fk = reinterpret_cast<const uint32_t *>(C.sfk[t]);
-        if (fk) key[h][s] = __ldg(fk + R[h].row);
-      }
-    }
-  }
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-#pragma unroll
-    for (uint32_t s = 0; s < BSLOT; ++s) {
-      v[h][s] = 0;
-      if (ld[h][s]) {
-        const uint32_t a = R[h].d[BQD_SLOT0 + BQD_SLOTW * s], t = a & 0xffu, w = (a >> 8) & 0xffu;
+  for (uint32_t s = 0; s < BSLOT; ++s) {
+    v0[s] = v1[s] = 0;
+    if (s < nslot) {
+      const uint32_t a = d[BQD_SLOT0 + BQD_SLOTW * s], t = a & 0xffu, w = (a >> 8) & 0xffu;
+      const bool kvs = (kv >> s) & 1u, fs = (filt >> s) & 1u;
+      bool l0 = ok0 && (kvs || (c0 && fs)), l1 = ok1 && (kvs || (c1 && fs));
+      uint32_t k0 = r0, k1 = r1;
+      const uint32_t *fk = reinterpret_cast<const uint32_t *>(C.sfk[t]);
+      if (fk) {
+        if (l0) k0 = __ldg(fk + r0);
+        if (l1) k1 = __ldg(fk + r1);
         const uint32_t dz = C.sdim[t];
-        if (C.sfk[t] && dz && key[h][s] >= dz) bad[h] |= 1u << s;
-        else v[h][s] = b_ldw(reinterpret_cast<const void *>(C.scol[t]), key[h][s], w);
+        if (dz) {
+          if (l0 && k0 >= dz) bad0 |= 1u << s, l0 = false;
+          if (l1 && k1 >= dz) bad1 |= 1u << s, l1 = false;
+        }
       }
+      const void *col = reinterpret_cast<const void *>(C.scol[t]);
+      if (l0) v0[s] = b_ldw(col, k0, w);
+      if (l1) v1[s] = b_ldw(col, k1, w);
     }
   }
-  bool keep[2], scal[2];
-  uint32_t slot[2];
-  uint64_t val[2];
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const uint32_t *d = R[h].d;
-    const uint32_t h0 = d[0], roles = d[5];
-    const uint32_t keym = (roles >> 16) & 0xffu, termm = roles >> 24;
-    bool kp = R[h].ok;
-    // candidate check of an uncertain row: the single-term clauses, bounds
-    // intersected per slot
-    if (R[h].chk) {
-#pragma unroll
-      for (uint32_t s = 0; s < BSLOT; ++s)
-        if ((termm >> s) & 1u) {
-          const uint32_t lo = d[BQD_SLOT0 + BQD_SLOTW * s + 1], hi = d[BQD_SLOT0 + BQD_SLOTW * s + 2];
-          kp = kp && !((bad[h] >> s) & 1u) && v[h][s] >= lo && v[h][s] <= hi;
-        }
-    }
-    // group key: sum over key slots of mul * (xform(value) - base); the
-    // transforms are computed branch-free and selected
-    uint32_t g = 0;
+  bool keep0 = ok0, keep1 = ok1;
+  // candidate check of uncertain rows: the single-term clauses, bounds
+  // intersected per slot
+  if (termm && __any_sync(0xffffffffu, c0 || c1)) {
 #pragma unroll
     for (uint32_t s = 0; s < BSLOT; ++s)
-      if ((keym >> s) & 1u) {
-        const uint32_t *sl = d + BQD_SLOT0 + BQD_SLOTW * s;
-        const uint32_t a = sl[0], xf = (a >> 16) & 0xffu, x = v[h][s];
-        kp = kp && !((bad[h] >> s) & 1u);
-        const uint32_t xd = div_by_magic(x, sl[3], (a >> 24) & 15u, a >> 28), xy = date_to_year(x);
-        const uint32_t xx = xf == MB_X_DIV ? xd : (xf == MB_X_YEAR ? xy : x);
-        g += sl[5] * (xx - sl[4]);
+      if ((termm >> s) & 1u) {
+        const uint32_t lo = d[BQD_SLOT0 + BQD_SLOTW * s + 1], hi = d[BQD_SLOT0 + BQD_SLOTW * s + 2];
+        keep0 = keep0 && (!c0 || (!((bad0 >> s) & 1u) && v0[s] >= lo && v0[s] <= hi));
+        keep1 = keep1 && (!c1 || (!((bad1 >> s) & 1u) && v1[s] >= lo && v1[s] <= hi));
       }
-    kp = kp && g < d[1];
-    const uint32_t vkind = (h0 >> 16) & 15u, va = (h0 >> 20) & 15u, vb = (h0 >> 24) & 15u;
-    uint64_t x = 1;
-    if (vkind != MB_V_ONE) {
-      uint64_t av = 0, bv = 0;
+  }
+  // group key: sum over key slots of mul * (xform(value) - base)
+  uint32_t g0 = 0, g1 = 0;
 #pragma unroll
-      for (uint32_t s = 0; s < BSLOT; ++s) {
-        if (s == va) av = v[h][s];
-        if (s == vb) bv = v[h][s];
+  for (uint32_t s = 0; s < BSLOT; ++s)
+    if ((keym >> s) & 1u) {
+      const uint32_t *sl = d + BQD_SLOT0 + BQD_SLOTW * s;
+      const uint32_t a = sl[0], xf = (a >> 16) & 0xffu;
+      keep0 = keep0 && !((bad0 >> s) & 1u);
+      keep1 = keep1 && !((bad1 >> s) & 1u);
+      uint32_t x0 = v0[s], x1 = v1[s];
+      if (xf == MB_X_DIV) {
+        const uint32_t m = sl[3], sh1 = (a >> 24) & 15u, sh2 = a >> 28;
+        x0 = div_by_magic(x0, m, sh1, sh2);
+        x1 = div_by_magic(x1, m, sh1, sh2);
+      } else if (xf == MB_X_YEAR) {
+        x0 = date_to_year(x0);
+        x1 = date_to_year(x1);
       }
-      kp = kp && !((bad[h] >> va) & 1u);
-      if (vkind == MB_V_COL) {
-        x = av;
-      } else {
-        kp = kp && !((bad[h] >> vb) & 1u);
-        x = vkind == MB_V_MUL ? av * bv : (uint64_t)((int64_t)av - (int64_t)bv);
+      const uint32_t base = sl[4], mul = sl[5];
+      g0 += mul * (x0 - base);
+      g1 += mul * (x1 - base);
+    }
+  const uint32_t ng = d[1];
+  keep0 = keep0 && g0 < ng;
+  keep1 = keep1 && g1 < ng;
+  // value
+  const uint32_t vkind = (h0 >> 16) & 15u, va = (h0 >> 20) & 15u, vb = (h0 >> 24) & 15u;
+  uint64_t x0 = 1, x1 = 1;
+  if (vkind != MB_V_ONE) {
+    uint64_t a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+#pragma unroll
+    for (uint32_t s = 0; s < BSLOT; ++s) {
+      if (s == va) a0 = v0[s], a1 = v1[s];
+      if (s == vb) b0 = v0[s], b1 = v1[s];
+    }
+    keep0 = keep0 && !((bad0 >> va) & 1u);
+    keep1 = keep1 && !((bad1 >> va) & 1u);
+    if (vkind == MB_V_COL) {
+      x0 = a0, x1 = a1;
+    } else {
+      keep0 = keep0 && !((bad0 >> vb) & 1u);
+      keep1 = keep1 && !((bad1 >> vb) & 1u);
+      x0 = vkind == MB_V_MUL ? a0 * b0 : (uint64_t)((int64_t)a0 - (int64_t)b0);
+      x1 = vkind == MB_V_MUL ? a1 * b1 : (uint64_t)((int64_t)a1 - (int64_t)b1);
+    }
+  }
+  const uint32_t kept = __popc(__ballot_sync(0xffffffffu, keep0)) + __popc(__ballot_sync(0xffffffffu, keep1));
+  if ((h0 >> 8) & 1u) {  // one group: a warp sum into the warp's slot
+    const uint64_t s = peer_sum64(0xffffffffu, (keep0 ? x0 : 0) + (keep1 ? x1 : 0));
+    if (lane == 0) C.usum[q] += s;
+  } else {
+    const uint32_t base = d[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && n <= 32) break;
+      const bool kp = h ? keep1 : keep0;
+      const uint32_t g = h ? g1 : g0;
+      const uint32_t peers = __match_any_sync(0xffffffffu, kp ? g : 0xffffffffu);
+      if (kp) {
+        const uint64_t s = peer_sum64(peers, h ? x1 : x0);
+        if (lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&C.out[base + g], (unsigned long long)s);
       }
     }
-    keep[h] = kp;
-    val[h] = x;
-    scal[h] = (h0 >> 8) & 1u;
-    slot[h] = d[2] + g;
   }
-  // aggregation: peers share a 1-group query (summed into the warp's slot)
-  // or an output slot (global atomics); rows are counted per query
+  if (lane == 0) C.ucnt[q] += kept;
+  __syncwarp();
+}
+
+// b_drain for a compiled shape SH (BSHAPES): the slots, their roles and the
+// key transforms are known at compile time; only the columns, bounds and key
+// constants are read from the descriptor.  Same results as b_drain.
+template <int SH>
+__device__ __forceinline__ void b_drain_s(const BCtx &C, uint32_t q, const uint32_t *qe, uint32_t n) {
+  constexpr BShape sh = BSHAPES[SH];
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t *d = C.Qd + q * BQD_WORDS;
+  const bool ok0 = lane < n, ok1 = lane + 32 < n;
+  const uint32_t e0 = ok0 ? qe[lane] : 0u, e1 = ok1 ? qe[lane + 32] : 0u;
+  const bool c0 = ok0 && (e0 >> 31), c1 = ok1 && (e1 >> 31);
+  const uint32_t r0 = e0 & 0x7fffffffu, r1 = e1 & 0x7fffffffu;
+  uint32_t v0[BSLOT], v1[BSLOT], bad0 = 0, bad1 = 0;
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    if (h == 1 && n <= 32) break;
-    const uint32_t key2 = keep[h] ? (scal[h] ? (0x80000000u | R[h].q) : slot[h]) : 0xffffffffu;
-    const uint32_t peers = __match_any_sync(0xffffffffu, key2);
-    if (keep[h]) {
-      const uint64_t s = peer_sum64(peers, val[h]);
-      if (lane == (uint32_t)(__ffs(peers) - 1)) {
-        if (scal[h]) C.wsum[R[h].q] += s;
-        else atomicAdd(&C.out[slot[h]], (unsigned long long)s);
+  for (uint32_t s = 0; s < BSLOT; ++s) {
+    v0[s] = v1[s] = 0;
+    if (s < sh.ns && (((sh.kv | sh.filt) >> s) & 1u)) {
+      const bool kvs = (sh.kv >> s) & 1u;
+      const uint32_t a = d[BQD_SLOT0 + BQD_SLOTW * s], t = a & 0xffu, w = (a >> 8) & 0xffu;
+      bool l0 = ok0 && (kvs || c0), l1 = ok1 && (kvs || c1);
+      uint32_t k0 = r0, k1 = r1;
+      const uint32_t *fk = reinterpret_cast<const uint32_t *>(C.sfk[t]);
+      if (fk) {
+        if (l0) k0 = __ldg(fk + r0);
+        if (l1) k1 = __ldg(fk + r1);
+        const uint32_t dz = C.sdim[t];
+        if (dz) {
+          if (l0 && k0 >= dz) bad0 |= 1u << s, l0 = false;
+          if (l1 && k1 >= dz) bad1 |= 1u << s, l1 = false;
+        }
+      }
+      const void *col = reinterpret_cast<const void *>(C.scol[t]);
+      if (l0) v0[s] = b_ldw(col, k0, w);
+      if (l1) v1[s] = b_ldw(col, k1, w);
+    }
+  }
+  bool keep0 = ok0, keep1 = ok1;
+  if (sh.filt && __any_sync(0xffffffffu, c0 || c1)) {
+#pragma unroll
+    for (uint32_t s = 0; s < BSLOT; ++s)
+      if ((sh.filt >> s) & 1u) {
+        const uint32_t lo = d[BQD_SLOT0 + BQD_SLOTW * s + 1], hi = d[BQD_SLOT0 + BQD_SLOTW * s + 2];
+        keep0 = keep0 && (!c0 || (!((bad0 >> s) & 1u) && v0[s] >= lo && v0[s] <= hi));
+        keep1 = keep1 && (!c1 || (!((bad1 >> s) & 1u) && v1[s] >= lo && v1[s] <= hi));
+      }
+  }
+  uint32_t g0 = 0, g1 = 0;
+#pragma unroll
+  for (uint32_t s = 0; s < BSLOT; ++s)
+    if ((sh.keym >> s) & 1u) {
+      const uint32_t *sl = d + BQD_SLOT0 + BQD_SLOTW * s;
+      keep0 = keep0 && !((bad0 >> s) & 1u);
+      keep1 = keep1 && !((bad1 >> s) & 1u);
+      uint32_t x0 = v0[s], x1 = v1[s];
+      constexpr uint32_t XDIV = 1, XYEAR = 2;
+      const uint32_t xf = (sh.xf >> (2 * s)) & 3u;
+      if (xf == XDIV) {
+        const uint32_t a = sl[0], m = sl[3], sh1 = (a >> 24) & 15u, sh2 = a >> 28;
+        x0 = div_by_magic(x0, m, sh1, sh2);
+        x1 = div_by_magic(x1, m, sh1, sh2);
+      } else if (xf == XYEAR) {
+        x0 = date_to_year(x0);
+        x1 = date_to_year(x1);
+      }
+      const uint32_t base = sl[4], mul = sl[5];
+      g0 += mul * (x0 - base);
+      g1 += mul * (x1 - base);
+    }
+  const uint32_t ng = d[1];
+  keep0 = keep0 && g0 < ng;
+  keep1 = keep1 && g1 < ng;
+  uint64_t x0 = 1, x1 = 1;
+  if (sh.vk != MB_V_ONE) {
+    keep0 = keep0 && !((bad0 >> sh.va) & 1u);
+    keep1 = keep1 && !((bad1 >> sh.va) & 1u);
+    const uint64_t a0 = v0[sh.va], a1 = v1[sh.va];
+    if (sh.vk == MB_V_COL) {
+      x0 = a0, x1 = a1;
+    } else {
+      keep0 = keep0 && !((bad0 >> sh.vb) & 1u);
+      keep1 = keep1 && !((bad1 >> sh.vb) & 1u);
+      const uint64_t b0 = v0[sh.vb], b1 = v1[sh.vb];
+      x0 = sh.vk == MB_V_MUL ? a0 * b0 : (uint64_t)((int64_t)a0 - (int64_t)b0);
+      x1 = sh.vk == MB_V_MUL ? a1 * b1 : (uint64_t)((int64_t)a1 - (int64_t)b1);
+    }
+  }
+  const uint32_t kept = __popc(__ballot_sync(0xffffffffu, keep0)) + __popc(__ballot_sync(0xffffffffu, keep1));
+  if ((d[0] >> 8) & 1u) {  // one group: a warp sum into the query's slot
+    const uint64_t s = peer_sum64(0xffffffffu, (keep0 ? x0 : 0) + (keep1 ? x1 : 0));
+    if (lane == 0) C.usum[q] += s;
+  } else {
+    const uint32_t base = d[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && n <= 32) break;
+      const bool kp = h ? keep1 : keep0;
+      const uint32_t g = h ? g1 : g0;
+      const uint32_t peers = __match_any_sync(0xffffffffu, kp ? g : 0xffffffffu);
+      if (kp) {
+        const uint64_t s = peer_sum64(peers, h ? x1 : x0);
+        if (lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&C.out[base + g], (unsigned long long)s);
       }
     }
-    const uint32_t qpeers = __match_any_sync(0xffffffffu, keep[h] ? R[h].q : 0xffffffffu);
-    if (keep[h] && lane == (uint32_t)(__ffs(qpeers) - 1)) C.wcnt[R[h].q] += __popc(qpeers);
-    __syncwarp();
   }
+  if (lane == 0) C.ucnt[q] += kept;
+  __syncwarp();
+}
+
+// The drain for query q: its compiled shape, or the generic one.  One
+// out-of-line copy serves every call site.
+__device__ __noinline__ void b_drain_any(const BCtx C, uint32_t q, const uint32_t *qe, uint32_t n) {
+  switch (C.Qd[q * BQD_WORDS + 6]) {
+  case 1: b_drain_s<0>(C, q, qe, n); break;
+  case 2: b_drain_s<1>(C, q, qe, n); break;
+  case 3: b_drain_s<2>(C, q, qe, n); break;
+  case 4: b_drain_s<3>(C, q, qe, n); break;
+  case 5: b_drain_s<4>(C, q, qe, n); break;
+  case 6: b_drain_s<5>(C, q, qe, n); break;
+  case 7: b_drain_s<6>(C, q, qe, n); break;
+  case 8: b_drain_s<7>(C, q, qe, n); break;
+  default: b_drain(C, q, qe, n); break;
+  }
+}
+
+// Posts the n (<= 64) rows at qe of query q as a job; false if every slot
+// is taken (the caller drains them itself).  Warp-collective.
+__device__ __forceinline__ bool job_post(const BCtx &C, uint32_t q, const uint32_t *qe, uint32_t n) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t slot = 0xffffffffu;
+  for (uint32_t base = 0; base < BJ && slot == 0xffffffffu; base += 32) {
+    const uint32_t st = *(volatile uint32_t *)&C.jobs[base + lane].state;
+    uint32_t freem = __ballot_sync(0xffffffffu, st == JOB_FREE);
+    if (lane == 0)
+      while (freem) {
+        const uint32_t j = base + __ffs(freem) - 1;
+        freem &= freem - 1;
+        if (atomicCAS(&C.jobs[j].state, JOB_FREE, JOB_FILL) == JOB_FREE) {
+          slot = j;
+          break;
+        }
+      }
+    slot = __shfl_sync(0xffffffffu, slot, 0);
+  }
+  if (slot == 0xffffffffu) return false;
+  Job &J = C.jobs[slot];
+  if (lane < n) J.rows[lane] = qe[lane];
+  if (lane + 32 < n) J.rows[lane + 32] = qe[lane + 32];
+  if (lane == 0) J.q = q, J.n = n;
+  __syncwarp();
+  if (lane == 0) {
+    __threadfence_block();
+    atomicExch(&J.state, JOB_READY);
+  }
+  __syncwarp();
+  return true;
+}
+
+__device__ __noinline__ void b_drain_any(const BCtx C, uint32_t q, const uint32_t *qe, uint32_t n);
+
+// Runs one posted job, if there is one; returns whether it did.
+// Warp-collective.
+__device__ __forceinline__ bool job_run(const BCtx &C) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t slot = 0xffffffffu;
+  for (uint32_t base = 0; base < BJ && slot == 0xffffffffu; base += 32) {
+    const uint32_t st = *(volatile uint32_t *)&C.jobs[base + lane].state;
+    uint32_t readym = __ballot_sync(0xffffffffu, st == JOB_READY);
+    if (lane == 0) {
+      while (readym) {
+        const uint32_t j = base + __ffs(readym) - 1;
+        readym &= readym - 1;
+        if (atomicCAS(&C.jobs[j].state, JOB_READY, JOB_RUN) == JOB_READY) {
+          slot = j;
+          break;
+        }
+      }
+      __threadfence_block();
+    }
+    slot = __shfl_sync(0xffffffffu, slot, 0);
+  }
+  __syncwarp();
+  if (slot == 0xffffffffu) return false;
+  Job &J = C.jobs[slot];
+  b_drain_any(C, J.q, J.rows, J.n);
+  __syncwarp();
+  if (lane == 0) {
+    __threadfence_block();
+    atomicExch(&J.state, JOB_FREE);
+  }
+  __syncwarp();
+  return true;
 }
 
 template <int V>
@@ -255,52 +448,68 @@ __device__ __forceinline__ void lds_words(const uint32_t *p, uint32_t (&x)[V]) {
   }
 }
 
-// Phase A for query q on the staged tile (words w0 + lane*V + k of the
-// table; word lane*V + k of the stage): the conjunctive chain, then the
-// selected rows appended to the tile list (or, if they do not fit, run
-// through the warp's own queue).
+// Query q on the staged tile (words w0 + lane*V + k of the table; word
+// lane*V + k of the stage): the conjunctive chain, then the selected rows
+// into the query's queue; every 64 become a job.
 template <int V>
 __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, const uint32_t *stage, uint64_t w0,
-                                        uint64_t nwords, uint32_t tail, uint32_t q, uint32_t *list, uint32_t *lcnt,
-                                        uint32_t *wq) {
+                                        uint64_t nwords, uint32_t tail, uint32_t urow0, uint32_t q, uint32_t *queue,
+                                        uint32_t *qlen) {
   constexpr uint32_t T = 32 * V;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t ch = C.Qd[q * BQD_WORDS + 4], c0 = ch & 0xffffu, nc = ch >> 16;
-  uint32_t acc[V], cur[V], ce[V], unc[V];
+  // the chain: per conjunct a header (middle bins | edge bins << 8 | negated
+  // << 15) and the union indices of its middle bins, then of its edge bins
+  uint32_t acc[V], unc[V];
 #pragma unroll
-  for (int k = 0; k < V; ++k) acc[k] = 0xffffffffu, cur[k] = ce[k] = unc[k] = 0;
+  for (int k = 0; k < V; ++k) acc[k] = 0xffffffffu, unc[k] = 0;
   const uint32_t *sl = stage + lane * V;
-  for (uint32_t i = 0; i < nc; ++i) {
-    const uint32_t e = chain[c0 + i];
-    uint32_t x[V];
-    lds_words<V>(sl + (e & 0xffu) * T, x);
-    const uint32_t em = (e & (CNF_EDGE << 8)) ? 0xffffffffu : 0u;
+  for (uint32_t i = 0; i < nc;) {
+    const uint32_t hd = chain[c0 + i++];
+    const uint32_t nm = hd & 0xffu, ne = (hd >> 8) & 0x7fu;
+    uint32_t cm[V], cx[V];
 #pragma unroll
-    for (int k = 0; k < V; ++k) {
-      cur[k] |= x[k];
-      ce[k] |= x[k] & em;
+    for (int k = 0; k < V; ++k) cm[k] = cx[k] = 0;
+    for (uint32_t j = 0; j < nm; ++j) {
+      uint32_t x[V];
+      lds_words<V>(sl + (chain[c0 + i++] - urow0) * T, x);
+#pragma unroll
+      for (int k = 0; k < V; ++k) cm[k] |= x[k];
     }
-    if (e & (CNF_END << 8)) {
-      const bool neg = (e & (CNF_NEG << 8)) != 0;
+    for (uint32_t j = 0; j < ne; ++j) {
+      uint32_t x[V];
+      lds_words<V>(sl + (chain[c0 + i++] - urow0) * T, x);
 #pragma unroll
-      for (int k = 0; k < V; ++k) {
-        acc[k] &= neg ? ~cur[k] : cur[k];
-        if (!neg) unc[k] |= ce[k];
-        cur[k] = ce[k] = 0;
-      }
+      for (int k = 0; k < V; ++k) cx[k] |= x[k];
+    }
+    if (hd >> 15) {
+#pragma unroll
+      for (int k = 0; k < V; ++k) acc[k] &= ~(cm[k] | cx[k]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < V; ++k) acc[k] &= cm[k] | cx[k], unc[k] |= cx[k];
     }
   }
   uint32_t p[V], u[V], pc = 0;
+  if (w0 + T <= nwords && (tail == 0 || w0 + T < nwords)) {  // an interior tile: no mask
 #pragma unroll
-  for (int k = 0; k < V; ++k) {
-    const uint64_t w = w0 + lane * V + k;
-    uint32_t m = w < nwords ? 0xffffffffu : 0u;
-    if (tail && w + 1 == nwords) m = (1u << tail) - 1u;
-    p[k] = acc[k] & m;
-    u[k] = unc[k] & p[k];
-    pc += __popc(p[k]);
+    for (int k = 0; k < V; ++k) p[k] = acc[k], u[k] = unc[k] & acc[k], pc += __popc(p[k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      const uint64_t w = w0 + lane * V + k;
+      uint32_t m = w < nwords ? 0xffffffffu : 0u;
+      if (tail && w + 1 == nwords) m = (1u << tail) - 1u;
+      p[k] = acc[k] & m;
+      u[k] = unc[k] & p[k];
+      pc += __popc(p[k]);
+    }
   }
-  // exclusive prefix of the lanes' row counts
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t rowbase = (uint32_t)((w0 + lane * V) * 32);  // first row of the lane's words
+  uint32_t qn = *qlen;
+  // fast path: every selected row fits the queue at once (a prefix sum of
+  // the lanes' counts places them)
   uint32_t incl = pc;
 #pragma unroll
   for (int dd = 1; dd < 32; dd <<= 1) {
@@ -308,36 +517,27 @@ __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, co
     if (lane >= (uint32_t)dd) incl += y;
   }
   const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-  if (total == 0) return;
-  uint32_t base = 0;
-  if (lane == 0) {
-    // a reservation that would pass the end is taken back; while it is out,
-    // every other reservation fails too, so the granted runs stay contiguous
-    base = atomicAdd(lcnt, total);
-    if (base + total > BL_CAP) {
-      atomicSub(lcnt, total);
-      base = 0xffffffffu;
-    }
-  }
-  base = __shfl_sync(0xffffffffu, base, 0);
-  const uint32_t lrow = lane * V * 32;  // first row of the lane's words within the tile
-  if (base != 0xffffffffu) {
-    uint32_t pos = base + incl - pc;
+  if (qn + total <= BQQ) {
+    uint32_t pos = qn + incl - pc;
 #pragma unroll
     for (int k = 0; k < V; ++k) {
       uint32_t m = p[k];
       while (m) {
         const uint32_t b = __ffs(m) - 1;
         m &= m - 1;
-        list[pos++] = ((lrow + k * 32 + b) << 8) | (((u[k] >> b) & 1u) << 7) | q;
+        queue[pos++] = (rowbase + k * 32 + b) | (((u[k] >> b) & 1u) << 31);
       }
     }
+    qn += total;
+    __syncwarp();
+    if (qn >= 64) {
+      qn -= 64;
+      if (!job_post(C, q, queue + qn, 64)) b_drain_any(C, q, queue + qn, 64);
+    }
+    if (lane == 0) *qlen = qn;
     return;
   }
-  // the list is full: the rows through the warp's queue, one per lane per round
-  const uint32_t lt = (1u << lane) - 1u;
-  const uint32_t row0 = (uint32_t)(w0 * 32);
-  uint32_t qn = 0;
+  // otherwise one row per lane per round, draining every 64
   while (true) {
     bool has = false;
     uint32_t e = 0;
@@ -347,28 +547,27 @@ __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, co
         const uint32_t b = __ffs(p[k]) - 1;
         p[k] &= p[k] - 1;
         has = true;
-        e = ((lrow + k * 32 + b) << 8) | (((u[k] >> b) & 1u) << 7) | q;
+        e = (rowbase + k * 32 + b) | (((u[k] >> b) & 1u) << 31);
       }
     }
     const uint32_t bal = __ballot_sync(0xffffffffu, has);
     if (!bal) break;
-    if (has) wq[qn + __popc(bal & lt)] = e;
+    if (has) queue[qn + __popc(bal & lt)] = e;
     qn += __popc(bal);
     if (qn >= 64) {
       __syncwarp();
       qn -= 64;
-      b_drain(C, wq + qn, 64, row0);
-      __syncwarp();
+      if (!job_post(C, q, queue + qn, 64)) b_drain_any(C, q, queue + qn, 64);
     }
   }
   __syncwarp();
-  if (qn) b_drain(C, wq, qn, row0);
-  __syncwarp();
+  if (lane == 0) *qlen = qn;
 }
 
 template <int V>
-__global__ void __launch_bounds__(BT_THREADS_MAX)
-batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParams P, unsigned long long *__restrict__ out,
+__global__ void __launch_bounds__(BT_THREADS_MAX, 1)
+batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParams P,
+                  const __grid_constant__ CUtensorMap tmap, unsigned long long *__restrict__ out,
                   unsigned long long *__restrict__ nqual, uint32_t *errw) {
   constexpr uint32_t T = 32 * V;
   extern __shared__ __align__(128) uint8_t smem[];
@@ -378,22 +577,25 @@ batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParam
   unsigned long long *scol = reinterpret_cast<unsigned long long *>(smem + L.off_src);
   unsigned long long *sfk = scol + BS_MAX;
   uint32_t *sdim = reinterpret_cast<uint32_t *>(sfk + BS_MAX), *swid = sdim + BS_MAX;
-  const uint32_t **ubmp = reinterpret_cast<const uint32_t **>(smem + L.off_ubmp);
-  unsigned long long *usum = reinterpret_cast<unsigned long long *>(smem + L.off_sum);  // [warp][nqs]
-  uint32_t *ucnt = reinterpret_cast<uint32_t *>(smem + L.off_cnt);                      // [warp][nqs]
+  unsigned long long *usum = reinterpret_cast<unsigned long long *>(smem + L.off_sum);
+  uint32_t *ucnt = reinterpret_cast<uint32_t *>(smem + L.off_cnt);
+  uint32_t *qlen = reinterpret_cast<uint32_t *>(smem + L.off_len);
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + L.off_bar);
-  uint32_t *qctr = reinterpret_cast<uint32_t *>(smem + L.off_ctr), *lcnt = qctr + 2, *cctr = qctr + 4;
+  uint32_t *qctr = reinterpret_cast<uint32_t *>(smem + L.off_ctr), *issued = qctr + 2, *pdone = qctr + 3,
+           *perr = qctr + 4, *cerr = qctr + 5;
   uint8_t *order = smem + L.off_order;
   uint16_t *chain = reinterpret_cast<uint16_t *>(smem + L.off_chain);
-  uint32_t *list = reinterpret_cast<uint32_t *>(smem + L.off_list);
-  uint32_t *wq = reinterpret_cast<uint32_t *>(smem + L.off_wq) + (size_t)warp * BWQ;
+  uint32_t *qbuf = reinterpret_cast<uint32_t *>(smem + L.off_qbuf);
+  Job *jobs = reinterpret_cast<Job *>(smem + L.off_jobs);
   uint32_t *stages = reinterpret_cast<uint32_t *>(smem + L.off_stage);
+  const uint32_t np = P.np;  // warps 0 .. np-1 produce, the others consume
 
   for (uint32_t i = tid; i < P.nq * BQD_WORDS; i += blockDim.x) Qd[i] = H->Qd[i];
+  for (uint32_t i = tid; i < BJ; i += blockDim.x) jobs[i].state = JOB_FREE;
+  for (uint32_t i = tid; i < nw * P.nq; i += blockDim.x) usum[i] = 0, ucnt[i] = 0;
   for (uint32_t i = tid; i < P.nchain; i += blockDim.x) chain[i] = H->chain[i];
-  for (uint32_t i = tid; i < P.nu; i += blockDim.x) ubmp[i] = H->ubmp[i];
   for (uint32_t i = tid; i < P.nq; i += blockDim.x) order[i] = H->order[i];
-  for (uint32_t i = tid; i < nw * L.nqs; i += blockDim.x) usum[i] = 0, ucnt[i] = 0;
+  for (uint32_t i = tid; i < P.nq; i += blockDim.x) qlen[i] = 0;
   if (tid < BS_MAX) {
     scol[tid] = reinterpret_cast<unsigned long long>(H->src[tid].col);
     sfk[tid] = reinterpret_cast<unsigned long long>(H->src[tid].fk);
@@ -402,7 +604,7 @@ batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParam
   }
   if (tid < 6) qctr[tid] = 0;
   if (tid == 0) {
-    for (uint32_t s = 0; s < P.S; ++s) mbar_init(&full[s], blockDim.x);
+    for (uint32_t s = 0; s < P.S; ++s) mbar_init(&full[s], 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -413,25 +615,24 @@ batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParam
   C.sfk = sfk;
   C.sdim = sdim;
   C.out = out;
-  C.wsum = usum + (size_t)warp * L.nqs;
-  C.wcnt = ucnt + (size_t)warp * L.nqs;
+  C.usum = usum + (size_t)warp * P.nq;
+  C.ucnt = ucnt + (size_t)warp * P.nq;
+  C.jobs = jobs;
 
   const uint64_t ntiles = (P.nwords + T - 1) / T;
   const uint64_t nit = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  // block-collective: stage j % S <- the CTA's j-th tile; every thread's
-  // copies complete one arrival on full[j % S]
+  // stage j % S <- the CTA's j-th tile: one tensor copy (thread 0) of rows
+  // [urow0, urow0 + nu) x T words, zeros past the table's end; the payload
+  // rows of the tile into L2 (threads < nsrc)
   auto fill = [&](uint64_t j) {
     const uint32_t s = (uint32_t)(j % P.S);
     const uint64_t w0 = ((uint64_t)blockIdx.x + j * gridDim.x) * T;
-    const uint64_t avail = P.stride - w0;  // a multiple of 32 words
-    const uint32_t cpb = (uint32_t)(avail < T ? avail : T) / 4;  // 16-byte chunks per bitmap
-    uint32_t *st = stages + (size_t)s * P.nu * T;
-    const uint32_t total = P.nu * cpb;
-    for (uint32_t i = tid; i < total; i += blockDim.x) {
-      const uint32_t u = i / cpb, c = i - u * cpb;
-      cp_async16(st + u * T + c * 4, ubmp[u] + w0 + c * 4);
+    if (tid == 0) {
+      ++*issued;
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&full[s], P.nu * T * 4);
+      tma_load_2d(stages + (size_t)s * P.nu * T, &tmap, (int)w0, (int)P.urow0, &full[s]);
     }
-    cp_async_mbar_arrive(&full[s]);
     if (tid < P.nsrc && ((P.pf_mask >> tid) & 1u)) {
       const uint64_t r0 = w0 * 32;
       if (r0 < P.nrows) {
@@ -444,55 +645,79 @@ batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParam
       }
     }
   };
-  for (uint64_t j = 0; j < P.S && j < nit; ++j) fill(j);
+  auto pbar = [&]() { asm volatile("bar.sync 1, %0;" ::"r"(np * 32) : "memory"); };  // producers only
 
-  bool err = false;
-  const uint32_t tail = (uint32_t)(P.nrows & 31u);
-  for (uint64_t it = 0; it < nit; ++it) {
-    const uint32_t s = (uint32_t)(it % P.S), par = (uint32_t)((it / P.S) & 1u), b = (uint32_t)(it & 1u);
-    const bool ok = mbar_wait_bounded(&full[s], par, errw, MB_DEVERR_TMA_WAIT);
-    if (!__syncthreads_and(ok ? 1 : 0)) {
-      err = true;
-      break;
+  if (warp < np) {
+    // ---------------------------------------------------------- producers
+    for (uint64_t j = 0; j < P.S && j < nit; ++j) fill(j);
+    const uint32_t tail = (uint32_t)(P.nrows & 31u);
+    for (uint64_t it = 0; it < nit; ++it) {
+      const uint32_t s = (uint32_t)(it % P.S), par = (uint32_t)((it / P.S) & 1u), b = (uint32_t)(it & 1u);
+      if (!mbar_wait_bounded(&full[s], par, errw, MB_DEVERR_TMA_WAIT)) atomicOr(perr, 1u);
+      pbar();
+      if (*(volatile uint32_t *)perr) break;
+      if (tid == 0) qctr[b ^ 1u] = 0;  // last used on the previous tile; next used after this tile's barrier
+      const uint64_t w0 = ((uint64_t)blockIdx.x + it * gridDim.x) * T;
+      const uint32_t *st = stages + (size_t)s * P.nu * T;
+      while (true) {
+        uint32_t qi = 0;
+        if (lane == 0) qi = atomicAdd(&qctr[b], 1u);
+        qi = __shfl_sync(0xffffffffu, qi, 0);
+        if (qi >= P.nq) break;
+        const uint32_t q = order[qi];
+        b_query<V>(C, chain, st, w0, P.nwords, tail, P.urow0, q, qbuf + (size_t)q * BQQ, &qlen[q]);
+      }
+      pbar();  // the stage is consumed: refill it
+      if (it + P.S < nit) fill(it + P.S);
     }
-    if (tid == 0) cctr[b] = 0;  // last used two tiles ago; next used after the barrier below
-    const uint64_t w0 = ((uint64_t)blockIdx.x + it * gridDim.x) * T;
-    const uint32_t *st = stages + (size_t)s * P.nu * T;
-    // phase A: the queries' chains into the tile row list
+    if (*(volatile uint32_t *)perr) {
+      // a wait ran out: let the copies still in flight land before exiting
+      if (tid == 0)
+        for (uint32_t j = *issued > P.S ? *issued - P.S : 0; j < *issued; ++j)
+          mbar_wait_bounded(&full[j % P.S], (j / P.S) & 1u, nullptr, 0, 1u << 16);
+    } else {
+      // every query's last rows become jobs
+      for (uint32_t q = warp; q < P.nq; q += np) {
+        const uint32_t n = qlen[q];
+        if (n && !job_post(C, q, qbuf + (size_t)q * BQQ, n)) b_drain_any(C, q, qbuf + (size_t)q * BQQ, n);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence_block();
+      atomicAdd(pdone, 1u);
+    }
+  } else {
+    // ---------------------------------------------------------- consumers
+    uint32_t idle = 0;
     while (true) {
-      uint32_t qi = 0;
-      if (lane == 0) qi = atomicAdd(&qctr[b], 1u);
-      qi = __shfl_sync(0xffffffffu, qi, 0);
-      if (qi >= P.nq) break;
-      b_query<V>(C, chain, st, w0, P.nwords, tail, order[qi], list, &lcnt[b], wq);
+      if (job_run(C)) {
+        idle = 0;
+        continue;
+      }
+      if (*(volatile uint32_t *)pdone == np) {
+        __threadfence_block();
+        if (!job_run(C)) break;  // nothing posted after the last producer finished
+        continue;
+      }
+      if (++idle >= CONSUMER_IDLE_TRIES) {
+        if (lane == 0) {
+          atomicOr(cerr, 1u);
+          if (atomicCAS(errw, 0u, 1u) == 0u) {
+            errw[1] = MB_DEVERR_IDLE_WAIT;
+            errw[2] = blockIdx.x;
+          }
+        }
+        break;
+      }
+      __nanosleep(128);
     }
-    __syncthreads();
-    // the stage is consumed: refill it; then the next tile's counters
-    if (it + P.S < nit) fill(it + P.S);
-    const uint32_t n = lcnt[b];
-    __syncthreads();  // every thread has read n before the next tile's counters are reset
-    if (tid == 0) qctr[b ^ 1u] = 0, lcnt[b ^ 1u] = 0;
-    // phase B: the ops over 64-entry chunks of the list
-    const uint32_t nch = (n + 63) / 64;
-    const uint32_t row0 = (uint32_t)(w0 * 32);
-    while (true) {
-      uint32_t c = 0;
-      if (lane == 0) c = atomicAdd(&cctr[b], 1u);
-      c = __shfl_sync(0xffffffffu, c, 0);
-      if (c >= nch) break;
-      b_drain(C, list + 64 * c, n - 64 * c < 64 ? n - 64 * c : 64, row0);
-    }
-    __syncthreads();  // the list is consumed
-  }
-  if (err) {
-    cp_async_wait_all();  // copies this thread issued land before the block exits
-    __syncthreads();
-    return;
   }
   __syncthreads();
+  if (*(volatile uint32_t *)perr || *(volatile uint32_t *)cerr) return;
   for (uint32_t q = tid; q < P.nq; q += blockDim.x) {
     unsigned long long sum = 0, cnt = 0;
-    for (uint32_t w = 0; w < nw; ++w) sum += usum[w * L.nqs + q], cnt += ucnt[w * L.nqs + q];
+    for (uint32_t w = 0; w < nw; ++w) sum += usum[w * P.nq + q], cnt += ucnt[w * P.nq + q];
     if (sum) atomicAdd(&out[Qd[q * BQD_WORDS + 2]], sum);
     if (cnt) atomicAdd(&nqual[Qd[q * BQD_WORDS + 3]], cnt);
   }
@@ -502,24 +727,50 @@ batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParam
 
 size_t batch_smem(const BatchHdr &h, const BatchCfg &c) {
   if (c.V != 1 && c.V != 2 && c.V != 4) return 0;
-  if (c.warps == 0 || c.warps > BW_MAX || c.stages == 0 || c.stages > 4) return 0;
+  if (c.warps < 2 || c.warps > BW_MAX || c.stages == 0 || c.stages > 4 || c.drainers == 0 || c.drainers >= c.warps)
+    return 0;
   return blayout(h.nq, h.nchain, h.nu, c.warps, c.stages, 32 * c.V).total;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+static mb_status encode_tmap(const BatchHdr &h, uint32_t T, CUtensorMap *map) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    MB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !fn) return fail(MB_ERR_CUDA, "batch: cuTensorMapEncodeTiled not found");
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t dim[2] = {h.stride, h.nslab};
+  const cuuint64_t gstride[1] = {h.stride * 4};
+  const cuuint32_t box[2] = {T, h.nu};
+  const cuuint32_t estride[2] = {1, 1};
+  const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<uint32_t *>(h.slab), dim, gstride, box,
+                            estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(MB_ERR_CUDA, "batch: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return MB_OK;
 }
 
 template <int V>
 static mb_status launch_bs(const BatchHdr &h, const BatchHdr *dh, const BatchCfg &c, int64_t *out, uint64_t *nqual,
                            cudaStream_t st) {
   auto kern = batch_scan_kernel<V>;
+  CUtensorMap tmap;
+  MB_CHECK(encode_tmap(h, 32 * V, &tmap));
   BParams P;
   P.nrows = h.nrows;
   P.nwords = h.nwords;
-  P.stride = h.stride;
   P.nq = h.nq;
   P.nu = h.nu;
+  P.urow0 = h.urow0;
   P.nsrc = h.nsrc;
   P.nchain = h.nchain;
   P.pf_mask = h.pf_mask;
   P.S = c.stages;
+  P.np = c.warps - c.drainers;
   P.L = blayout(h.nq, h.nchain, h.nu, c.warps, c.stages, 32 * V);
   const DevInfo &di = dev_info();
   const size_t smem = P.L.total;
@@ -534,7 +785,7 @@ static mb_status launch_bs(const BatchHdr &h, const BatchHdr *dh, const BatchCfg
   if (grid > ntiles) grid = ntiles;
   uint32_t *errw = device_error_word();
   if (!errw) return fail(MB_ERR_OOM, "batch: device error word");
-  kern<<<(unsigned)grid, c.warps * 32, smem, st>>>(dh, P, reinterpret_cast<unsigned long long *>(out),
+  kern<<<(unsigned)grid, c.warps * 32, smem, st>>>(dh, P, tmap, reinterpret_cast<unsigned long long *>(out),
                                                    reinterpret_cast<unsigned long long *>(nqual), errw);
   MB_LAUNCH_CHECK("batch_scan_kernel");
   return MB_OK;
@@ -545,8 +796,9 @@ mb_status batch_scan(const BatchHdr &h, const BatchHdr *dh, const BatchCfg &c, i
   if (h.nq == 0 || h.nrows == 0) return MB_OK;
   if (h.nq > BQ_MAX || h.nu > BU_MAX || h.nsrc > BS_MAX || h.nchain > BC_MAX)
     return fail(MB_ERR_INVALID, "batch: descriptor over its limits");
-  if (h.stride % 32 != 0 || h.stride < h.nwords) return fail(MB_ERR_INVALID, "batch: bitmap stride %llu",
-                                                              (unsigned long long)h.stride);
+  if (h.stride % 32 != 0 || h.stride < h.nwords || ((uintptr_t)h.slab & 15) != 0 || h.urow0 + h.nu > h.nslab)
+    return fail(MB_ERR_INVALID, "batch: bitmap slab (stride %llu, rows %u..%u of %u)", (unsigned long long)h.stride,
+                h.urow0, h.urow0 + h.nu, h.nslab);
   if (batch_smem(h, c) == 0) return fail(MB_ERR_INVALID, "batch: launch shape V=%u warps=%u stages=%u", c.V,
                                          c.warps, c.stages);
   switch (c.V) {

@@ -24,7 +24,7 @@
 namespace mb {
 
 constexpr uint32_t BQ_MAX = 128;   // queries per launch (7-bit query field of a row entry)
-constexpr uint32_t BU_MAX = 256;   // distinct bitmaps per launch (8-bit index)
+constexpr uint32_t BU_MAX = 256;   // bitmap rows staged per tile (a tensor-copy box side)
 constexpr uint32_t BS_MAX = 16;    // distinct op sources per launch
 constexpr uint32_t BC_MAX = 4096;  // chain entries per launch
 constexpr uint32_t BW_MAX = 16;    // warps per CTA
@@ -43,31 +43,58 @@ struct BatchSrc {
 //   [1] groups   [2] first output slot   [3] row-count slot
 //   [4] first chain entry | entries << 16
 //   [5] kv mask | filt mask << 8 | key mask << 16 | term mask << 24 (bit s: slot s)
-//   [6], [7] unused
+//   [6] compiled op shape (BSHAPES index + 1; 0: the generic drain)
+//   [7] unused
 //   slot s at 8 + 7 * s:
 //     [0] source index | width << 8 | key xform << 16 | division shifts << 24
 //     [1] term lo  [2] term hi (inclusive)  [3] division magic  [4] key base
 //     [5] key multiplier  [6] divisor
 enum : uint32_t { BQD_SLOT0 = 8, BQD_SLOTW = 7, BQD_WORDS = 8 + 7 * BSLOT };
 
+// The bitmaps are rows of one slab (`stride` words apart); a batch stages
+// rows [urow0, urow0 + nu) of every tile.
+// Op shapes with a compiled drain: which slots every row loads (kv), which
+// only uncertain rows load (filt), which are group-key slots and their
+// transform (2 bits per slot: 0 identity, 1 division, 2 year), the value
+// kind and its slots.  The engine's four query templates lower to these
+// (tmpl 1; tmpl 2; tmpl 3 at city or nation level; tmpl 4 with either key
+// scaled); any other op runs the generic drain.
+struct BShape {
+  uint32_t ns, kv, filt, keym, xf, vk, va, vb;
+};
+constexpr BShape BSHAPES[] = {
+    {4, 0x0a, 0x07, 0x00, 0x00, MB_V_MUL, 3, 1},  // tmpl 1
+    {4, 0x0e, 0x03, 0x06, 0x20, MB_V_COL, 3, 0},  // tmpl 2
+    {4, 0x0f, 0x07, 0x07, 0x08, MB_V_COL, 3, 0},  // tmpl 3, city keys
+    {4, 0x0f, 0x07, 0x07, 0x19, MB_V_COL, 3, 0},  // tmpl 3, nation keys
+    {6, 0x3b, 0x0f, 0x0b, 0x08, MB_V_SUB, 4, 5},  // tmpl 4
+    {6, 0x3b, 0x0f, 0x0b, 0x09, MB_V_SUB, 4, 5},
+    {6, 0x3b, 0x0f, 0x0b, 0x48, MB_V_SUB, 4, 5},
+    {6, 0x3b, 0x0f, 0x0b, 0x49, MB_V_SUB, 4, 5},
+};
+constexpr uint32_t BNSHAPE = sizeof(BSHAPES) / sizeof(BSHAPES[0]);
+
 struct BatchHdr {
   uint64_t nrows, nwords;
-  uint64_t stride;       // allocated words per bitmap: a multiple of 32, >= nwords
-  uint32_t nq, nu, nsrc, nchain;
+  uint64_t stride;       // words per slab row: a multiple of 32, >= nwords
+  const uint32_t *slab;
+  uint32_t nslab;        // rows of the slab
+  uint32_t urow0, nu;    // the staged run of rows
+  uint32_t nq, nsrc, nchain;
   uint32_t pf_mask;      // bit i: prefetch source i's row-indexed column into L2
-  uint32_t pad_[3];
+  uint32_t pad_;
   BatchSrc src[BS_MAX];
-  const uint32_t *ubmp[BU_MAX];
   uint32_t Qd[BQ_MAX * BQD_WORDS];
-  uint16_t chain[BC_MAX];  // union bitmap index | CNF_* flags << 8
+  uint16_t chain[BC_MAX];  // per conjunct: header, then slab rows (batch_add)
   uint8_t order[BQ_MAX];   // the order in which warps take the queries (costliest first)
 };
 
 // Launch shape of the batched scan.
 struct BatchCfg {
   uint32_t V;       // words per lane: tile = 32 * V words
-  uint32_t warps;   // warps per CTA
-  uint32_t stages;  // staged tiles in flight per CTA
+  uint32_t warps;     // warps per CTA
+  uint32_t drainers;  // of them, warps that run the jobs (the others produce them)
+  uint32_t stages;    // staged tiles in flight per CTA
   uint32_t cps;     // CTAs per SM (0: as many as fit)
 };
 

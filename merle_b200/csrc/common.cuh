@@ -51,7 +51,7 @@ inline uint64_t round_up(uint64_t a, uint64_t b) { return ceil_div(a, b) * b; }
 // ---------------------------------------------------------------- device
 // Error word written by kernels whose bounded waits ran out.  Index 0 is a
 // flag, index 1 a code (which wait), index 2 the block that gave up.
-enum { MB_DEVERR_NONE = 0, MB_DEVERR_TMA_WAIT = 1 };
+enum { MB_DEVERR_NONE = 0, MB_DEVERR_TMA_WAIT = 1, MB_DEVERR_IDLE_WAIT = 2 };
 uint32_t *device_error_word();   // per-device, allocated on first use
 mb_status check_device_error(cudaStream_t s);
 

@@ -65,7 +65,10 @@ void Engine::free_star() {
   partmfgr = nullptr;
   free_denorm();
   for (auto &c : idx)
-    for (auto &l : c.levels) free_one(allocs, l.slab);
+    for (auto &l : c.levels) l.slab = nullptr;
+  free_one(allocs, islab);
+  islab = nullptr;
+  nbm = 0;
   for (auto &c : idx) c.levels.clear();
   indexed = false;
 }
@@ -634,10 +637,10 @@ extern "C" mb_status mb_engine_build_index_ex(mb_engine *e, uint32_t flags) {
   if (!E.custkey) return fail(MB_ERR_INVALID, "mb_engine_build_index: no table");
   MB_CUDA(cudaSetDevice(E.device));
   for (auto &c : E.idx)
-    for (auto &l : c.levels) {
-      free_one(E.allocs, l.slab);
-      l.slab = nullptr;
-    }
+    for (auto &l : c.levels) l.slab = nullptr;
+  free_one(E.allocs, E.islab);
+  E.islab = nullptr;
+  E.nbm = 0;
   E.indexed = false;
   MB_CUDA(cudaEventRecord(E.ev0, E.stream));
   if (flags & MB_INDEX_PROBE_DIMS) E.free_denorm();
@@ -645,11 +648,16 @@ extern "C" mb_status mb_engine_build_index_ex(mb_engine *e, uint32_t flags) {
   MB_CHECK(E.setup_index_cols());
   uint64_t *d_pop = nullptr;
   MB_CHECK(E.alloc((void **)&d_pop, 1024 * 8));
+  for (auto &c : E.idx)
+    for (auto &l : c.levels) E.nbm += l.nbins();
+  MB_CHECK(E.alloc((void **)&E.islab, (size_t)E.nbm * E.stride * 4));
+  MB_CUDA(cudaMemsetAsync(E.islab, 0, (size_t)E.nbm * E.stride * 4, E.stream));
+  uint64_t first = 0;
   for (auto &c : E.idx) {
     for (auto &l : c.levels) {
       const uint32_t nb = l.nbins();
-      MB_CHECK(E.alloc((void **)&l.slab, (size_t)nb * E.stride * 4));
-      MB_CUDA(cudaMemsetAsync(l.slab, 0, (size_t)nb * E.stride * 4, E.stream));
+      l.slab = E.islab + first * E.stride;
+      first += nb;
       MB_CUDA(cudaMemsetAsync(d_pop, 0, nb * 8, E.stream));
       std::vector<uint64_t> lo(l.bounds.begin(), l.bounds.end() - 1), hi(l.bounds.begin() + 1, l.bounds.end());
       MB_CHECK(mb_bitmap_create(&c.src, E.nrows, lo.data(), hi.data(), nb, l.slab, E.stride, d_pop, E.stream));
@@ -872,21 +880,30 @@ enum { BADD_OK = 0, BADD_FULL = 1, BADD_ALONE = 2 };
 // Batch under construction: the staging header and its lookup tables.
 struct BatchBuild {
   BatchHdr *h = nullptr;
-  std::unordered_map<const uint32_t *, uint32_t> umap;
-  std::vector<double> cost;        // estimated cost of each query (per bitmap word)
-  double src_weight[BS_MAX] = {};  // selected-row fraction reading each source
+  uint32_t umin = 0xffffffffu, umax = 0;  // slab rows the batch reads
+  std::vector<double> cost;               // estimated cost of each query (per bitmap word)
+  double src_weight[BS_MAX] = {};         // selected-row fraction reading each source
 
-  void reset(BatchHdr *hh, uint64_t nrows, uint64_t stride) {
+  void reset(BatchHdr *hh, const Engine &E) {
     h = hh;
     memset(h, 0, sizeof(*h));
-    h->nrows = nrows;
-    h->nwords = (nrows + 31) / 32;
-    h->stride = stride;
-    umap.clear();
+    h->nrows = E.nrows;
+    h->nwords = (E.nrows + 31) / 32;
+    h->stride = E.stride;
+    h->slab = E.islab;
+    h->nslab = E.nbm;
+    umin = 0xffffffffu, umax = 0;
     cost.clear();
     for (double &w : src_weight) w = 0;
   }
 };
+
+// Row of the index slab holding bitmap p, or -1.
+static int64_t slab_row(const BatchHdr &h, const uint32_t *p) {
+  if (p < h.slab || p >= h.slab + (uint64_t)h.nslab * h.stride) return -1;
+  const uint64_t off = (uint64_t)(p - h.slab);
+  return off % h.stride ? -1 : (int64_t)(off / h.stride);
+}
 
 static bool same_src(const mb_src &a, const mb_src &b) {
   return a.col == b.col && a.fk == b.fk && a.width == b.width && a.dimsz == b.dimsz;
@@ -949,6 +966,21 @@ static bool slot_plan(const mb_op &O, uint32_t *d) {
   }
   d[0] = O.nsrc | (O.vkind << 16) | (O.va << 20) | (O.vb << 24);
   d[5] = (N.kv_mask & 0xffu) | ((N.filt_mask & 0xffu) << 8) | (keym << 16) | (termm << 24);
+  // a compiled drain for this shape, if there is one
+  uint32_t xf = 0;
+  for (uint32_t k = 0; k < O.nkey; ++k) {
+    const uint32_t x = O.keys[k].xform == MB_X_DIV ? 1u : O.keys[k].xform == MB_X_YEAR ? 2u : 0u;
+    xf |= x << (2 * O.keys[k].src);
+  }
+  const uint32_t va = O.vkind == MB_V_ONE ? 0 : O.va, vb = (O.vkind == MB_V_MUL || O.vkind == MB_V_SUB) ? O.vb : 0;
+  for (uint32_t i = 0; i < BNSHAPE; ++i) {
+    const BShape &b = BSHAPES[i];
+    if (b.ns == O.nsrc && b.kv == (N.kv_mask & 0xffu) && b.filt == (N.filt_mask & 0xffu) && b.keym == keym &&
+        b.xf == xf && b.vk == O.vkind && b.va == va && b.vb == vb && termm == b.filt) {
+      d[6] = i + 1;
+      break;
+    }
+  }
   return true;
 }
 
@@ -964,12 +996,13 @@ static int batch_add(BatchBuild &B, const Lowered &L, const DevPrg &P, uint64_t 
   uint32_t d[BQD_WORDS];
   memset(d, 0, sizeof(d));
   if (!slot_plan(O, d)) return BADD_ALONE;
-  // bitmaps and sources this query adds to the batch
-  std::vector<const uint32_t *> fresh;
+  // the slab rows this query reads
+  uint32_t rmin = B.umin, rmax = B.umax;
   for (uint32_t i = 0; i < P.ncnf; ++i) {
-    const uint32_t *p = P.cnf_ptr[i];
-    if (((uintptr_t)p & 15) != 0) return BADD_ALONE;
-    if (!B.umap.count(p) && std::find(fresh.begin(), fresh.end(), p) == fresh.end()) fresh.push_back(p);
+    const int64_t r = slab_row(h, P.cnf_ptr[i]);
+    if (r < 0) return BADD_ALONE;
+    rmin = std::min(rmin, (uint32_t)r);
+    rmax = std::max(rmax, (uint32_t)r);
   }
   uint32_t newsrc = 0;
   for (uint32_t s = 0; s < O.nsrc; ++s) {
@@ -977,15 +1010,13 @@ static int batch_add(BatchBuild &B, const Lowered &L, const DevPrg &P, uint64_t 
     for (uint32_t t = 0; t < s && !seen; ++t) seen = same_src(O.src[t], O.src[s]);
     if (!seen) ++newsrc;
   }
-  if (fresh.size() > BU_MAX || newsrc > BS_MAX || P.ncnf > BC_MAX) return BADD_ALONE;
-  if (h.nq + 1 > BQ_MAX || h.nu + fresh.size() > BU_MAX || h.nsrc + newsrc > BS_MAX || h.nchain + P.ncnf > BC_MAX)
-    return BADD_FULL;
+  const uint32_t nch = P.ncnf + MB_MAXCOLS;  // entries + at most one header per operand
+  const bool spans = P.ncnf && rmax - rmin + 1 > BU_MAX;
+  if (newsrc > BS_MAX || nch > BC_MAX || (spans && B.umin == 0xffffffffu)) return BADD_ALONE;
+  if (h.nq + 1 > BQ_MAX || spans || h.nsrc + newsrc > BS_MAX || h.nchain + nch > BC_MAX) return BADD_FULL;
   // commit
   const uint32_t q = h.nq++;
-  for (const uint32_t *p : fresh) {
-    B.umap[p] = h.nu;
-    h.ubmp[h.nu++] = p;
-  }
+  if (P.ncnf) B.umin = rmin, B.umax = rmax;
   const OpNeeds N = op_needs(O);
   for (uint32_t s = 0; s < O.nsrc; ++s) {
     int t = src_slot(h, O.src[s]);
@@ -1004,10 +1035,20 @@ static int batch_add(BatchBuild &B, const Lowered &L, const DevPrg &P, uint64_t 
   d[1] = L.ngroups;
   d[2] = (uint32_t)out_off;
   d[3] = nq_slot;
-  d[4] = h.nchain | ((uint32_t)P.ncnf << 16);
+  // the chain: per conjunct a header (middle bins | edge bins << 8 | negated
+  // << 15), then the union indices of its middle bins and of its edge bins
+  const uint32_t c0 = h.nchain;
+  for (uint32_t i = 0; i < P.ncnf;) {
+    uint32_t j = i;
+    while (!(P.cnf_flag[j] & CNF_END)) ++j;  // [i, j] is one conjunct, edges last
+    uint32_t nm = 0, ne = 0;
+    for (uint32_t k = i; k <= j; ++k) (P.cnf_flag[k] & CNF_EDGE) ? ++ne : ++nm;
+    h.chain[h.nchain++] = (uint16_t)(nm | (ne << 8) | ((P.cnf_flag[j] & CNF_NEG) ? 0x8000u : 0u));
+    for (uint32_t k = i; k <= j; ++k) h.chain[h.nchain++] = (uint16_t)slab_row(h, P.cnf_ptr[k]);
+    i = j + 1;
+  }
+  d[4] = c0 | ((h.nchain - c0) << 16);
   memcpy(h.Qd + (size_t)q * BQD_WORDS, d, sizeof(d));
-  for (uint32_t i = 0; i < P.ncnf; ++i)
-    h.chain[h.nchain++] = (uint16_t)(B.umap[P.cnf_ptr[i]] | ((uint32_t)P.cnf_flag[i] << 8));
   // cost per bitmap word of a tile: the chain entries, the compaction, and
   // the ops of the selected rows (about 2 chain entries' worth per row)
   B.cost.push_back((double)P.ncnf + 2.0 + 64.0 * sel);
@@ -1029,17 +1070,16 @@ static double est_selectivity(const Engine &E, const Lowered &L) {
 static BatchCfg batch_cfg(const BatchHdr &h, const mb_batch_opts &o) {
   BatchCfg c;
   c.V = o.words_per_lane ? o.words_per_lane : 2;
-  c.warps = o.warps ? std::min<uint32_t>(o.warps, BW_MAX) : BW_MAX;
+  c.warps = o.warps ? std::min<uint32_t>(o.warps, BW_MAX) : 16;
+  c.drainers = o.drain_warps ? o.drain_warps : c.warps / 2;
   c.cps = o.ctas_per_sm;
-  c.stages = o.stages;
   const size_t cap = (size_t)dev_info().max_smem_optin;
-  if (!c.stages) {
-    while (true) {
-      for (c.stages = 4; c.stages > 1; --c.stages)
-        if (batch_smem(h, c) && batch_smem(h, c) <= cap) break;
-      if (c.stages > 1 || c.V == 1 || o.words_per_lane) break;
-      c.V >>= 1;
-    }
+  const uint32_t smax = o.stages ? o.stages : 4;
+  while (true) {
+    for (c.stages = smax; c.stages > 1; --c.stages)
+      if (batch_smem(h, c) && batch_smem(h, c) <= cap) break;
+    if (c.stages > 1 || smax == 1 || c.V == 1 || o.words_per_lane) break;
+    c.V >>= 1;  // not even two stages of this tile fit: narrower tiles
   }
   return c;
 }
@@ -1054,6 +1094,8 @@ static mb_status batch_flush(Engine &E, BatchBuild &B, const mb_batch_opts &o, i
   for (uint32_t q = 0; q < h.nq; ++q) order[q] = q;
   std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return B.cost[a] > B.cost[b]; });
   for (uint32_t i = 0; i < h.nq; ++i) h.order[i] = (uint8_t)order[i];
+  if (B.umin == 0xffffffffu) h.urow0 = 0, h.nu = 1;  // no bitmap read: stage one row anyway
+  else h.urow0 = B.umin, h.nu = B.umax - B.umin + 1;
   h.pf_mask = 0;
   for (uint32_t i = 0; i < h.nsrc; ++i) {
     const void *base = h.src[i].fk ? (const void *)h.src[i].fk : h.src[i].col;
@@ -1095,7 +1137,8 @@ extern "C" mb_status mb_engine_enqueue_batch(mb_engine *e, const mb_query *qs, u
   if (opts) o = *opts;
   else memset(&o, 0, sizeof(o));
   if ((o.words_per_lane && o.words_per_lane != 1 && o.words_per_lane != 2 && o.words_per_lane != 4) ||
-      o.warps > 16 || o.stages > 4 || o.prefetch > MB_PREFETCH_ALL)
+      o.warps == 1 || o.warps > 16 || o.stages > 4 || o.prefetch > MB_PREFETCH_ALL ||
+      o.drain_warps >= (o.warps ? o.warps : 16u))
     return fail(MB_ERR_INVALID, "mb_engine_enqueue_batch: options out of range");
   std::vector<uint64_t> offs(n);
   const uint64_t total = mb_queries_layout(qs, n, offs.data());
@@ -1109,7 +1152,7 @@ extern "C" mb_status mb_engine_enqueue_batch(mb_engine *e, const mb_query *qs, u
   BatchHdr *h = nullptr;
   uint32_t slot = 0;
   MB_CHECK(batch_staging(E, &h, &slot));
-  B.reset(h, E.nrows, E.stride);
+  B.reset(h, E);
   Lowered L;
   DevPrg P;
   for (uint32_t i = 0; i < n; ++i) {
@@ -1122,7 +1165,7 @@ extern "C" mb_status mb_engine_enqueue_batch(mb_engine *e, const mb_query *qs, u
     if (r == BADD_FULL) {
       MB_CHECK(batch_flush(E, B, o, out_dev, nqual_dev, slot));
       MB_CHECK(batch_staging(E, &h, &slot));
-      B.reset(h, E.nrows, E.stride);
+      B.reset(h, E);
       r = batch_add(B, L, P, offs[i], i, sel);
     }
     if (r != BADD_OK) MB_CHECK(run_lowered(E, L, pl, out_dev + offs[i], nqual_dev + i, false));

@@ -80,6 +80,11 @@ struct Engine {
   uint8_t *custcity_row = nullptr;
   uint16_t *partmfgr_row = nullptr;
   IdxCol idx[IC_N];
+  // Every bitmap of the index in one slab, `stride` words apart (level by
+  // level, bin by bin): the batched scan stages a tile of any run of them
+  // with one 2-D tensor copy.
+  uint32_t *islab = nullptr;
+  uint32_t nbm = 0;  // bitmaps in the slab
   bool indexed = false;
   float index_build_ms = 0;
   // query scratch

@@ -2,6 +2,7 @@
 // completion, and a bounded mbarrier wait.  Single-GPU, CTA-local only: no
 // cluster multicast anywhere in this library.
 #pragma once
+#include <cuda.h>
 #include <stdint.h>
 
 namespace mb {
@@ -35,6 +36,18 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
           smem_addr(dst)),
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// 2-D tiled tensor copy global -> shared of the box at (x, y) (x the inner
+// coordinate; x * element size a multiple of 16 bytes), completing on `bar`.
+// Elements outside the tensor read as zero.  `map` is the generic address of
+// a kernel-parameter (__grid_constant__) tensor map.
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
       : "memory");
 }
 

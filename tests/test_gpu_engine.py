@@ -164,6 +164,7 @@ BATCH_OPTS = [
     (2, 16, 3, 0, abi.PREFETCH_ALL),
     (4, 16, 0, 0, abi.PREFETCH_AUTO),
     (2, 4, 1, 2, abi.PREFETCH_AUTO),
+    (2, 12, 0, 0, abi.PREFETCH_AUTO),
 ]
 
 
