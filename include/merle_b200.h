@@ -499,14 +499,15 @@ typedef enum mb_prefetch {
   MB_PREFETCH_ALL = 2       /* every column an op reads for every selected row */
 } mb_prefetch;
 typedef struct mb_batch_opts {
-  uint32_t words_per_lane;  /* 1, 2 or 4 (0 = auto): a tile is 1024 * words_per_lane rows */
+  uint32_t words_per_lane;  /* 1, 2 or 4 (0 = 4, narrower if a tile does not fit): a tile is
+                               1024 * words_per_lane rows */
   uint32_t warps;           /* warps per CTA, 2..16 (0 = 16) */
   uint32_t stages;          /* at most this many staged tiles in flight per CTA, 1..4
                                (0 = 4); fewer if they do not fit in shared memory */
   uint32_t ctas_per_sm;     /* 0 = occupancy */
   uint32_t prefetch;        /* mb_prefetch */
-  uint32_t drain_warps;     /* of the warps, those that run the ops (0 = half); the others
-                               evaluate the bitmaps */
+  uint32_t drain_warps;     /* of the warps, those that run the ops (0 = about a fifth);
+                               the others evaluate the bitmaps */
   uint32_t pad_[2];
 } mb_batch_opts;
 MB_API mb_status mb_engine_enqueue_batch(mb_engine *e, const mb_query *qs, uint32_t n,

@@ -123,9 +123,9 @@ __device__ __forceinline__ uint32_t b_ldw(const void *col, uint32_t i, uint32_t 
 }
 
 // Runs query q's op on the first n (<= 64) entries of qe (row | uncertain
-// << 31), two rows per lane, and accumulates them: 1-group sums and kept
-// rows into the query's slots (its warp's alone while it holds the query),
-// group sums by warp-aggregated global atomics.  q is warp-uniform: descriptor reads are broadcasts, branches on
+// << 31), two rows per lane, and accumulates them: 1-group sums (a warp
+// reduction) and kept rows into the warp's own slots, group sums by one
+// global atomic add per row.  q is warp-uniform: descriptor reads are broadcasts, branches on
 // the descriptor uniform, and the slots unrolled, so no value is picked by
 // a run-time index.  All 32 lanes call it.
 __device__ __forceinline__ void b_drain(const BCtx &C, uint32_t q, const uint32_t *qe, uint32_t n) {
@@ -225,26 +225,34 @@ __device__ __forceinline__ void b_drain(const BCtx &C, uint32_t q, const uint32_
     const uint64_t s = peer_sum64(0xffffffffu, (keep0 ? x0 : 0) + (keep1 ? x1 : 0));
     if (lane == 0) C.usum[q] += s;
   } else {
+    // one atomic add per kept row: the rows of a chunk spread over many
+    // groups, and grouping peers first (match + reduce per group) costs more
+    // than it saves
     const uint32_t base = d[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (h == 1 && n <= 32) break;
-      const bool kp = h ? keep1 : keep0;
-      const uint32_t g = h ? g1 : g0;
-      const uint32_t peers = __match_any_sync(0xffffffffu, kp ? g : 0xffffffffu);
-      if (kp) {
-        const uint64_t s = peer_sum64(peers, h ? x1 : x0);
-        if (lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&C.out[base + g], (unsigned long long)s);
-      }
-    }
+    if (keep0) atomicAdd(&C.out[base + g0], (unsigned long long)x0);
+    if (keep1) atomicAdd(&C.out[base + g1], (unsigned long long)x1);
   }
   if (lane == 0) C.ucnt[q] += kept;
   __syncwarp();
 }
 
-// b_drain for a compiled shape SH (BSHAPES): the slots, their roles and the
-// key transforms are known at compile time; only the columns, bounds and key
-// constants are read from the descriptor.  Same results as b_drain.
+// A predicated 32-bit read-only load: 0 where pred is false.  Written out so
+// that a drain's loads form one straight run the warp issues back to back.
+__device__ __forceinline__ uint32_t ldg_pred(const void *p, bool pred) {
+  uint32_t v;
+  asm volatile(
+      "{\n .reg .pred q;\n setp.ne.b32 q, %2, 0;\n mov.b32 %0, 0;\n @q ld.global.nc.b32 %0, [%1];\n}\n"
+      : "=r"(v)
+      : "l"(p), "r"(pred ? 1u : 0u));
+  return v;
+}
+
+// b_drain for a compiled shape SH (BSHAPES) whose sources are fact columns
+// (no foreign keys): the slots, their roles and the key transforms are known
+// at compile time; only the columns, bounds and key constants are read from
+// the descriptor.  Every address is formed first and every load issued in
+// one run, so a drain waits for one memory round trip, not one per slot.
+// Same results as b_drain.
 template <int SH>
 __device__ __forceinline__ void b_drain_s(const BCtx &C, uint32_t q, const uint32_t *qe, uint32_t n) {
   constexpr BShape sh = BSHAPES[SH];
@@ -254,30 +262,44 @@ __device__ __forceinline__ void b_drain_s(const BCtx &C, uint32_t q, const uint3
   const uint32_t e0 = ok0 ? qe[lane] : 0u, e1 = ok1 ? qe[lane + 32] : 0u;
   const bool c0 = ok0 && (e0 >> 31), c1 = ok1 && (e1 >> 31);
   const uint32_t r0 = e0 & 0x7fffffffu, r1 = e1 & 0x7fffffffu;
-  uint32_t v0[BSLOT], v1[BSLOT], bad0 = 0, bad1 = 0;
+  // addresses
+  uintptr_t a0[BSLOT], a1[BSLOT];
+  uint32_t wd[BSLOT];
+  bool l0[BSLOT], l1[BSLOT];
 #pragma unroll
   for (uint32_t s = 0; s < BSLOT; ++s) {
-    v0[s] = v1[s] = 0;
+    a0[s] = a1[s] = 0;
+    wd[s] = 4;
+    l0[s] = l1[s] = false;
     if (s < sh.ns && (((sh.kv | sh.filt) >> s) & 1u)) {
       const bool kvs = (sh.kv >> s) & 1u;
-      const uint32_t a = d[BQD_SLOT0 + BQD_SLOTW * s], t = a & 0xffu, w = (a >> 8) & 0xffu;
-      bool l0 = ok0 && (kvs || c0), l1 = ok1 && (kvs || c1);
-      uint32_t k0 = r0, k1 = r1;
-      const uint32_t *fk = reinterpret_cast<const uint32_t *>(C.sfk[t]);
-      if (fk) {
-        if (l0) k0 = __ldg(fk + r0);
-        if (l1) k1 = __ldg(fk + r1);
-        const uint32_t dz = C.sdim[t];
-        if (dz) {
-          if (l0 && k0 >= dz) bad0 |= 1u << s, l0 = false;
-          if (l1 && k1 >= dz) bad1 |= 1u << s, l1 = false;
-        }
-      }
-      const void *col = reinterpret_cast<const void *>(C.scol[t]);
-      if (l0) v0[s] = b_ldw(col, k0, w);
-      if (l1) v1[s] = b_ldw(col, k1, w);
+      const uint32_t a = d[BQD_SLOT0 + BQD_SLOTW * s], t = a & 0xffu;
+      wd[s] = (a >> 8) & 0xffu;
+      const uintptr_t col = (uintptr_t)C.scol[t];
+      l0[s] = ok0 && (kvs || c0);
+      l1[s] = ok1 && (kvs || c1);
+      a0[s] = col + (uintptr_t)r0 * wd[s];
+      a1[s] = col + (uintptr_t)r1 * wd[s];
     }
   }
+  // loads: the aligned words holding the values, all issued before any use
+  uint32_t raw0[BSLOT], raw1[BSLOT];
+#pragma unroll
+  for (uint32_t s = 0; s < BSLOT; ++s) {
+    raw0[s] = raw1[s] = 0;
+    if (s < sh.ns && (((sh.kv | sh.filt) >> s) & 1u)) {
+      raw0[s] = ldg_pred(reinterpret_cast<const void *>(a0[s] & ~(uintptr_t)3), l0[s]);
+      raw1[s] = ldg_pred(reinterpret_cast<const void *>(a1[s] & ~(uintptr_t)3), l1[s]);
+    }
+  }
+  uint32_t v0[BSLOT], v1[BSLOT];
+#pragma unroll
+  for (uint32_t s = 0; s < BSLOT; ++s) {
+    const uint32_t mask = wd[s] >= 4 ? 0xffffffffu : ((1u << (8 * wd[s])) - 1u);
+    v0[s] = (raw0[s] >> ((uint32_t)(a0[s] & 3) * 8)) & mask;
+    v1[s] = (raw1[s] >> ((uint32_t)(a1[s] & 3) * 8)) & mask;
+  }
+  const uint32_t bad0 = 0, bad1 = 0;
   bool keep0 = ok0, keep1 = ok1;
   if (sh.filt && __any_sync(0xffffffffu, c0 || c1)) {
 #pragma unroll
@@ -333,27 +355,21 @@ __device__ __forceinline__ void b_drain_s(const BCtx &C, uint32_t q, const uint3
     const uint64_t s = peer_sum64(0xffffffffu, (keep0 ? x0 : 0) + (keep1 ? x1 : 0));
     if (lane == 0) C.usum[q] += s;
   } else {
+    // one atomic add per kept row: the rows of a chunk spread over many
+    // groups, and grouping peers first (match + reduce per group) costs more
+    // than it saves
     const uint32_t base = d[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (h == 1 && n <= 32) break;
-      const bool kp = h ? keep1 : keep0;
-      const uint32_t g = h ? g1 : g0;
-      const uint32_t peers = __match_any_sync(0xffffffffu, kp ? g : 0xffffffffu);
-      if (kp) {
-        const uint64_t s = peer_sum64(peers, h ? x1 : x0);
-        if (lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&C.out[base + g], (unsigned long long)s);
-      }
-    }
+    if (keep0) atomicAdd(&C.out[base + g0], (unsigned long long)x0);
+    if (keep1) atomicAdd(&C.out[base + g1], (unsigned long long)x1);
   }
   if (lane == 0) C.ucnt[q] += kept;
   __syncwarp();
 }
 
-// The drain for query q: its compiled shape, or the generic one.  One
-// out-of-line copy serves every call site.
+// The drain for query q: its compiled shape (fact-column sources only), or
+// the generic one.  One out-of-line copy serves every call site.
 __device__ __noinline__ void b_drain_any(const BCtx C, uint32_t q, const uint32_t *qe, uint32_t n) {
-  switch (C.Qd[q * BQD_WORDS + 6]) {
+  switch (C.Qd[q * BQD_WORDS + 7] ? 0u : C.Qd[q * BQD_WORDS + 6]) {  // word 7: slots read through a foreign key
   case 1: b_drain_s<0>(C, q, qe, n); break;
   case 2: b_drain_s<1>(C, q, qe, n); break;
   case 3: b_drain_s<2>(C, q, qe, n); break;
@@ -470,13 +486,26 @@ __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, co
     uint32_t cm[V], cx[V];
 #pragma unroll
     for (int k = 0; k < V; ++k) cm[k] = cx[k] = 0;
-    for (uint32_t j = 0; j < nm; ++j) {
+    // middle bins four at a time: the indices, then the words, then the ORs
+    uint32_t j = 0;
+    for (; j + 4 <= nm; j += 4, i += 4) {
+      const uint32_t b0 = chain[c0 + i] - urow0, b1 = chain[c0 + i + 1] - urow0, b2 = chain[c0 + i + 2] - urow0,
+                     b3 = chain[c0 + i + 3] - urow0;
+      uint32_t x0[V], x1[V], x2[V], x3[V];
+      lds_words<V>(sl + b0 * T, x0);
+      lds_words<V>(sl + b1 * T, x1);
+      lds_words<V>(sl + b2 * T, x2);
+      lds_words<V>(sl + b3 * T, x3);
+#pragma unroll
+      for (int k = 0; k < V; ++k) cm[k] |= (x0[k] | x1[k]) | (x2[k] | x3[k]);
+    }
+    for (; j < nm; ++j) {
       uint32_t x[V];
       lds_words<V>(sl + (chain[c0 + i++] - urow0) * T, x);
 #pragma unroll
       for (int k = 0; k < V; ++k) cm[k] |= x[k];
     }
-    for (uint32_t j = 0; j < ne; ++j) {
+    for (uint32_t j2 = 0; j2 < ne; ++j2) {
       uint32_t x[V];
       lds_words<V>(sl + (chain[c0 + i++] - urow0) * T, x);
 #pragma unroll

@@ -44,7 +44,7 @@ struct BatchSrc {
 //   [4] first chain entry | entries << 16
 //   [5] kv mask | filt mask << 8 | key mask << 16 | term mask << 24 (bit s: slot s)
 //   [6] compiled op shape (BSHAPES index + 1; 0: the generic drain)
-//   [7] unused
+//   [7] slots read through a foreign key (bit s)
 //   slot s at 8 + 7 * s:
 //     [0] source index | width << 8 | key xform << 16 | division shifts << 24
 //     [1] term lo  [2] term hi (inclusive)  [3] division magic  [4] key base

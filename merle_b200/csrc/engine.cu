@@ -966,6 +966,8 @@ static bool slot_plan(const mb_op &O, uint32_t *d) {
   }
   d[0] = O.nsrc | (O.vkind << 16) | (O.va << 20) | (O.vb << 24);
   d[5] = (N.kv_mask & 0xffu) | ((N.filt_mask & 0xffu) << 8) | (keym << 16) | (termm << 24);
+  for (uint32_t s2 = 0; s2 < O.nsrc; ++s2)
+    if (O.src[s2].fk) d[7] |= 1u << s2;
   // a compiled drain for this shape, if there is one
   uint32_t xf = 0;
   for (uint32_t k = 0; k < O.nkey; ++k) {
@@ -1069,17 +1071,18 @@ static double est_selectivity(const Engine &E, const Lowered &L) {
 // (up to 4) that fit in shared memory, narrowing the tile if not even two do.
 static BatchCfg batch_cfg(const BatchHdr &h, const mb_batch_opts &o) {
   BatchCfg c;
-  c.V = o.words_per_lane ? o.words_per_lane : 2;
+  c.V = o.words_per_lane ? o.words_per_lane : 4;
   c.warps = o.warps ? std::min<uint32_t>(o.warps, BW_MAX) : 16;
-  c.drainers = o.drain_warps ? o.drain_warps : c.warps / 2;
+  c.drainers = o.drain_warps ? o.drain_warps : std::max<uint32_t>(1, (c.warps + 2) / 5);
   c.cps = o.ctas_per_sm;
   const size_t cap = (size_t)dev_info().max_smem_optin;
   const uint32_t smax = o.stages ? o.stages : 4;
   while (true) {
     for (c.stages = smax; c.stages > 1; --c.stages)
       if (batch_smem(h, c) && batch_smem(h, c) <= cap) break;
-    if (c.stages > 1 || smax == 1 || c.V == 1 || o.words_per_lane) break;
-    c.V >>= 1;  // not even two stages of this tile fit: narrower tiles
+    if (batch_smem(h, c) && batch_smem(h, c) <= cap) break;  // (one stage, if that is all that fits)
+    if (c.V == 1 || o.words_per_lane) break;
+    c.V >>= 1;  // not even one stage of this tile fits: narrower tiles
   }
   return c;
 }
