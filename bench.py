@@ -9,13 +9,17 @@ device time.  With N GPUs every rank holds its own 120M-row shard of an
 N x 120M-row table (weak scaling) and each step ends with one NCCL all-reduce
 of the int64 group tables (the only exchange step of a sharded query).
 
-  value     device-resident: queries enqueued back to back, results in HBM,
-            CUDA events on the engine stream around the timed steps
-  e2e       through the public C ABI (mb_engine_query): query descriptors from
-            host memory, int64 results read back to host every query
-  roofline  the fused kernel: algorithmic bytes (canonical bitmaps + touched
-            32-byte payload sectors + dimensions + outputs, computed by the
-            oracle on a host row sample) / its event-timed duration
+  value     device-resident: one step = the 64 queries in one batched
+            launch (mb_engine_enqueue_batch), results in HBM, CUDA events on
+            the engine stream around the timed steps; "plain" beside it times
+            the same queries one fused launch each
+  e2e       through the public C ABI (mb_engine_query_batch): query
+            descriptors from host memory, int64 results read back to host
+            every step, host wall clock
+  roofline  the batch kernel: algorithmic bytes (each distinct canonical
+            bitmap once + the union of the 32-byte payload sectors holding a
+            selected row + outputs, computed by the oracle on a host row
+            sample) / the event-timed step
   cpu_baseline  the reference's own CPU oracle (ssb/cpuref.c s1ref..s4ref,
             built from its sources into oracle/_ref) on a 24M-row sample, one
             query per thread over all host cores (the ssb_cpujoin shape)
@@ -203,6 +207,42 @@ def config_of(args, nrows_per_gpu):
 
 
 # ------------------------------------------------------------- ours
+# payload columns (width in bytes) a query's selected rows read, with the
+# engine's denormalised customer city / part mfgr columns
+BATCH_GATHER = {1: [("extendedprice", 4), ("discount", 4)],
+                2: [("partmfgr_row", 2), ("orderdate", 4), ("revenue", 4)],
+                3: [("custcity_row", 1), ("suppcity", 4), ("orderdate", 4), ("revenue", 4)],
+                4: [("suppcity", 4), ("orderdate", 4), ("partmfgr_row", 2), ("revenue", 4), ("supplycost", 4)]}
+# bytes of the batch descriptor block the engine copies to the device per
+# launch (BatchHdr: 64-byte head, 16 sources, 128 x 64-word query
+# descriptors, 4096 chain entries, 128 order bytes)
+BATCH_HDR_BYTES = 64 + 16 * 24 + 128 * 64 * 4 + 4096 * 2 + 128
+
+
+def batch_algo_bytes(star, scale: float, nrows: int, qs, ngroups) -> dict:
+    """Algorithmic bytes of one batched pass: every DISTINCT canonical bitmap
+    once, the union over the queries of the 32-byte payload sectors holding a
+    selected row (counted on the host sample, scaled), the int64 outputs."""
+    from oracle import oracle as O
+    from merle_b200 import workload as WL
+    W = (nrows + 31) // 32
+    bins = set()
+    sectors = {}
+    rows = 0
+    for q in qs:
+        t, p = WL.as_tuple(q)
+        bins |= O.canonical_bins(t, p)
+        r = np.flatnonzero(O.qualifying_mask(star, t, p))
+        rows += len(r)
+        for col, w in BATCH_GATHER[t]:
+            sectors.setdefault((col, w), []).append(r // (32 // w))
+    sec = sum(len(np.unique(np.concatenate(v))) for v in sectors.values()) * 32
+    bm = len(bins) * W * 4
+    out = 8 * sum(ngroups)
+    return {"bitmap": bm, "distinct_bitmaps": len(bins), "gather": int(sec * scale), "out": out,
+            "total": int(bm + sec * scale + out), "rows": int(rows * scale)}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -231,79 +271,94 @@ def main():
     qs = WL.random_mix(SEED_QUERIES, args.queries, args.narrow)
     Q = len(qs)
     qarr = (abi.mb_query * Q)(*qs)
+    ngroups = [Engine.ngroups(q) for q in qs]
     total_g = int(L.mb_queries_layout(qarr, Q, None))
     out = torch.zeros(total_g, dtype=torch.int64, device="cuda")
     nq = torch.zeros(Q, dtype=torch.int64, device="cuda")
     ext = torch.cuda.ExternalStream(int(L.mb_engine_stream(eng.handle) or 0))
 
-    def step(record=False):
-        check(L.mb_engine_enqueue(eng.handle, qarr, Q, None, out.data_ptr(), nq.data_ptr(), 1 if record else 0))
+    def allreduce():
         if world > 1:
             with torch.cuda.stream(ext):
                 dist.all_reduce(out)
 
+    def step_batch():
+        check(L.mb_engine_enqueue_batch(eng.handle, qarr, Q, None, out.data_ptr(), nq.data_ptr()))
+        allreduce()
+
+    def step_plain(record=False):
+        check(L.mb_engine_enqueue(eng.handle, qarr, Q, None, out.data_ptr(), nq.data_ptr(), 1 if record else 0))
+        allreduce()
+
+    def timed(step, steps, mark0, mark1):
+        check(L.mb_engine_mark(eng.handle, mark0))
+        for _ in range(steps):
+            step()
+        check(L.mb_engine_mark(eng.handle, mark1))
+        ms = C.c_float(0)
+        check(L.mb_engine_marks_ms(eng.handle, mark0, mark1, C.byref(ms)))
+        v = float(ms.value)
+        if world > 1:
+            t = torch.tensor([v], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            v = float(t.item())
+        return v
+
+    rows_total = n * world
+    # ---- the batched path: warm-up, then K timed steps (one launch each)
     for _ in range(args.warmup):
-        step()
+        step_batch()
     check(L.mb_engine_sync(eng.handle, None, 0))
+    batch_out = out.clone()
     if world > 1:
         dist.barrier()
-    # ---- timed region: K steps, per-query events on the last one
-    times = np.zeros((args.steps, Q), np.float32)
     with Clocks(local) as clk:
-        check(L.mb_engine_mark(eng.handle, 0))
-        for s in range(args.steps):
-            step(record=(s == args.steps - 1))
-        check(L.mb_engine_mark(eng.handle, 1))
-        tbuf = (C.c_float * Q)()
-        check(L.mb_engine_sync(eng.handle, tbuf, Q))
-        ms = C.c_float(0)
-        check(L.mb_engine_marks_ms(eng.handle, 0, 1, C.byref(ms)))
+        ms_total = timed(step_batch, args.steps, 0, 1)
     torch.cuda.synchronize()
-    ms_total = float(ms.value)
-    if world > 1:
-        t = torch.tensor([ms_total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
-    qtimes = np.array(tbuf[:], np.float64)
-    rows_total = n * world
     value = rows_total * Q * args.steps / (ms_total / 1e3)
 
-    # ---- per-query latency through the public API with host buffers (e2e)
-    lat = []
-    e2e_ms = 0.0
-    h2d = C.sizeof(abi.mb_query) * Q
-    d2h = 8 * total_g + 8 * Q
-    res_host = np.zeros(max(info["nbitmaps"], 8192), np.int64)
-    nqh = C.c_uint64(0)
-    for _ in range(1):
-        for q in qs:  # warm
-            check(L.mb_engine_query(eng.handle, C.byref(q), None, res_host.ctypes.data, C.addressof(nqh), None))
+    # ---- the plain path (one launch sequence per query), for comparison
+    for _ in range(args.warmup):
+        step_plain()
+    check(L.mb_engine_sync(eng.handle, None, 0))
+    same = bool(torch.equal(out, batch_out))
     if world > 1:
         dist.barrier()
-    check(L.mb_engine_mark(eng.handle, 2))
+    plain_ms = timed(step_plain, args.steps, 2, 3)
+    step_plain(record=True)
+    tbuf = (C.c_float * Q)()
+    check(L.mb_engine_sync(eng.handle, tbuf, Q))
+    qtimes = np.array(tbuf[:], np.float64)
+
+    # ---- e2e through the public API with host buffers: mb_engine_query_batch
+    res_host = np.zeros(total_g, np.int64)
+    nq_host = np.zeros(Q, np.uint64)
+    check(L.mb_engine_query_batch(eng.handle, qarr, Q, None, res_host.ctypes.data, nq_host.ctypes.data))
+    if world > 1:
+        dist.barrier()
+    lat = []
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        for q in qs:
-            t1 = time.perf_counter()
-            check(L.mb_engine_query(eng.handle, C.byref(q), None, res_host.ctypes.data, C.addressof(nqh), None))
-            lat.append((time.perf_counter() - t1) * 1e3)
-    check(L.mb_engine_mark(eng.handle, 3))
+        t1 = time.perf_counter()
+        check(L.mb_engine_mark(eng.handle, 4))
+        check(L.mb_engine_query_batch(eng.handle, qarr, Q, None, res_host.ctypes.data, nq_host.ctypes.data))
+        check(L.mb_engine_mark(eng.handle, 5))
+        lat.append((time.perf_counter() - t1) * 1e3)
     e2e_wall = time.perf_counter() - t0
-    ems = C.c_float(0)
-    check(L.mb_engine_marks_ms(eng.handle, 2, 3, C.byref(ems)))
-    e2e_ms = float(ems.value)
+    e2e_ms = float(e2e_wall * 1e3)
     if world > 1:
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e = {"value": rows_total * Q * args.e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
-           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "api": "mb_engine_query per query (host query descriptor in, host int64 results out)",
-           "wall_s": e2e_wall}
+           "h2d_bytes_per_step": C.sizeof(abi.mb_query) * Q + BATCH_HDR_BYTES,
+           "d2h_bytes_per_step": 8 * total_g + 8 * Q,
+           "api": "mb_engine_query_batch (host query descriptors in, host int64 group sums and row counts out, "
+                  "returns when they are on the host)",
+           "timing": "host wall clock around each call", "ms_per_step": e2e_ms / args.e2e_steps}
 
     line = None
     if rank == 0:
-        # ---- roofline of the fused kernel (algorithmic bytes from the oracle)
         from oracle import oracle as O
         peaks = {}
         pk = ROOT / "MEASURED_PEAKS.json"
@@ -312,36 +367,48 @@ def main():
         peak = float(peaks.get("hbm_gbs", 6650.0))
         sample_n = min(CPU_SAMPLE_ROWS, n)
         star = cpu_sample(args.k, sample_n)
+        ab = batch_algo_bytes(star, n / sample_n, n, qs, ngroups)
+        step_s = ms_total / args.steps / 1e3
+        achieved = ab["total"] / step_s / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy), of measured" if peaks
+                               else "fallback 6.65 TB/s",
+                "kernel": "batch_scan_kernel (one launch per 64-query step)",
+                "algo_bytes_per_launch": ab["total"], "algo_bytes_detail": ab,
+                "launch_ms_avg": ms_total / args.steps,
+                "traffic": None, "traffic_note": "per-launch DRAM bytes in profiles/ (ncu)"}
+        tj = ROOT / "profiles" / "traffic.json"
+        if tj.exists():
+            t = json.loads(tj.read_text()).get("batch_scan_kernel")
+            if t:
+                roof["traffic"] = t["dram_bytes_per_row"] * n
+                roof["traffic_note"] = "ncu capture of a 24M-row launch scaled to this launch's rows: " + t["source"]
         widths = {c: (4 if args.width4 else {"orderdate": 2, "discount": 1, "quantity": 1, "suppcity": 1}.get(c, 4))
                   for c in ["extendedprice", "discount", "partkey", "orderdate", "revenue", "custkey", "suppcity",
                             "supplycost", "quantity"]}
-        ab = []
-        for q in qs:
-            t, p = WL.as_tuple(q)
-            ab.append(O.algo_bytes(star, n / sample_n, n, t, p, Engine.ngroups(q), widths))
-        algo_total = sum(a["total"] for a in ab)
-        kern_s = qtimes.sum() / 1e3
-        achieved = algo_total / kern_s / 1e9
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6.65 TB/s",
-                "kernel": "vbp_grpby_kernel (one launch per query)",
-                "algo_bytes_per_launch": algo_total / Q, "launch_ms_avg": float(qtimes.mean()),
-                "traffic": None, "traffic_note": "per-launch DRAM bytes in profiles/ (ncu)"}
+        plain_algo = sum(O.algo_bytes(star, n / sample_n, n, *WL.as_tuple(q), Engine.ngroups(q), widths)["total"]
+                         for q in qs)
         cpu = None if args.no_cpu or world > 1 else cpu_baseline(args, qs)
         lat_a = np.array(lat)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-                "config": config_of(args, n), "impl": "ours", "plan": "plain (rule planner, one launch per query)",
+                "config": config_of(args, n), "impl": "ours",
+                "plan": "batched: the whole mix in one persistent launch per step (rule-planner covers)",
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-                "latency_ms": {"p50": float(np.percentile(lat_a, 50)), "p99": float(np.percentile(lat_a, 99)),
-                               "kernel_p50": float(np.percentile(qtimes, 50)),
-                               "kernel_p99": float(np.percentile(qtimes, 99))},
-                "gpu_launches": Q * args.steps,
+                "plain": {"value": rows_total * Q * args.steps / (plain_ms / 1e3), "ms_per_step": plain_ms / args.steps,
+                          "batched_speedup": plain_ms / ms_total, "results_identical": same,
+                          "roofline_frac": plain_algo / (qtimes.sum() / 1e3) / 1e9 / peak,
+                          "plan": "one fused launch per query (rule planner)"},
+                "latency_ms": {"batch_e2e_p50": float(np.percentile(lat_a, 50)),
+                               "batch_e2e_p99": float(np.percentile(lat_a, 99)),
+                               "plain_kernel_p50": float(np.percentile(qtimes, 50)),
+                               "plain_kernel_p99": float(np.percentile(qtimes, 99))},
+                "gpu_launches": args.steps,
                 "clocks": clk.summary(),
                 "index": {"bitmaps": info["nbitmaps"], "bytes": info["index_bytes"],
-                          "build_ms": info["index_build_ms"]},
-                "selected_rows_per_step": sum(a["rows"] for a in ab)}
+                          "build_ms": info["index_build_ms"], "denorm_bytes": info["denorm_bytes"]},
+                "selected_rows_per_step": ab["rows"]}
         print(json.dumps(line))
     eng.close()
     if world > 1:

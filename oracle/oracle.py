@@ -295,6 +295,46 @@ def canonical_bitmaps(tmpl: int, p) -> int:
     return total
 
 
+def canonical_bins(tmpl: int, p) -> set:
+    """The bitmaps (column, level, bin) of canonical_bitmaps' choice per
+    predicate: the exact cover or the exact cover of the complement, whichever
+    has fewer bins (the finest level's bins when no exact cover exists)."""
+    out = set()
+    for col, a, b in PREDS[tmpl]:
+        dlo, dhi, levels = INDEX_LEVELS[col]
+        lo, hi = max(p[a], dlo), min(p[b], dhi)
+        if lo >= hi or (lo == dlo and hi == dhi):
+            continue
+
+        def cover(x, y):
+            bins = []
+            while x < y:
+                for li, bnd in enumerate(levels):
+                    if x in bnd:
+                        j = bnd.index(x)
+                        if j + 1 < len(bnd) and bnd[j + 1] <= y:
+                            bins.append((col, li, j))
+                            x = bnd[j + 1]
+                            break
+                else:
+                    return None
+            return bins
+        cands = []
+        d = cover(lo, hi)
+        if d is not None:
+            cands.append(d)
+        c1 = cover(dlo, lo) if dlo < lo else []
+        c2 = cover(hi, dhi) if hi < dhi else []
+        if c1 is not None and c2 is not None:
+            cands.append(c1 + c2)
+        if not cands:
+            f = levels[-1]
+            li = len(levels) - 1
+            cands.append([(col, li, j) for j in range(len(f) - 1) if f[j + 1] > lo and f[j] < hi])
+        out.update(min(cands, key=len))
+    return out
+
+
 def qualifying_mask(star: "StarHost", tmpl: int, p) -> np.ndarray:
     """Rows that satisfy every predicate of the query (numpy, vectorised)."""
     c = star.cols
