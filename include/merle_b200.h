@@ -520,6 +520,66 @@ MB_API mb_status mb_engine_query_batch(mb_engine *e, const mb_query *qs, uint32_
                                        const mb_batch_opts *opts, int64_t *out_host,
                                        uint64_t *nqual_host);
 
+/* ------------------------------------------------------------------------
+ * Learned planner.  No counterpart in the reference, whose programs come from
+ * fixed rules (col::from_bin / from_bin2, bmpidx_create.cu:138-226).
+ *
+ * A 3-layer perceptron (in -> hidden -> hidden -> out, ReLU between), FP32
+ * weights, trained on the GPU by the library's own forward, backward and Adam
+ * kernels on timings the engine records; planning runs it in BF16.  It
+ * predicts the log device time of each of MB_PLAN_CANDIDATES candidate plans
+ * of a query from MB_PLAN_FEATURES features, and the engine runs the
+ * candidate it predicts fastest.  Plans never change the arithmetic, so the
+ * answers are the same under any plan. */
+typedef struct mb_mlp mb_mlp;
+typedef struct mb_mlp_config {
+  uint32_t in, hidden, out;  /* layer widths */
+  uint32_t seed;             /* initial weights (He-uniform from a counter hash) */
+} mb_mlp_config;
+typedef struct mb_mlp_train_opts {
+  uint32_t epochs, batch;
+  float lr, beta1, beta2;    /* Adam */
+  uint32_t seed;             /* the order of the rows in each epoch */
+} mb_mlp_train_opts;
+MB_API mb_status mb_mlp_create(int device, const mb_mlp_config *cfg, mb_mlp **out);
+MB_API mb_status mb_mlp_destroy(mb_mlp *m);
+MB_API uint32_t mb_mlp_nparams(const mb_mlp *m);
+/* Parameters, layer by layer: W1 [hidden x in], b1, W2 [hidden x hidden], b2,
+ * W3 [out x hidden], b3 (row-major: W[j][i] weighs input i into output j). */
+MB_API mb_status mb_mlp_get_params(mb_mlp *m, float *host);
+MB_API mb_status mb_mlp_set_params(mb_mlp *m, const float *host);
+/* y [n x out] for x [n x in] (host arrays); bf16 != 0 rounds weights and
+ * activations to bfloat16 (FP32 accumulation). */
+MB_API mb_status mb_mlp_forward(mb_mlp *m, const float *x_host, uint32_t n, int bf16, float *y_host);
+/* Gradient of the masked mean squared error mean((y - t)^2 over mask != 0)
+ * with respect to every parameter (layout of mb_mlp_get_params), and the
+ * loss; for checking the backward kernels. */
+MB_API mb_status mb_mlp_gradients(mb_mlp *m, const float *x, const float *t, const float *mask, uint32_t n,
+                                  float *grad_host, float *loss);
+/* Mini-batch Adam on (x, t, mask), all on the GPU; *final_loss = the mean
+ * loss of the last epoch. */
+MB_API mb_status mb_mlp_train(mb_mlp *m, const float *x, const float *t, const float *mask, uint32_t n,
+                              const mb_mlp_train_opts *opts, float *final_loss);
+
+#define MB_PLAN_FEATURES 32
+#define MB_PLAN_CANDIDATES 12
+/* A query's planner features (MB_PLAN_FEATURES floats): template, per
+ * predicate its bins, edge bins and estimated selectivity (bin popcounts),
+ * the popcount of the whole program on the first 1% of the rows (a GPU
+ * pass), column and group-domain sizes. */
+MB_API mb_status mb_engine_query_features(mb_engine *e, const mb_query *q, float *features);
+/* Candidate plan idx (0 = the rule plan) of a query: fused or materialised
+ * predicates, predicate order, group-by strategy, tile width, staging, scan. */
+MB_API mb_status mb_engine_plan_candidate(mb_engine *e, const mb_query *q, uint32_t idx, mb_plan *out);
+/* The network the engine plans with (borrowed: it must outlive its use);
+ * NULL returns to the rule planner. */
+MB_API mb_status mb_engine_set_planner(mb_engine *e, mb_mlp *m);
+/* Plans n queries with the network (one BF16 forward pass for all of them):
+ * plans[i] = the candidate with the least predicted time, chosen[i] its
+ * index (may be NULL).  Without a network: the rule plan. */
+MB_API mb_status mb_engine_plan_learned(mb_engine *e, const mb_query *qs, uint32_t n, mb_plan *plans,
+                                        uint32_t *chosen);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -129,6 +129,19 @@ class mb_plan(C.Structure):
                 ("launch", mb_launch)]
 
 
+MB_PLAN_FEATURES = 32
+MB_PLAN_CANDIDATES = 12
+
+
+class mb_mlp_config(C.Structure):
+    _fields_ = [("in_", C.c_uint32), ("hidden", C.c_uint32), ("out", C.c_uint32), ("seed", C.c_uint32)]
+
+
+class mb_mlp_train_opts(C.Structure):
+    _fields_ = [("epochs", C.c_uint32), ("batch", C.c_uint32), ("lr", C.c_float), ("beta1", C.c_float),
+                ("beta2", C.c_float), ("seed", C.c_uint32)]
+
+
 class mb_query_stats(C.Structure):
     _fields_ = [("ms", C.c_float), ("nbitmaps", C.c_uint32), ("chk", C.c_uint32), ("algo_bytes", C.c_uint64)]
 
@@ -187,6 +200,18 @@ SIGNATURES: dict[str, tuple] = {
     "mb_engine_stream": (VOIDP, [VOIDP]),
     "mb_engine_enqueue_batch": (I32, [VOIDP, C.POINTER(mb_query), U32, C.POINTER(mb_batch_opts), VOIDP, VOIDP]),
     "mb_engine_query_batch": (I32, [VOIDP, C.POINTER(mb_query), U32, C.POINTER(mb_batch_opts), VOIDP, VOIDP]),
+    "mb_mlp_create": (I32, [I32, C.POINTER(mb_mlp_config), C.POINTER(VOIDP)]),
+    "mb_mlp_destroy": (I32, [VOIDP]),
+    "mb_mlp_nparams": (U32, [VOIDP]),
+    "mb_mlp_get_params": (I32, [VOIDP, VOIDP]),
+    "mb_mlp_set_params": (I32, [VOIDP, VOIDP]),
+    "mb_mlp_forward": (I32, [VOIDP, VOIDP, U32, I32, VOIDP]),
+    "mb_mlp_gradients": (I32, [VOIDP, VOIDP, VOIDP, VOIDP, U32, VOIDP, C.POINTER(C.c_float)]),
+    "mb_mlp_train": (I32, [VOIDP, VOIDP, VOIDP, VOIDP, U32, C.POINTER(mb_mlp_train_opts), C.POINTER(C.c_float)]),
+    "mb_engine_query_features": (I32, [VOIDP, C.POINTER(mb_query), VOIDP]),
+    "mb_engine_plan_candidate": (I32, [VOIDP, C.POINTER(mb_query), U32, C.POINTER(mb_plan)]),
+    "mb_engine_set_planner": (I32, [VOIDP, VOIDP]),
+    "mb_engine_plan_learned": (I32, [VOIDP, C.POINTER(mb_query), U32, C.POINTER(mb_plan), VOIDP]),
     "mb_gen_flat": (I32, [U64, U64, U64, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP]),
     "mb_gen_star": (I32, [U64, U32, U64, U64, I32, C.POINTER(mb_star_cols), VOIDP]),
     "mb_gen_star_dims": (I32, [U64, U32, VOIDP, VOIDP, VOIDP, VOIDP]),

@@ -1194,3 +1194,185 @@ extern "C" mb_status mb_engine_query_batch(mb_engine *e, const mb_query *qs, uin
   MB_CUDA(cudaStreamSynchronize(E.stream));
   return check_device_error(E.stream);
 }
+
+// ------------------------------------------------------------ learned planner
+namespace mb {
+
+// Popcounts of the program's possible and uncertain bits over its first nw
+// words (the planner's 1% sample).
+__global__ void sample_popc_kernel(const __grid_constant__ DevPrg P, uint64_t nw, unsigned long long *cnt) {
+  unsigned long long pc = 0, uc = 0;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t p[1], u[1];
+    vbp_eval<1, true>(P, w, p, u);
+    pc += __popc(p[0]);
+    uc += __popc(u[0]);
+  }
+  for (int o = 16; o; o >>= 1) {
+    pc += __shfl_down_sync(0xffffffffu, pc, o);
+    uc += __shfl_down_sync(0xffffffffu, uc, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (pc) atomicAdd(&cnt[0], pc);
+    if (uc) atomicAdd(&cnt[1], uc);
+  }
+}
+
+// The rule lowering of a query plus its per-predicate facts (template order).
+struct QueryFacts {
+  Lowered L;
+  uint32_t npred = 0;
+  double est[4] = {1, 1, 1, 1};  // estimated selected fraction per predicate
+  bool full[4] = {}, comp[4] = {};
+  uint32_t nb[4] = {}, ne[4] = {};
+};
+
+static mb_status query_facts(Engine &E, const mb_query &q, QueryFacts &F) {
+  mb_plan pl;
+  memset(&pl, 0, sizeof(pl));
+  MB_CHECK(lower_query(E, q, pl, F.L));
+  F.npred = (uint32_t)std::min<size_t>(4, F.L.preds.size());
+  for (uint32_t i = 0; i < F.npred; ++i) {
+    const Cover &c = F.L.covers[i];
+    F.full[i] = c.full;
+    F.comp[i] = c.complement;
+    F.nb[i] = c.nb();
+    F.ne[i] = (c.left ? 1 : 0) + (c.right ? 1 : 0);
+    F.est[i] = c.full ? 1.0 : c.empty ? 0.0 : std::min(1.0, (double)c.est_rows / std::max<uint64_t>(1, E.nrows));
+  }
+  return MB_OK;
+}
+
+static float nlog10(double x, double floor_, double span) {  // log10 scaled into about [0, 1]
+  return (float)((log10(std::max(x, floor_)) - log10(floor_)) / span);
+}
+
+static mb_status features_of(Engine &E, const mb_query &q, QueryFacts &F, float *f) {
+  MB_CHECK(query_facts(E, q, F));
+  memset(f, 0, MB_PLAN_FEATURES * sizeof(float));
+  if (q.tmpl >= 1 && q.tmpl <= 4) f[q.tmpl - 1] = 1.f;
+  double sel = 1;
+  for (uint32_t i = 0; i < F.npred; ++i) {
+    float *g = f + 4 + 5 * i;
+    g[0] = log2f(1.f + (float)F.nb[i]) / 6.f;
+    g[1] = (float)F.ne[i] * 0.5f;
+    g[2] = nlog10(F.est[i], 1e-7, 7.0);
+    g[3] = F.comp[i] ? 1.f : 0.f;
+    g[4] = F.full[i] ? 1.f : 0.f;
+    sel *= F.est[i];
+  }
+  f[24] = nlog10(sel, 1e-9, 9.0);
+  // popcount of the whole program on the first 1% of the rows
+  double ssel = 0, sunc = 0;
+  if (!F.L.empty && F.L.prg.ncols + F.L.prg.instrs[0].opcode > 0) {
+    DevPrg P;
+    bool v4 = false;
+    MB_CHECK(flatten_prg(&F.L.prg, 1, &P, &v4));
+    const uint64_t nw = std::max<uint64_t>(1, P.nwords / 100);
+    if (!E.d_feat) MB_CHECK(E.alloc((void **)&E.d_feat, 16));
+    MB_CUDA(cudaMemsetAsync(E.d_feat, 0, 16, E.stream));
+    const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(nw, 256), 148ull * 4);
+    sample_popc_kernel<<<grid, 256, 0, E.stream>>>(P, nw, E.d_feat);
+    MB_LAUNCH_CHECK("sample_popc_kernel");
+    unsigned long long h[2] = {0, 0};
+    MB_CUDA(cudaMemcpyAsync(h, E.d_feat, 16, cudaMemcpyDeviceToHost, E.stream));
+    MB_CUDA(cudaStreamSynchronize(E.stream));
+    const double rows = (double)std::min<uint64_t>(E.nrows, nw * 32);
+    ssel = (double)h[0] / std::max(1.0, rows);
+    sunc = h[0] ? (double)h[1] / (double)h[0] : 0.0;
+  }
+  f[25] = nlog10(ssel, 1e-7, 7.0);
+  f[26] = (float)sunc;
+  f[27] = log2f((float)std::max<uint32_t>(1, F.L.ngroups)) / 16.f;
+  f[28] = (float)log10((double)std::max<uint64_t>(1, E.nrows)) / 10.f;
+  f[29] = F.L.chk ? 1.f : 0.f;
+  f[30] = (float)F.L.nbitmaps / 64.f;
+  f[31] = 1.f;
+  return MB_OK;
+}
+
+static void candidate_of(const QueryFacts &F, uint32_t idx, mb_plan &p) {
+  memset(&p, 0, sizeof(p));
+  p.kind = MB_PLAN_FUSED;
+  p.launch.grp_strategy = MB_GRP_AUTO;
+  int most = -1, least = -1;
+  for (uint32_t i = 0; i < F.npred; ++i) {
+    if (F.full[i]) continue;
+    if (most < 0 || F.est[i] < F.est[most]) most = (int)i;
+    if (least < 0 || F.est[i] > F.est[least]) least = (int)i;
+  }
+  switch (idx) {
+  case 1: p.order_mode = 1; break;
+  case 2: p.launch.words_per_lane = 4; break;
+  case 3: p.launch.words_per_lane = 1; break;
+  case 4:
+    if (most >= 0) p.materialise = 1u << most;
+    break;
+  case 5:
+    for (uint32_t i = 0; i < F.npred; ++i)
+      if (!F.full[i] && (int)i != least) p.materialise |= 1u << i;
+    break;
+  case 6: p.kind = MB_PLAN_MATERIALISED; break;
+  case 7: p.kind = MB_PLAN_SCAN; break;
+  case 8:
+    if (F.L.ngroups <= 4096) p.launch.grp_strategy = MB_GRP_SHARED;
+    break;
+  case 9: p.launch.grp_strategy = MB_GRP_GLOBAL; break;
+  case 10: p.launch.grp_strategy = MB_GRP_HASH; break;
+  case 11: p.launch.staging = MB_STAGE_TMA; break;
+  default: break;  // 0: the rule plan
+  }
+}
+
+}  // namespace mb
+
+extern "C" mb_status mb_engine_query_features(mb_engine *e, const mb_query *q, float *features) {
+  if (!e || !q || !features) return fail(MB_ERR_INVALID, "mb_engine_query_features: NULL argument");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  QueryFacts F;
+  return features_of(E, *q, F, features);
+}
+
+extern "C" mb_status mb_engine_plan_candidate(mb_engine *e, const mb_query *q, uint32_t idx, mb_plan *out) {
+  if (!e || !q || !out) return fail(MB_ERR_INVALID, "mb_engine_plan_candidate: NULL argument");
+  if (idx >= MB_PLAN_CANDIDATES) return fail(MB_ERR_INVALID, "mb_engine_plan_candidate: candidate %u", idx);
+  QueryFacts F;
+  MB_CHECK(query_facts(e->E, *q, F));
+  candidate_of(F, idx, *out);
+  return MB_OK;
+}
+
+extern "C" mb_status mb_engine_set_planner(mb_engine *e, mb_mlp *m) {
+  if (!e) return fail(MB_ERR_INVALID, "mb_engine_set_planner: NULL engine");
+  e->E.planner = m;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_engine_plan_learned(mb_engine *e, const mb_query *qs, uint32_t n, mb_plan *plans,
+                                           uint32_t *chosen) {
+  if (!e || (n && (!qs || !plans))) return fail(MB_ERR_INVALID, "mb_engine_plan_learned: NULL argument");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  std::vector<QueryFacts> F(n);
+  std::vector<float> x((size_t)n * MB_PLAN_FEATURES);
+  for (uint32_t i = 0; i < n; ++i) MB_CHECK(features_of(E, qs[i], F[i], &x[(size_t)i * MB_PLAN_FEATURES]));
+  std::vector<uint32_t> pick(n, 0);
+  if (E.planner && n) {
+    const uint32_t no = mb_mlp_nparams(E.planner) ? MB_PLAN_CANDIDATES : 0;
+    std::vector<float> y((size_t)n * MB_PLAN_CANDIDATES);
+    MB_CHECK(mb_mlp_forward(E.planner, x.data(), n, 1, y.data()));
+    for (uint32_t i = 0; i < n; ++i) {
+      const float *yi = &y[(size_t)i * MB_PLAN_CANDIDATES];
+      uint32_t best = 0;
+      for (uint32_t c = 1; c < no; ++c)
+        if (yi[c] < yi[best]) best = c;
+      pick[i] = best;
+    }
+  }
+  for (uint32_t i = 0; i < n; ++i) {
+    candidate_of(F[i], pick[i], plans[i]);
+    if (chosen) chosen[i] = pick[i];
+  }
+  return MB_OK;
+}

@@ -99,6 +99,8 @@ struct Engine {
   uint64_t rows_cap = 0;
   uint64_t *d_rowcnt = nullptr;  // row count of the materialised plan
   std::vector<void *> allocs;
+  unsigned long long *d_feat = nullptr;  // the planner's sample popcounts
+  mb_mlp *planner = nullptr;             // borrowed (mb_engine_set_planner)
   // batch descriptors: a ring of pinned host staging headers (each reusable
   // once its copy event completed) and the device copy
   static constexpr int BQ_RING = 4;
