@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--width4", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="default launch shape instead of the autotuner's")
+    ap.add_argument("--no-graph", action="store_true", help="enqueue each step instead of replaying a CUDA graph")
     return ap.parse_args()
 
 
@@ -214,9 +216,9 @@ BATCH_GATHER = {1: [("extendedprice", 4), ("discount", 4)],
                 3: [("custcity_row", 1), ("suppcity", 4), ("orderdate", 4), ("revenue", 4)],
                 4: [("suppcity", 4), ("orderdate", 4), ("partmfgr_row", 2), ("revenue", 4), ("supplycost", 4)]}
 # bytes of the batch descriptor block the engine copies to the device per
-# launch (BatchHdr: 64-byte head, 16 sources, 128 x 64-word query
-# descriptors, 4096 chain entries, 128 order bytes)
-BATCH_HDR_BYTES = 64 + 16 * 24 + 128 * 64 * 4 + 4096 * 2 + 128
+# launch (BatchHdr: 256-byte head with the 48 staging copies, 16 sources,
+# 128 x 64-word query descriptors, 4096 chain entries, 128 order bytes)
+BATCH_HDR_BYTES = 256 + 16 * 24 + 128 * 64 * 4 + 4096 * 2 + 128
 
 
 def batch_algo_bytes(star, scale: float, nrows: int, qs, ngroups) -> dict:
@@ -282,8 +284,26 @@ def main():
             with torch.cuda.stream(ext):
                 dist.all_reduce(out)
 
+    # the launch shape from the autotuner (timed on this mix, before the
+    # measured steps), and the batch captured once as a CUDA graph
+    bopts = abi.mb_batch_opts()
+    tune = {"tuned": False}
+    if not args.no_tune:
+        tms, tried = C.c_float(0), C.c_uint32(0)
+        t0 = time.perf_counter()
+        check(L.mb_engine_tune_batch(eng.handle, qarr, Q, 3, C.byref(bopts), C.byref(tms), C.byref(tried)))
+        tune = {"tuned": True, "shapes_timed": tried.value, "best_ms": tms.value, "tune_s": time.perf_counter() - t0,
+                "opts": {f: getattr(bopts, f) for f, _ in bopts._fields_ if f != "pad_"}}
+    graph = C.c_void_p()
+    if not args.no_graph:
+        check(L.mb_batch_graph_create(eng.handle, qarr, Q, C.byref(bopts), out.data_ptr(), nq.data_ptr(),
+                                      C.byref(graph)))
+
     def step_batch():
-        check(L.mb_engine_enqueue_batch(eng.handle, qarr, Q, None, out.data_ptr(), nq.data_ptr()))
+        if graph:
+            check(L.mb_batch_graph_launch(graph))
+        else:
+            check(L.mb_engine_enqueue_batch(eng.handle, qarr, Q, C.byref(bopts), out.data_ptr(), nq.data_ptr()))
         allreduce()
 
     def step_plain(record=False):
@@ -333,7 +353,7 @@ def main():
     # ---- e2e through the public API with host buffers: mb_engine_query_batch
     res_host = np.zeros(total_g, np.int64)
     nq_host = np.zeros(Q, np.uint64)
-    check(L.mb_engine_query_batch(eng.handle, qarr, Q, None, res_host.ctypes.data, nq_host.ctypes.data))
+    check(L.mb_engine_query_batch(eng.handle, qarr, Q, C.byref(bopts), res_host.ctypes.data, nq_host.ctypes.data))
     if world > 1:
         dist.barrier()
     lat = []
@@ -341,7 +361,8 @@ def main():
     for _ in range(args.e2e_steps):
         t1 = time.perf_counter()
         check(L.mb_engine_mark(eng.handle, 4))
-        check(L.mb_engine_query_batch(eng.handle, qarr, Q, None, res_host.ctypes.data, nq_host.ctypes.data))
+        check(L.mb_engine_query_batch(eng.handle, qarr, Q, C.byref(bopts), res_host.ctypes.data,
+                                      nq_host.ctypes.data))
         check(L.mb_engine_mark(eng.handle, 5))
         lat.append((time.perf_counter() - t1) * 1e3)
     e2e_wall = time.perf_counter() - t0
@@ -394,7 +415,9 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
                 "config": config_of(args, n), "impl": "ours",
-                "plan": "batched: the whole mix in one persistent launch per step (rule-planner covers)",
+                "plan": "batched: the whole mix in one persistent launch per step (rule-planner covers)"
+                        + ("; replayed as a CUDA graph" if graph else ""),
+                "batch_shape": tune,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "plain": {"value": rows_total * Q * args.steps / (plain_ms / 1e3), "ms_per_step": plain_ms / args.steps,
                           "batched_speedup": plain_ms / ms_total, "results_identical": same,
@@ -410,6 +433,8 @@ def main():
                           "build_ms": info["index_build_ms"], "denorm_bytes": info["denorm_bytes"]},
                 "selected_rows_per_step": ab["rows"]}
         print(json.dumps(line))
+    if graph:
+        check(L.mb_batch_graph_destroy(graph))
     eng.close()
     if world > 1:
         dist.barrier()

@@ -53,7 +53,9 @@ typedef enum mb_status {
   MB_ERR_CUDA = 3,        /* a CUDA runtime call or launch failed */
   MB_ERR_TIMEOUT = 4,     /* a bounded device-side wait ran out */
   MB_ERR_UNSUPPORTED = 5, /* feature not available in this build */
-  MB_ERR_IO = 6           /* file open / read / write failed */
+  MB_ERR_IO = 6,          /* file open / read / write failed */
+  MB_ERR_REJECTED = 7,    /* serving: the request can never fit the admission budget */
+  MB_ERR_CANCELLED = 8    /* serving: the request was cancelled before it launched */
 } mb_status;
 
 /* Thread-local message for the last failing call on this thread. */
@@ -520,6 +522,38 @@ MB_API mb_status mb_engine_query_batch(mb_engine *e, const mb_query *qs, uint32_
                                        const mb_batch_opts *opts, int64_t *out_host,
                                        uint64_t *nqual_host);
 
+/* The launches a batch takes, planned on the host without GPU work: per
+ * batched launch its queries, the bitmap rows it stages per tile, its
+ * staging copies and its launch shape; *nalone = queries outside the batch
+ * kernel's form (they run alone on the plain path). */
+typedef struct mb_batch_launch_info {
+  uint32_t queries, staged_rows, copies;
+  uint32_t words_per_lane, warps, drain_warps, stages;
+  uint32_t pad_;
+} mb_batch_launch_info;
+MB_API mb_status mb_engine_batch_info(mb_engine *e, const mb_query *qs, uint32_t n,
+                                      const mb_batch_opts *opts, mb_batch_launch_info *launches,
+                                      uint32_t cap, uint32_t *nlaunches, uint32_t *nalone);
+
+/* A batch captured once as a CUDA graph (its descriptors stay resident on
+ * the device), replayed by mb_batch_graph_launch on the engine stream with
+ * the same outputs: for a query mix that repeats, each replay is one graph
+ * launch with no host planning or descriptor copy. */
+typedef struct mb_batch_graph mb_batch_graph;
+MB_API mb_status mb_batch_graph_create(mb_engine *e, const mb_query *qs, uint32_t n,
+                                       const mb_batch_opts *opts, int64_t *out_dev,
+                                       uint64_t *nqual_dev, mb_batch_graph **out);
+MB_API mb_status mb_batch_graph_launch(mb_batch_graph *g);
+MB_API mb_status mb_batch_graph_destroy(mb_batch_graph *g);
+
+/* Autotuner of the batched scan's launch shape for a query mix: times the
+ * mix (median of reps launches, CUDA events on the engine stream) over tile
+ * widths x warps, then drain warps, then L2 prefetch, each stage keeping the
+ * best so far; *best receives the fastest options, *best_ms its time,
+ * *tried the shapes timed. */
+MB_API mb_status mb_engine_tune_batch(mb_engine *e, const mb_query *qs, uint32_t n, uint32_t reps,
+                                      mb_batch_opts *best, float *best_ms, uint32_t *tried);
+
 /* ------------------------------------------------------------------------
  * Learned planner.  No counterpart in the reference, whose programs come from
  * fixed rules (col::from_bin / from_bin2, bmpidx_create.cu:138-226).
@@ -579,6 +613,93 @@ MB_API mb_status mb_engine_set_planner(mb_engine *e, mb_mlp *m);
  * index (may be NULL).  Without a network: the rule plan. */
 MB_API mb_status mb_engine_plan_learned(mb_engine *e, const mb_query *qs, uint32_t n, mb_plan *plans,
                                         uint32_t *chosen);
+
+/* ------------------------------------------------------------------------
+ * Serving loop.  No counterpart in the reference (its drivers run a fixed
+ * list of queries once, ssb/ssbdemo.cu).
+ *
+ * A server owns a dispatcher thread over one engine whose columns and index
+ * stay resident.  Requests queue on submission; whenever fewer than
+ * max_inflight launches are on the GPU, the dispatcher launches every queued
+ * request that fits (continuous batching: up to max_batch queries per
+ * persistent batched-scan launch, or one query per launch in plain mode).
+ * Admission: a request reserves its group table (8 bytes per group plus its
+ * row count) and the intermediate bitmaps its plan writes; requests wait
+ * while the reservations in flight would exceed mem_budget and are rejected
+ * (MB_ERR_REJECTED) if theirs alone does.  Group tables live in a device
+ * arena of mem_budget bytes and are copied back to the caller's buffer when
+ * their launch completes.  While a server runs, its engine belongs to the
+ * dispatcher thread: make no other call on that engine until
+ * mb_server_destroy. */
+typedef struct mb_server mb_server;
+typedef enum mb_serve_mode {
+  MB_SERVE_BATCHED = 0,     /* batched scan, up to max_batch queries per launch */
+  MB_SERVE_PLAIN = 1        /* one query per launch sequence */
+} mb_serve_mode;
+typedef struct mb_server_opts {
+  uint64_t mem_budget;      /* admission bytes and arena size (0 = 256 MiB) */
+  uint32_t mode;            /* mb_serve_mode */
+  uint32_t max_batch;       /* 1..MB_BATCH_MAX (0 = 64) */
+  uint32_t max_inflight;    /* launches on the GPU at once, 1..8 (0 = 2) */
+  uint32_t use_planner;     /* plan with the engine's learned planner (mb_engine_set_planner) */
+  uint32_t min_batch;       /* batched mode: launches of fewer queries run them on the plain
+                               path, one after another (0 = 6; 1 = always the batched scan) */
+  uint32_t pad_;
+  mb_batch_opts batch;      /* batched-scan launch shape */
+} mb_server_opts;
+typedef struct mb_request_info {
+  int32_t status;           /* MB_OK, MB_ERR_REJECTED, MB_ERR_CANCELLED or the launch's error */
+  uint32_t launch;          /* index of the launch that ran it */
+  uint32_t batch_size;      /* queries in that launch */
+  uint32_t plan;            /* candidate plan index (plain mode with the planner; else 0) */
+  uint64_t nqual;           /* qualifying rows */
+  double t_submit_us;       /* times since the server started */
+  double t_launch_us;       /* the dispatcher enqueued its launch */
+  double t_done_us;         /* its results were in the caller's buffer */
+  float gpu_ms;             /* device time of its launch */
+  float pad_;
+} mb_request_info;
+typedef struct mb_server_stats {
+  uint64_t submitted, completed, rejected, cancelled, failed;
+  uint64_t launches, launched_queries;
+  uint64_t peak_reserved;   /* largest admission reservation in flight (bytes) */
+  double gpu_ms;            /* sum of launch device times */
+} mb_server_stats;
+MB_API mb_status mb_server_create(mb_engine *e, const mb_server_opts *opts, mb_server **out);
+/* Stops accepting requests, finishes the launches in flight (queued requests
+ * complete as MB_ERR_CANCELLED) and joins the dispatcher. */
+MB_API mb_status mb_server_destroy(mb_server *s);
+/* Queues a query; out_host (mb_query_ngroups(q) int64 values) receives its
+ * group sums.  *id identifies it for wait and cancel. */
+MB_API mb_status mb_server_submit(mb_server *s, const mb_query *q, int64_t *out_host, uint64_t *id);
+/* Cancels a request that has not launched yet (MB_ERR_INVALID if it has
+ * launched or finished: its results arrive as usual). */
+MB_API mb_status mb_server_cancel(mb_server *s, uint64_t id);
+/* Waits up to timeout_ms (< 0: without limit) for a request, fills *info
+ * and forgets the request.  MB_ERR_TIMEOUT if it is not done in time. */
+MB_API mb_status mb_server_wait(mb_server *s, uint64_t id, int64_t timeout_ms, mb_request_info *info);
+MB_API mb_status mb_server_get_stats(mb_server *s, mb_server_stats *out);
+/* Open-loop load: submits qs[i] at Poisson arrival times of rate_qps (the
+ * arrivals of mb_poisson_arrivals(seed, ...)), waits for every request and
+ * fills out_host (layout of mb_queries_layout) and info[i]. */
+MB_API mb_status mb_server_run_load(mb_server *s, const mb_query *qs, uint32_t n, double rate_qps, uint64_t seed,
+                                    int64_t *out_host, mb_request_info *info);
+/* Arrival times (microseconds from 0) of n Poisson arrivals at rate_qps:
+ * exponential gaps by inversion of a counter-based uniform (SplitMix64 of
+ * seed and i).  Host only. */
+MB_API mb_status mb_poisson_arrivals(uint64_t seed, double rate_qps, uint32_t n, double *t_us);
+
+/* Host-side fault injection for the serving loop (no GPU fault is made):
+ * the next `count` launches fail their arena allocation (MB_ERR_OOM), fail
+ * their enqueue as a CUDA error would (MB_ERR_CUDA), or are held on the host
+ * for arg_us microseconds before they launch (a slow query). */
+typedef enum mb_fault {
+  MB_FAULT_NONE = 0,
+  MB_FAULT_ALLOC = 1,
+  MB_FAULT_LAUNCH = 2,
+  MB_FAULT_SLOW = 3
+} mb_fault;
+MB_API mb_status mb_server_inject(mb_server *s, uint32_t fault, uint32_t count, uint32_t arg_us);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -19,9 +19,10 @@ MB_MAXTERM = 16
 MB_MAXKEY = 4
 
 # mb_status
-MB_OK, MB_ERR_INVALID, MB_ERR_OOM, MB_ERR_CUDA, MB_ERR_TIMEOUT, MB_ERR_UNSUPPORTED, MB_ERR_IO = range(7)
+(MB_OK, MB_ERR_INVALID, MB_ERR_OOM, MB_ERR_CUDA, MB_ERR_TIMEOUT, MB_ERR_UNSUPPORTED, MB_ERR_IO, MB_ERR_REJECTED,
+ MB_ERR_CANCELLED) = range(9)
 STATUS_NAMES = ["MB_OK", "MB_ERR_INVALID", "MB_ERR_OOM", "MB_ERR_CUDA", "MB_ERR_TIMEOUT",
-                "MB_ERR_UNSUPPORTED", "MB_ERR_IO"]
+                "MB_ERR_UNSUPPORTED", "MB_ERR_IO", "MB_ERR_REJECTED", "MB_ERR_CANCELLED"]
 
 # mb_opcode (the reference's enum ops, primitive.cuh:169-173)
 END, AND, OR, NOT, ANDM, ORM = range(6)
@@ -124,6 +125,11 @@ class mb_batch_opts(C.Structure):
                 ("pad_", C.c_uint32 * 2)]
 
 
+class mb_batch_launch_info(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("queries", "staged_rows", "copies", "words_per_lane", "warps",
+                                          "drain_warps", "stages", "pad_")]
+
+
 class mb_plan(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("order_mode", C.c_uint32), ("materialise", C.c_uint32),
                 ("launch", mb_launch)]
@@ -140,6 +146,27 @@ class mb_mlp_config(C.Structure):
 class mb_mlp_train_opts(C.Structure):
     _fields_ = [("epochs", C.c_uint32), ("batch", C.c_uint32), ("lr", C.c_float), ("beta1", C.c_float),
                 ("beta2", C.c_float), ("seed", C.c_uint32)]
+
+
+SERVE_BATCHED, SERVE_PLAIN = range(2)
+FAULT_NONE, FAULT_ALLOC, FAULT_LAUNCH, FAULT_SLOW = range(4)
+
+
+class mb_server_opts(C.Structure):
+    _fields_ = [("mem_budget", C.c_uint64), ("mode", C.c_uint32), ("max_batch", C.c_uint32),
+                ("max_inflight", C.c_uint32), ("use_planner", C.c_uint32), ("min_batch", C.c_uint32),
+                ("pad_", C.c_uint32), ("batch", mb_batch_opts)]
+
+
+class mb_request_info(C.Structure):
+    _fields_ = [("status", C.c_int32), ("launch", C.c_uint32), ("batch_size", C.c_uint32), ("plan", C.c_uint32),
+                ("nqual", C.c_uint64), ("t_submit_us", C.c_double), ("t_launch_us", C.c_double),
+                ("t_done_us", C.c_double), ("gpu_ms", C.c_float), ("pad_", C.c_float)]
+
+
+class mb_server_stats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "rejected", "cancelled", "failed", "launches",
+                                          "launched_queries", "peak_reserved")] + [("gpu_ms", C.c_double)]
 
 
 class mb_query_stats(C.Structure):
@@ -212,6 +239,24 @@ SIGNATURES: dict[str, tuple] = {
     "mb_engine_plan_candidate": (I32, [VOIDP, C.POINTER(mb_query), U32, C.POINTER(mb_plan)]),
     "mb_engine_set_planner": (I32, [VOIDP, VOIDP]),
     "mb_engine_plan_learned": (I32, [VOIDP, C.POINTER(mb_query), U32, C.POINTER(mb_plan), VOIDP]),
+    "mb_engine_batch_info": (I32, [VOIDP, C.POINTER(mb_query), U32, C.POINTER(mb_batch_opts),
+                                   C.POINTER(mb_batch_launch_info), U32, C.POINTER(U32), C.POINTER(U32)]),
+    "mb_batch_graph_create": (I32, [VOIDP, C.POINTER(mb_query), U32, C.POINTER(mb_batch_opts), VOIDP, VOIDP,
+                                    C.POINTER(VOIDP)]),
+    "mb_batch_graph_launch": (I32, [VOIDP]),
+    "mb_batch_graph_destroy": (I32, [VOIDP]),
+    "mb_engine_tune_batch": (I32, [VOIDP, C.POINTER(mb_query), U32, U32, C.POINTER(mb_batch_opts),
+                                   C.POINTER(C.c_float), C.POINTER(U32)]),
+    "mb_server_create": (I32, [VOIDP, C.POINTER(mb_server_opts), C.POINTER(VOIDP)]),
+    "mb_server_destroy": (I32, [VOIDP]),
+    "mb_server_submit": (I32, [VOIDP, C.POINTER(mb_query), VOIDP, C.POINTER(U64)]),
+    "mb_server_cancel": (I32, [VOIDP, U64]),
+    "mb_server_wait": (I32, [VOIDP, U64, C.c_int64, C.POINTER(mb_request_info)]),
+    "mb_server_get_stats": (I32, [VOIDP, C.POINTER(mb_server_stats)]),
+    "mb_server_run_load": (I32, [VOIDP, C.POINTER(mb_query), U32, C.c_double, U64, VOIDP,
+                                 C.POINTER(mb_request_info)]),
+    "mb_poisson_arrivals": (I32, [U64, C.c_double, U32, VOIDP]),
+    "mb_server_inject": (I32, [VOIDP, U32, U32, U32]),
     "mb_gen_flat": (I32, [U64, U64, U64, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP]),
     "mb_gen_star": (I32, [U64, U32, U64, U64, I32, C.POINTER(mb_star_cols), VOIDP]),
     "mb_gen_star_dims": (I32, [U64, U32, VOIDP, VOIDP, VOIDP, VOIDP]),

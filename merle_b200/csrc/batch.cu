@@ -9,10 +9,11 @@
 // A CTA's warps split into producers and consumers.
 //
 // Producers walk the CTA's row tiles (T = 32 * V words), S tiles of the
-// bitmaps in flight: the index is one slab of bitmap rows, so one thread
-// stages a tile of the whole run of rows the batch reads with a single 2-D
-// tensor copy (TMA, box = rows x T words, completing on the stage's
-// mbarrier) and prefetches the tile's payload rows into L2.  On a tile,
+// bitmaps in flight: the index is one slab of bitmap rows, so a tile of the
+// rows the batch reads is staged by one 2-D tensor copy per run of rows
+// (TMA, box = run x T words, all completing on the stage's mbarrier; the
+// copies are issued by lane 0 of every producer warp in turn) and the tile's
+// payload rows are prefetched into L2.  On a tile,
 // producers take the batch's queries off a counter, costliest first; for its
 // query a producer evaluates the conjunctive chain on the staged words and
 // appends the selected rows to the query's own row queue.  Every 64 queued
@@ -35,6 +36,8 @@
 // and lets its copies land before exiting.
 #include <cudaTypedefs.h>
 #include <string.h>
+#include <mutex>
+#include <vector>
 #include "batch.cuh"
 #include "opeval.cuh"
 #include "tma.cuh"
@@ -96,9 +99,12 @@ __host__ __device__ inline BLayout blayout(uint32_t nq, uint32_t nchain, uint32_
 
 struct BParams {
   uint64_t nrows, nwords;
-  uint32_t nq, nu, urow0, nsrc, nchain, pf_mask, S, np;  // np: producer warps
+  uint32_t nq, nu, nsrc, nchain, pf_mask, S, np;  // np: producer warps
+  uint32_t ncopy;
+  uint32_t copy[BCP_MAX];  // BatchHdr::copy
   BLayout L;
 };
+
 
 // The batch's tables as a warp sees them (shared memory).
 struct BCtx {
@@ -469,7 +475,7 @@ __device__ __forceinline__ void lds_words(const uint32_t *p, uint32_t (&x)[V]) {
 // into the query's queue; every 64 become a job.
 template <int V>
 __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, const uint32_t *stage, uint64_t w0,
-                                        uint64_t nwords, uint32_t tail, uint32_t urow0, uint32_t q, uint32_t *queue,
+                                        uint64_t nwords, uint32_t tail, uint32_t q, uint32_t *queue,
                                         uint32_t *qlen) {
   constexpr uint32_t T = 32 * V;
   const uint32_t lane = threadIdx.x & 31;
@@ -489,8 +495,7 @@ __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, co
     // middle bins four at a time: the indices, then the words, then the ORs
     uint32_t j = 0;
     for (; j + 4 <= nm; j += 4, i += 4) {
-      const uint32_t b0 = chain[c0 + i] - urow0, b1 = chain[c0 + i + 1] - urow0, b2 = chain[c0 + i + 2] - urow0,
-                     b3 = chain[c0 + i + 3] - urow0;
+      const uint32_t b0 = chain[c0 + i], b1 = chain[c0 + i + 1], b2 = chain[c0 + i + 2], b3 = chain[c0 + i + 3];
       uint32_t x0[V], x1[V], x2[V], x3[V];
       lds_words<V>(sl + b0 * T, x0);
       lds_words<V>(sl + b1 * T, x1);
@@ -501,13 +506,13 @@ __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, co
     }
     for (; j < nm; ++j) {
       uint32_t x[V];
-      lds_words<V>(sl + (chain[c0 + i++] - urow0) * T, x);
+      lds_words<V>(sl + chain[c0 + i++] * T, x);
 #pragma unroll
       for (int k = 0; k < V; ++k) cm[k] |= x[k];
     }
     for (uint32_t j2 = 0; j2 < ne; ++j2) {
       uint32_t x[V];
-      lds_words<V>(sl + (chain[c0 + i++] - urow0) * T, x);
+      lds_words<V>(sl + chain[c0 + i++] * T, x);
 #pragma unroll
       for (int k = 0; k < V; ++k) cx[k] |= x[k];
     }
@@ -596,7 +601,7 @@ __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, co
 template <int V>
 __global__ void __launch_bounds__(BT_THREADS_MAX, 1)
 batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParams P,
-                  const __grid_constant__ CUtensorMap tmap, unsigned long long *__restrict__ out,
+                  const CUtensorMap *__restrict__ maps, unsigned long long *__restrict__ out,
                   unsigned long long *__restrict__ nqual, uint32_t *errw) {
   constexpr uint32_t T = 32 * V;
   extern __shared__ __align__(128) uint8_t smem[];
@@ -650,17 +655,25 @@ batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParam
 
   const uint64_t ntiles = (P.nwords + T - 1) / T;
   const uint64_t nit = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  // stage j % S <- the CTA's j-th tile: one tensor copy (thread 0) of rows
-  // [urow0, urow0 + nu) x T words, zeros past the table's end; the payload
-  // rows of the tile into L2 (threads < nsrc)
+  // stage j % S <- the CTA's j-th tile: the tensor copies of the staged
+  // rows x T words (copy c by lane 0 of producer warp c % np; thread 0 sets
+  // the stage's byte count, and a copy landing before that only takes the
+  // count below zero for a while), zeros past the table's end; the payload
+  // rows of the tile into L2 (threads < nsrc).  Called by every producer.
   auto fill = [&](uint64_t j) {
     const uint32_t s = (uint32_t)(j % P.S);
     const uint64_t w0 = ((uint64_t)blockIdx.x + j * gridDim.x) * T;
-    if (tid == 0) {
-      ++*issued;
+    if (lane == 0) {
+      if (warp == 0) {
+        ++*issued;
+        mbar_arrive_expect_tx(&full[s], P.nu * T * 4);
+      }
       fence_proxy_async_smem();
-      mbar_arrive_expect_tx(&full[s], P.nu * T * 4);
-      tma_load_2d(stages + (size_t)s * P.nu * T, &tmap, (int)w0, (int)P.urow0, &full[s]);
+      uint32_t *dst = stages + (size_t)s * P.nu * T;
+      for (uint32_t c = warp; c < P.ncopy; c += np) {
+        const uint32_t e = P.copy[c];
+        tma_load_2d(dst + ((e >> 12) & 0xfffu) * T, maps + (e >> 24), (int)w0, (int)(e & 0xfffu), &full[s]);
+      }
     }
     if (tid < P.nsrc && ((P.pf_mask >> tid) & 1u)) {
       const uint64_t r0 = w0 * 32;
@@ -694,7 +707,7 @@ batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParam
         qi = __shfl_sync(0xffffffffu, qi, 0);
         if (qi >= P.nq) break;
         const uint32_t q = order[qi];
-        b_query<V>(C, chain, st, w0, P.nwords, tail, P.urow0, q, qbuf + (size_t)q * BQQ, &qlen[q]);
+        b_query<V>(C, chain, st, w0, P.nwords, tail, q, qbuf + (size_t)q * BQQ, &qlen[q]);
       }
       pbar();  // the stage is consumed: refill it
       if (it + P.S < nit) fill(it + P.S);
@@ -763,8 +776,10 @@ size_t batch_smem(const BatchHdr &h, const BatchCfg &c) {
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against the driver library).
-static mb_status encode_tmap(const BatchHdr &h, uint32_t T, CUtensorMap *map) {
+mb_status batch_encode_maps(const uint32_t *slab, uint64_t stride, uint32_t nslab, uint32_t T, void *host_maps) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
   if (!encode) {
     void *fn = nullptr;
     cudaDriverEntryPointQueryResult q;
@@ -772,29 +787,34 @@ static mb_status encode_tmap(const BatchHdr &h, uint32_t T, CUtensorMap *map) {
     if (q != cudaDriverEntryPointSuccess || !fn) return fail(MB_ERR_CUDA, "batch: cuTensorMapEncodeTiled not found");
     encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
-  const cuuint64_t dim[2] = {h.stride, h.nslab};
-  const cuuint64_t gstride[1] = {h.stride * 4};
-  const cuuint32_t box[2] = {T, h.nu};
+  static_assert(sizeof(CUtensorMap) == BMAP_BYTES, "tensor map size");
+  if (T == 0 || T > 256 || (T * 4) % 16 != 0 || ((uintptr_t)slab & 15) != 0 || (stride * 4) % 16 != 0)
+    return fail(MB_ERR_INVALID, "batch: tensor map shape (T %u, stride %llu)", T, (unsigned long long)stride);
+  CUtensorMap *m = static_cast<CUtensorMap *>(host_maps);
+  const cuuint64_t dim[2] = {stride, nslab};
+  const cuuint64_t gstride[1] = {stride * 4};
   const cuuint32_t estride[2] = {1, 1};
-  const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<uint32_t *>(h.slab), dim, gstride, box,
-                            estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return fail(MB_ERR_CUDA, "batch: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  for (uint32_t h = 1; h <= BMAP_COUNT; ++h) {
+    const cuuint32_t box[2] = {T, h};
+    const CUresult r = encode(&m[h - 1], CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<uint32_t *>(slab), dim,
+                              gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(MB_ERR_CUDA, "batch: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  }
   return MB_OK;
 }
 
 template <int V>
-static mb_status launch_bs(const BatchHdr &h, const BatchHdr *dh, const BatchCfg &c, int64_t *out, uint64_t *nqual,
-                           cudaStream_t st) {
+static mb_status launch_bs(const BatchHdr &h, const BatchHdr *dh, const BatchCfg &c, const void *maps, int64_t *out,
+                           uint64_t *nqual, cudaStream_t st) {
   auto kern = batch_scan_kernel<V>;
-  CUtensorMap tmap;
-  MB_CHECK(encode_tmap(h, 32 * V, &tmap));
   BParams P;
   P.nrows = h.nrows;
   P.nwords = h.nwords;
   P.nq = h.nq;
   P.nu = h.nu;
-  P.urow0 = h.urow0;
+  P.ncopy = h.ncopy;
+  memcpy(P.copy, h.copy, sizeof(P.copy));
   P.nsrc = h.nsrc;
   P.nchain = h.nchain;
   P.pf_mask = h.pf_mask;
@@ -814,26 +834,40 @@ static mb_status launch_bs(const BatchHdr &h, const BatchHdr *dh, const BatchCfg
   if (grid > ntiles) grid = ntiles;
   uint32_t *errw = device_error_word();
   if (!errw) return fail(MB_ERR_OOM, "batch: device error word");
-  kern<<<(unsigned)grid, c.warps * 32, smem, st>>>(dh, P, tmap, reinterpret_cast<unsigned long long *>(out),
+  kern<<<(unsigned)grid, c.warps * 32, smem, st>>>(dh, P, static_cast<const CUtensorMap *>(maps), reinterpret_cast<unsigned long long *>(out),
                                                    reinterpret_cast<unsigned long long *>(nqual), errw);
   MB_LAUNCH_CHECK("batch_scan_kernel");
   return MB_OK;
 }
 
-mb_status batch_scan(const BatchHdr &h, const BatchHdr *dh, const BatchCfg &c, int64_t *out, uint64_t *nqual,
-                     cudaStream_t st) {
+mb_status batch_scan(const BatchHdr &h, const BatchHdr *dh, const BatchCfg &c, const void *maps, int64_t *out,
+                     uint64_t *nqual, cudaStream_t st) {
   if (h.nq == 0 || h.nrows == 0) return MB_OK;
   if (h.nq > BQ_MAX || h.nu > BU_MAX || h.nsrc > BS_MAX || h.nchain > BC_MAX)
     return fail(MB_ERR_INVALID, "batch: descriptor over its limits");
-  if (h.stride % 32 != 0 || h.stride < h.nwords || ((uintptr_t)h.slab & 15) != 0 || h.urow0 + h.nu > h.nslab)
-    return fail(MB_ERR_INVALID, "batch: bitmap slab (stride %llu, rows %u..%u of %u)", (unsigned long long)h.stride,
-                h.urow0, h.urow0 + h.nu, h.nslab);
+  if (h.stride % 32 != 0 || h.stride < h.nwords || ((uintptr_t)h.slab & 15) != 0 || h.nslab > 4096 ||
+      h.nrows >= (1ull << 31))
+    return fail(MB_ERR_INVALID, "batch: bitmap slab (stride %llu, %u rows) over %llu table rows",
+                (unsigned long long)h.stride, h.nslab, (unsigned long long)h.nrows);
+  // the copies must tile stage rows [0, nu) exactly, from rows of the slab
+  if (h.nu == 0 || h.ncopy == 0 || h.ncopy > BCP_MAX) return fail(MB_ERR_INVALID, "batch: %u staging copies", h.ncopy);
+  if (!maps || ((uintptr_t)maps & 63) != 0) return fail(MB_ERR_INVALID, "batch: tensor maps not 64-byte aligned");
+  {
+    uint32_t next = 0;
+    for (uint32_t i = 0; i < h.ncopy; ++i) {
+      const uint32_t e = h.copy[i], r0 = e & 0xfffu, t0 = (e >> 12) & 0xfffu, hh = (e >> 24) + 1;
+      if (t0 != next || r0 + hh > h.nslab)
+        return fail(MB_ERR_INVALID, "batch: staging copy %u (rows %u+%u to %u)", i, r0, hh, t0);
+      next = t0 + hh;
+    }
+    if (next != h.nu) return fail(MB_ERR_INVALID, "batch: staging copies cover %u of %u rows", next, h.nu);
+  }
   if (batch_smem(h, c) == 0) return fail(MB_ERR_INVALID, "batch: launch shape V=%u warps=%u stages=%u", c.V,
                                          c.warps, c.stages);
   switch (c.V) {
-  case 4: return launch_bs<4>(h, dh, c, out, nqual, st);
-  case 2: return launch_bs<2>(h, dh, c, out, nqual, st);
-  default: return launch_bs<1>(h, dh, c, out, nqual, st);
+  case 4: return launch_bs<4>(h, dh, c, maps, out, nqual, st);
+  case 2: return launch_bs<2>(h, dh, c, maps, out, nqual, st);
+  default: return launch_bs<1>(h, dh, c, maps, out, nqual, st);
   }
 }
 

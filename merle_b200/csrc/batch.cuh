@@ -4,13 +4,13 @@
 //
 // Per row tile (T = 32 * V words = 1024 * V rows) a CTA stages the tile of
 // every DISTINCT bitmap the batch reads (the union: each word fetched from
-// HBM once per batch instead of once per query) and prefetches into L2 the
-// tile's rows of every payload column the batch's ops read densely.  The
-// CTA's warps then take the batch's queries off a counter, costliest first,
-// evaluate each query's conjunctive chain from shared memory and append the
-// selected rows of all queries to one tile-wide row list; the ops then run
-// over that list in 64-row chunks, so every query of the batch gathers from
-// the same prefetched payload lines.
+// HBM once per batch instead of once per query) with a few 2-D tensor copies
+// of runs of index-slab rows, and prefetches into L2 the tile's rows of the
+// payload columns the batch's ops read densely.  Producer warps take the
+// batch's queries off a counter, costliest first, evaluate each query's
+// conjunctive chain on the staged words and queue its selected rows; every
+// 64 queued rows of a query become a job that consumer warps run through the
+// query's op (batch.cu).
 //
 // The op of a batch query is its mb_op restated per source slot: the
 // intersected bounds of the single-term clauses on the slot (re-checked for
@@ -24,7 +24,8 @@
 namespace mb {
 
 constexpr uint32_t BQ_MAX = 128;   // queries per launch (7-bit query field of a row entry)
-constexpr uint32_t BU_MAX = 256;   // bitmap rows staged per tile (a tensor-copy box side)
+constexpr uint32_t BU_MAX = 256;   // bitmap rows staged per tile
+constexpr uint32_t BCP_MAX = 48;   // tensor copies per tile
 constexpr uint32_t BS_MAX = 16;    // distinct op sources per launch
 constexpr uint32_t BC_MAX = 4096;  // chain entries per launch
 constexpr uint32_t BW_MAX = 16;    // warps per CTA
@@ -51,8 +52,6 @@ struct BatchSrc {
 //     [5] key multiplier  [6] divisor
 enum : uint32_t { BQD_SLOT0 = 8, BQD_SLOTW = 7, BQD_WORDS = 8 + 7 * BSLOT };
 
-// The bitmaps are rows of one slab (`stride` words apart); a batch stages
-// rows [urow0, urow0 + nu) of every tile.
 // Op shapes with a compiled drain: which slots every row loads (kv), which
 // only uncertain rows load (filt), which are group-key slots and their
 // transform (2 bits per slot: 0 identity, 1 division, 2 year), the value
@@ -79,13 +78,16 @@ struct BatchHdr {
   uint64_t stride;       // words per slab row: a multiple of 32, >= nwords
   const uint32_t *slab;
   uint32_t nslab;        // rows of the slab
-  uint32_t urow0, nu;    // the staged run of rows
+  uint32_t nu;           // rows staged per tile
   uint32_t nq, nsrc, nchain;
   uint32_t pf_mask;      // bit i: prefetch source i's row-indexed column into L2
-  uint32_t pad_;
+  uint32_t ncopy;
+  // The staging copies of a tile: slab rows [r0, r0 + h) to stage rows
+  // [t0, t0 + h), packed r0 | t0 << 12 | (h - 1) << 24 (1 <= h <= 256).
+  uint32_t copy[BCP_MAX];
   BatchSrc src[BS_MAX];
   uint32_t Qd[BQ_MAX * BQD_WORDS];
-  uint16_t chain[BC_MAX];  // per conjunct: header, then slab rows (batch_add)
+  uint16_t chain[BC_MAX];  // per conjunct: header, then stage rows (batch_add, batch_flush)
   uint8_t order[BQ_MAX];   // the order in which warps take the queries (costliest first)
 };
 
@@ -98,10 +100,18 @@ struct BatchCfg {
   uint32_t cps;     // CTAs per SM (0: as many as fit)
 };
 
+// Tensor maps of a bitmap slab for one tile width T (words): map h - 1 has
+// a box of T words x h rows, h = 1..BU_MAX.  A staging copy of h rows uses
+// map h - 1, so every run of rows is one copy.
+constexpr uint32_t BMAP_COUNT = BU_MAX;
+constexpr size_t BMAP_BYTES = 128;  // sizeof(CUtensorMap)
+mb_status batch_encode_maps(const uint32_t *slab, uint64_t stride, uint32_t nslab, uint32_t T, void *host_maps);
+
 // Launches the batched scan over the header at dh (device copy of h, which
-// the host keeps for the sizes); out / nqual are zeroed by the caller.
-mb_status batch_scan(const BatchHdr &h, const BatchHdr *dh, const BatchCfg &cfg, int64_t *out, uint64_t *nqual,
-                     cudaStream_t st);
+// the host keeps for the sizes) with the slab's maps for T = 32 * cfg.V in
+// device memory at maps; out / nqual are zeroed by the caller.
+mb_status batch_scan(const BatchHdr &h, const BatchHdr *dh, const BatchCfg &cfg, const void *maps, int64_t *out,
+                     uint64_t *nqual, cudaStream_t st);
 
 // Shared-memory bytes of a launch (0 if the configuration is invalid).
 size_t batch_smem(const BatchHdr &h, const BatchCfg &cfg);

@@ -12,6 +12,7 @@
 // choosing by the bytes each option reads.
 #include <string.h>
 #include <algorithm>
+#include <memory>
 #include <unordered_map>
 #include "batch.cuh"
 #include "engine.h"
@@ -44,6 +45,15 @@ mb_status Engine::alloc(void **p, size_t bytes) {
   return MB_OK;
 }
 
+static void free_one(std::vector<void *> &allocs, void *p);
+
+void Engine::free_bmaps() {
+  for (void *&m : bmaps) {
+    free_one(allocs, m);
+    m = nullptr;
+  }
+}
+
 static void free_one(std::vector<void *> &allocs, void *p) {
   if (!p) return;
   auto it = std::find(allocs.begin(), allocs.end(), p);
@@ -68,6 +78,7 @@ void Engine::free_star() {
     for (auto &l : c.levels) l.slab = nullptr;
   free_one(allocs, islab);
   islab = nullptr;
+  free_bmaps();
   nbm = 0;
   for (auto &c : idx) c.levels.clear();
   indexed = false;
@@ -640,6 +651,7 @@ extern "C" mb_status mb_engine_build_index_ex(mb_engine *e, uint32_t flags) {
     for (auto &l : c.levels) l.slab = nullptr;
   free_one(E.allocs, E.islab);
   E.islab = nullptr;
+  E.free_bmaps();
   E.nbm = 0;
   E.indexed = false;
   MB_CUDA(cudaEventRecord(E.ev0, E.stream));
@@ -880,9 +892,10 @@ enum { BADD_OK = 0, BADD_FULL = 1, BADD_ALONE = 2 };
 // Batch under construction: the staging header and its lookup tables.
 struct BatchBuild {
   BatchHdr *h = nullptr;
-  uint32_t umin = 0xffffffffu, umax = 0;  // slab rows the batch reads
-  std::vector<double> cost;               // estimated cost of each query (per bitmap word)
-  double src_weight[BS_MAX] = {};         // selected-row fraction reading each source
+  std::vector<uint8_t> used;  // slab rows the batch reads
+  uint32_t nused = 0;
+  std::vector<double> cost;   // estimated cost of each query (per bitmap word)
+  double src_weight[BS_MAX] = {};  // selected-row fraction reading each source
 
   void reset(BatchHdr *hh, const Engine &E) {
     h = hh;
@@ -892,11 +905,50 @@ struct BatchBuild {
     h->stride = E.stride;
     h->slab = E.islab;
     h->nslab = E.nbm;
-    umin = 0xffffffffu, umax = 0;
+    used.assign(E.nbm, 0);
+    nused = 0;
     cost.clear();
     for (double &w : src_weight) w = 0;
   }
 };
+
+// The staging of a set of slab rows: runs of rows (gaps of up to two unused
+// rows merged in: reading them costs less than issuing another copy), one
+// tensor copy per run.  Fills copy[] (BatchHdr packing) and, if stage_of is
+// given, the stage row of every used slab row; returns the rows staged, or
+// 0 if the set needs more than BU_MAX rows or BCP_MAX copies.
+static uint32_t stage_plan(const std::vector<uint8_t> &used, uint32_t *copy, uint32_t *ncopy, uint16_t *stage_of) {
+  std::vector<std::pair<uint32_t, uint32_t>> runs;  // [a, b)
+  for (uint32_t r = 0; r < used.size(); ++r) {
+    if (!used[r]) continue;
+    if (!runs.empty() && r - runs.back().second <= 2) runs.back().second = r + 1;
+    else runs.push_back({r, r + 1});
+  }
+  if (runs.empty()) runs.push_back({0, 1});  // no bitmap read: stage one row anyway
+  uint32_t staged = 0;
+  for (auto &r : runs) staged += r.second - r.first;
+  // too many copies: merge the runs with the smallest gap
+  while (runs.size() > BCP_MAX) {
+    size_t bi = 0;
+    for (size_t i = 1; i + 1 < runs.size(); ++i)
+      if (runs[i + 1].first - runs[i].second < runs[bi + 1].first - runs[bi].second) bi = i;
+    staged += runs[bi + 1].first - runs[bi].second;
+    runs[bi].second = runs[bi + 1].second;
+    runs.erase(runs.begin() + bi + 1);
+  }
+  if (staged > BU_MAX) return 0;
+  uint32_t t = 0, c = 0;
+  for (auto &r : runs) {
+    const uint32_t h = r.second - r.first;
+    if (stage_of)
+      for (uint32_t x = r.first; x < r.second; ++x) stage_of[x] = (uint16_t)(t + x - r.first);
+    if (copy) copy[c] = r.first | (t << 12) | ((h - 1) << 24);
+    ++c;
+    t += h;
+  }
+  if (ncopy) *ncopy = c;
+  return staged;
+}
 
 // Row of the index slab holding bitmap p, or -1.
 static int64_t slab_row(const BatchHdr &h, const uint32_t *p) {
@@ -998,13 +1050,12 @@ static int batch_add(BatchBuild &B, const Lowered &L, const DevPrg &P, uint64_t 
   uint32_t d[BQD_WORDS];
   memset(d, 0, sizeof(d));
   if (!slot_plan(O, d)) return BADD_ALONE;
-  // the slab rows this query reads
-  uint32_t rmin = B.umin, rmax = B.umax;
+  // the slab rows this query reads, added to the batch's
+  std::vector<uint32_t> fresh;
   for (uint32_t i = 0; i < P.ncnf; ++i) {
     const int64_t r = slab_row(h, P.cnf_ptr[i]);
     if (r < 0) return BADD_ALONE;
-    rmin = std::min(rmin, (uint32_t)r);
-    rmax = std::max(rmax, (uint32_t)r);
+    if (!B.used[r] && std::find(fresh.begin(), fresh.end(), (uint32_t)r) == fresh.end()) fresh.push_back((uint32_t)r);
   }
   uint32_t newsrc = 0;
   for (uint32_t s = 0; s < O.nsrc; ++s) {
@@ -1013,12 +1064,22 @@ static int batch_add(BatchBuild &B, const Lowered &L, const DevPrg &P, uint64_t 
     if (!seen) ++newsrc;
   }
   const uint32_t nch = P.ncnf + MB_MAXCOLS;  // entries + at most one header per operand
-  const bool spans = P.ncnf && rmax - rmin + 1 > BU_MAX;
-  if (newsrc > BS_MAX || nch > BC_MAX || (spans && B.umin == 0xffffffffu)) return BADD_ALONE;
-  if (h.nq + 1 > BQ_MAX || spans || h.nsrc + newsrc > BS_MAX || h.nchain + nch > BC_MAX) return BADD_FULL;
+  bool stages_ok = true;
+  if (!fresh.empty()) {
+    for (uint32_t r : fresh) B.used[r] = 1;
+    stages_ok = stage_plan(B.used, nullptr, nullptr, nullptr) != 0;
+    if (!stages_ok)
+      for (uint32_t r : fresh) B.used[r] = 0;
+  }
+  if (newsrc > BS_MAX || nch > BC_MAX || (!stages_ok && B.nused == 0)) return BADD_ALONE;
+  if (h.nq + 1 > BQ_MAX || !stages_ok || h.nsrc + newsrc > BS_MAX || h.nchain + nch > BC_MAX) {
+    if (stages_ok)
+      for (uint32_t r : fresh) B.used[r] = 0;
+    return BADD_FULL;
+  }
+  B.nused += (uint32_t)fresh.size();
   // commit
   const uint32_t q = h.nq++;
-  if (P.ncnf) B.umin = rmin, B.umax = rmax;
   const OpNeeds N = op_needs(O);
   for (uint32_t s = 0; s < O.nsrc; ++s) {
     int t = src_slot(h, O.src[s]);
@@ -1038,7 +1099,8 @@ static int batch_add(BatchBuild &B, const Lowered &L, const DevPrg &P, uint64_t 
   d[2] = (uint32_t)out_off;
   d[3] = nq_slot;
   // the chain: per conjunct a header (middle bins | edge bins << 8 | negated
-  // << 15), then the union indices of its middle bins and of its edge bins
+  // << 15), then the slab rows of its middle bins and of its edge bins (made
+  // stage rows by batch_flush)
   const uint32_t c0 = h.nchain;
   for (uint32_t i = 0; i < P.ncnf;) {
     uint32_t j = i;
@@ -1087,18 +1149,29 @@ static BatchCfg batch_cfg(const BatchHdr &h, const mb_batch_opts &o) {
   return c;
 }
 
-// Orders the batch's queries, copies its header to the device and launches
-// the scan.
-static mb_status batch_flush(Engine &E, BatchBuild &B, const mb_batch_opts &o, int64_t *out, uint64_t *nq,
-                             uint32_t slot) {
+// Completes a batch's header: the order of its queries, its staging copies
+// (the chain's slab rows become stage rows), its L2 prefetches, and its
+// launch shape.
+static mb_status batch_finish(BatchBuild &B, const mb_batch_opts &o, BatchCfg *cfg) {
   BatchHdr &h = *B.h;
-  if (h.nq == 0) return MB_OK;
   std::vector<uint32_t> order(h.nq);
   for (uint32_t q = 0; q < h.nq; ++q) order[q] = q;
   std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return B.cost[a] > B.cost[b]; });
   for (uint32_t i = 0; i < h.nq; ++i) h.order[i] = (uint8_t)order[i];
-  if (B.umin == 0xffffffffu) h.urow0 = 0, h.nu = 1;  // no bitmap read: stage one row anyway
-  else h.urow0 = B.umin, h.nu = B.umax - B.umin + 1;
+  std::vector<uint16_t> stage_of(h.nslab ? h.nslab : 1, 0xffffu);
+  h.nu = stage_plan(B.used, h.copy, &h.ncopy, stage_of.data());
+  if (h.nu == 0) return fail(MB_ERR_INVALID, "batch: staging plan over its limits");
+  for (uint32_t q = 0; q < h.nq; ++q) {
+    const uint32_t c0 = h.Qd[(size_t)q * BQD_WORDS + 4] & 0xffffu, n = h.Qd[(size_t)q * BQD_WORDS + 4] >> 16;
+    for (uint32_t i = c0; i < c0 + n;) {
+      const uint32_t hd = h.chain[i++], m = (hd & 0xffu) + ((hd >> 8) & 0x7fu);
+      for (uint32_t k = 0; k < m; ++k, ++i) {
+        const uint16_t t = h.chain[i] < h.nslab ? stage_of[h.chain[i]] : 0xffffu;
+        if (t >= h.nu) return fail(MB_ERR_INVALID, "batch: chain row %u not staged", (unsigned)h.chain[i]);
+        h.chain[i] = t;
+      }
+    }
+  }
   h.pf_mask = 0;
   for (uint32_t i = 0; i < h.nsrc; ++i) {
     const void *base = h.src[i].fk ? (const void *)h.src[i].fk : h.src[i].col;
@@ -1106,10 +1179,129 @@ static mb_status batch_flush(Engine &E, BatchBuild &B, const mb_batch_opts &o, i
     const bool dense = o.prefetch == MB_PREFETCH_ALL || (o.prefetch == MB_PREFETCH_AUTO && B.src_weight[i] >= 0.02);
     if (aligned && dense && B.src_weight[i] > 0) h.pf_mask |= 1u << i;
   }
-  const BatchCfg c = batch_cfg(h, o);
-  MB_CUDA(cudaMemcpyAsync(E.bq_dev, &h, sizeof(BatchHdr), cudaMemcpyHostToDevice, E.stream));
-  MB_CUDA(cudaEventRecord(E.bq_copied[slot], E.stream));
-  return batch_scan(h, static_cast<const BatchHdr *>(E.bq_dev), c, out, nq, E.stream);
+  *cfg = batch_cfg(h, o);
+  return MB_OK;
+}
+
+// A planned enqueue: the batched launches (complete headers, host copies)
+// and the queries that run alone on the plain path.
+struct BatchPlanned {
+  std::vector<std::unique_ptr<BatchHdr>> hdrs;
+  std::vector<BatchCfg> cfgs;
+  std::vector<uint32_t> alone;
+  std::vector<uint64_t> offs;
+  uint64_t total = 0;
+};
+
+static mb_status batch_plan(Engine &E, const mb_query *qs, uint32_t n, const mb_batch_opts &o, BatchPlanned &P) {
+  P.offs.resize(n);
+  P.total = mb_queries_layout(qs, n, P.offs.data());
+  mb_plan pl;  // the rule plan
+  memset(&pl, 0, sizeof(pl));
+  pl.kind = MB_PLAN_FUSED;
+  pl.launch.grp_strategy = MB_GRP_AUTO;
+  BatchBuild B;
+  auto fresh = [&]() -> mb_status {
+    BatchHdr *h = new (std::nothrow) BatchHdr;
+    if (!h) return fail(MB_ERR_OOM, "batch: host header");
+    P.hdrs.emplace_back(h);
+    B.reset(h, E);
+    return MB_OK;
+  };
+  auto close = [&]() -> mb_status {
+    if (B.h->nq == 0) {
+      P.hdrs.pop_back();
+      return MB_OK;
+    }
+    BatchCfg c;
+    MB_CHECK(batch_finish(B, o, &c));
+    P.cfgs.push_back(c);
+    return MB_OK;
+  };
+  MB_CHECK(fresh());
+  Lowered L;
+  DevPrg D;
+  for (uint32_t i = 0; i < n; ++i) {
+    MB_CHECK(lower_query(E, qs[i], pl, L));
+    if (L.empty) continue;  // outputs stay zero
+    bool v4 = false;
+    MB_CHECK(flatten_prg(&L.prg, L.chk ? 1 : 0, &D, &v4));
+    const double sel = est_selectivity(E, L);
+    int r = batch_add(B, L, D, P.offs[i], i, sel);
+    if (r == BADD_FULL) {
+      MB_CHECK(close());
+      MB_CHECK(fresh());
+      r = batch_add(B, L, D, P.offs[i], i, sel);
+    }
+    if (r != BADD_OK) P.alone.push_back(i);
+  }
+  return close();
+}
+
+// The slab's tensor maps for tile width T, in device memory (encoded once
+// per index).
+static mb_status batch_maps(Engine &E, uint32_t V, const void **out) {
+  const int k = V == 4 ? 2 : V == 2 ? 1 : 0;
+  if (!E.bmaps[k]) {
+    std::vector<uint8_t> host(BMAP_COUNT * BMAP_BYTES);
+    MB_CHECK(batch_encode_maps(E.islab, E.stride, E.nbm, 32 * V, host.data()));
+    void *d = nullptr;
+    MB_CHECK(E.alloc(&d, host.size()));
+    MB_CUDA(cudaMemcpy(d, host.data(), host.size(), cudaMemcpyHostToDevice));
+    E.bmaps[k] = d;
+  }
+  *out = E.bmaps[k];
+  return MB_OK;
+}
+
+static mb_status batch_staging(Engine &E, BatchHdr **out, uint32_t *slot);
+
+static mb_status batch_opts_check(const mb_batch_opts &o, const char *who) {
+  if ((o.words_per_lane && o.words_per_lane != 1 && o.words_per_lane != 2 && o.words_per_lane != 4) ||
+      o.warps == 1 || o.warps > 16 || o.stages > 4 || o.prefetch > MB_PREFETCH_ALL ||
+      o.drain_warps >= (o.warps ? o.warps : 16u))
+    return fail(MB_ERR_INVALID, "%s: options out of range", who);
+  return MB_OK;
+}
+
+// Enqueues a planned batch: zeroes the outputs, then per batched launch its
+// header (copied through the pinned staging ring into the device header,
+// or, with dev_hdrs, already resident there) and the scan; then the queries
+// that run alone.
+static mb_status batch_launch(Engine &E, const mb_query *qs, const BatchPlanned &P, int64_t *out, uint64_t *nq,
+                              uint32_t n, BatchHdr *const *dev_hdrs) {
+  MB_CUDA(cudaMemsetAsync(out, 0, P.total * 8, E.stream));
+  MB_CUDA(cudaMemsetAsync(nq, 0, (size_t)n * 8, E.stream));
+  for (size_t i = 0; i < P.hdrs.size(); ++i) {
+    const BatchHdr &h = *P.hdrs[i];
+    const void *maps = nullptr;
+    MB_CHECK(batch_maps(E, P.cfgs[i].V, &maps));
+    const BatchHdr *dh;
+    if (dev_hdrs) {
+      dh = dev_hdrs[i];
+    } else {
+      BatchHdr *st = nullptr;
+      uint32_t slot = 0;
+      MB_CHECK(batch_staging(E, &st, &slot));
+      memcpy(st, &h, sizeof(BatchHdr));
+      MB_CUDA(cudaMemcpyAsync(E.bq_dev, st, sizeof(BatchHdr), cudaMemcpyHostToDevice, E.stream));
+      MB_CUDA(cudaEventRecord(E.bq_copied[slot], E.stream));
+      dh = static_cast<const BatchHdr *>(E.bq_dev);
+    }
+    MB_CHECK(batch_scan(h, dh, P.cfgs[i], maps, out, nq, E.stream));
+  }
+  if (!P.alone.empty()) {
+    mb_plan pl;
+    memset(&pl, 0, sizeof(pl));
+    pl.kind = MB_PLAN_FUSED;
+    pl.launch.grp_strategy = MB_GRP_AUTO;
+    Lowered L;
+    for (uint32_t i : P.alone) {
+      MB_CHECK(lower_query(E, qs[i], pl, L));
+      MB_CHECK(run_lowered(E, L, pl, out + P.offs[i], nq + i, false));
+    }
+  }
+  return MB_OK;
 }
 
 // The next staging header of the ring, once its previous copy is done.
@@ -1139,41 +1331,38 @@ extern "C" mb_status mb_engine_enqueue_batch(mb_engine *e, const mb_query *qs, u
   mb_batch_opts o;
   if (opts) o = *opts;
   else memset(&o, 0, sizeof(o));
-  if ((o.words_per_lane && o.words_per_lane != 1 && o.words_per_lane != 2 && o.words_per_lane != 4) ||
-      o.warps == 1 || o.warps > 16 || o.stages > 4 || o.prefetch > MB_PREFETCH_ALL ||
-      o.drain_warps >= (o.warps ? o.warps : 16u))
-    return fail(MB_ERR_INVALID, "mb_engine_enqueue_batch: options out of range");
-  std::vector<uint64_t> offs(n);
-  const uint64_t total = mb_queries_layout(qs, n, offs.data());
-  MB_CUDA(cudaMemsetAsync(out_dev, 0, total * 8, E.stream));
-  MB_CUDA(cudaMemsetAsync(nqual_dev, 0, (size_t)n * 8, E.stream));
-  mb_plan pl;  // the rule plan (queries the batch kernel cannot take run with it alone)
-  memset(&pl, 0, sizeof(pl));
-  pl.kind = MB_PLAN_FUSED;
-  pl.launch.grp_strategy = MB_GRP_AUTO;
-  BatchBuild B;
-  BatchHdr *h = nullptr;
-  uint32_t slot = 0;
-  MB_CHECK(batch_staging(E, &h, &slot));
-  B.reset(h, E);
-  Lowered L;
-  DevPrg P;
-  for (uint32_t i = 0; i < n; ++i) {
-    MB_CHECK(lower_query(E, qs[i], pl, L));
-    if (L.empty) continue;  // outputs stay zero
-    bool v4 = false;
-    MB_CHECK(flatten_prg(&L.prg, L.chk ? 1 : 0, &P, &v4));
-    const double sel = est_selectivity(E, L);
-    int r = batch_add(B, L, P, offs[i], i, sel);
-    if (r == BADD_FULL) {
-      MB_CHECK(batch_flush(E, B, o, out_dev, nqual_dev, slot));
-      MB_CHECK(batch_staging(E, &h, &slot));
-      B.reset(h, E);
-      r = batch_add(B, L, P, offs[i], i, sel);
-    }
-    if (r != BADD_OK) MB_CHECK(run_lowered(E, L, pl, out_dev + offs[i], nqual_dev + i, false));
+  MB_CHECK(batch_opts_check(o, "mb_engine_enqueue_batch"));
+  BatchPlanned P;
+  MB_CHECK(batch_plan(E, qs, n, o, P));
+  return batch_launch(E, qs, P, out_dev, nqual_dev, n, nullptr);
+}
+
+extern "C" mb_status mb_engine_batch_info(mb_engine *e, const mb_query *qs, uint32_t n, const mb_batch_opts *opts,
+                                          mb_batch_launch_info *launches, uint32_t cap, uint32_t *nlaunches,
+                                          uint32_t *nalone) {
+  if (!e || (!qs && n) || (!launches && cap)) return fail(MB_ERR_INVALID, "mb_engine_batch_info: NULL argument");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  mb_batch_opts o;
+  if (opts) o = *opts;
+  else memset(&o, 0, sizeof(o));
+  MB_CHECK(batch_opts_check(o, "mb_engine_batch_info"));
+  BatchPlanned P;
+  MB_CHECK(batch_plan(E, qs, n, o, P));
+  for (size_t i = 0; i < P.hdrs.size() && i < cap; ++i) {
+    mb_batch_launch_info &l = launches[i];
+    memset(&l, 0, sizeof(l));
+    l.queries = P.hdrs[i]->nq;
+    l.staged_rows = P.hdrs[i]->nu;
+    l.copies = P.hdrs[i]->ncopy;
+    l.words_per_lane = P.cfgs[i].V;
+    l.warps = P.cfgs[i].warps;
+    l.drain_warps = P.cfgs[i].drainers;
+    l.stages = P.cfgs[i].stages;
   }
-  return batch_flush(E, B, o, out_dev, nqual_dev, slot);
+  if (nlaunches) *nlaunches = (uint32_t)P.hdrs.size();
+  if (nalone) *nalone = (uint32_t)P.alone.size();
+  return MB_OK;
 }
 
 extern "C" mb_status mb_engine_query_batch(mb_engine *e, const mb_query *qs, uint32_t n, const mb_batch_opts *opts,
@@ -1193,6 +1382,151 @@ extern "C" mb_status mb_engine_query_batch(mb_engine *e, const mb_query *qs, uin
   if (nqual_host) MB_CUDA(cudaMemcpyAsync(nqual_host, E.bout + total, (size_t)n * 8, cudaMemcpyDeviceToHost, E.stream));
   MB_CUDA(cudaStreamSynchronize(E.stream));
   return check_device_error(E.stream);
+}
+
+// ------------------------------------------------------------ batch graphs
+struct mb_batch_graph {
+  mb_engine *e = nullptr;
+  BatchHdr *dh = nullptr;  // the launches' descriptors, resident
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t x = nullptr;
+};
+
+extern "C" mb_status mb_batch_graph_destroy(mb_batch_graph *g) {
+  if (!g) return MB_OK;
+  cudaSetDevice(g->e->E.device);
+  cudaStreamSynchronize(g->e->E.stream);
+  if (g->x) cudaGraphExecDestroy(g->x);
+  if (g->g) cudaGraphDestroy(g->g);
+  if (g->dh) cudaFree(g->dh);
+  delete g;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_batch_graph_create(mb_engine *e, const mb_query *qs, uint32_t n, const mb_batch_opts *opts,
+                                           int64_t *out_dev, uint64_t *nqual_dev, mb_batch_graph **out) {
+  if (!e || (!qs && n) || !out_dev || !nqual_dev || !out) return fail(MB_ERR_INVALID, "mb_batch_graph_create: NULL argument");
+  *out = nullptr;
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  mb_batch_opts o;
+  if (opts) o = *opts;
+  else memset(&o, 0, sizeof(o));
+  MB_CHECK(batch_opts_check(o, "mb_batch_graph_create"));
+  BatchPlanned P;
+  MB_CHECK(batch_plan(E, qs, n, o, P));
+  std::unique_ptr<mb_batch_graph, mb_status (*)(mb_batch_graph *)> G(new mb_batch_graph(), mb_batch_graph_destroy);
+  G->e = e;
+  const size_t nh = P.hdrs.size();
+  std::vector<BatchHdr *> dptr(nh);
+  if (nh) {
+    MB_CUDA(cudaMalloc(&G->dh, nh * sizeof(BatchHdr)));
+    for (size_t i = 0; i < nh; ++i) {
+      dptr[i] = G->dh + i;
+      MB_CUDA(cudaMemcpy(dptr[i], P.hdrs[i].get(), sizeof(BatchHdr), cudaMemcpyHostToDevice));
+    }
+  }
+  if (!device_error_word()) return fail(MB_ERR_OOM, "mb_batch_graph_create: device error word");
+  // one launch outside the capture makes every lazily allocated buffer
+  // (tensor maps, plain-path scratch) exist before it
+  MB_CHECK(batch_launch(E, qs, P, out_dev, nqual_dev, n, dptr.data()));
+  MB_CUDA(cudaStreamSynchronize(E.stream));
+  MB_CHECK(check_device_error(E.stream));
+  MB_CUDA(cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeRelaxed));
+  const mb_status st = batch_launch(E, qs, P, out_dev, nqual_dev, n, dptr.data());
+  const cudaError_t ce = cudaStreamEndCapture(E.stream, &G->g);
+  MB_CHECK(st);
+  MB_CUDA(ce);
+  MB_CUDA(cudaGraphInstantiate(&G->x, G->g, 0));
+  *out = G.release();
+  return MB_OK;
+}
+
+extern "C" mb_status mb_batch_graph_launch(mb_batch_graph *g) {
+  if (!g || !g->x) return fail(MB_ERR_INVALID, "mb_batch_graph_launch: NULL graph");
+  MB_CUDA(cudaSetDevice(g->e->E.device));
+  MB_CUDA(cudaGraphLaunch(g->x, g->e->E.stream));
+  return MB_OK;
+}
+
+// ------------------------------------------------------------ autotuner
+extern "C" mb_status mb_engine_tune_batch(mb_engine *e, const mb_query *qs, uint32_t n, uint32_t reps,
+                                          mb_batch_opts *best, float *best_ms, uint32_t *tried) {
+  if (!e || !qs || n == 0 || !best) return fail(MB_ERR_INVALID, "mb_engine_tune_batch: bad argument");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  if (reps == 0) reps = 3;
+  const uint64_t total = mb_queries_layout(qs, n, nullptr);
+  if (E.bout_cap < total + n) {
+    free_one(E.allocs, E.bout);
+    E.bout = nullptr;
+    MB_CHECK(E.alloc((void **)&E.bout, (total + n) * 8));
+    E.bout_cap = total + n;
+  }
+  int64_t *out = E.bout;
+  uint64_t *nq = reinterpret_cast<uint64_t *>(E.bout + total);
+  uint32_t count = 0;
+  std::vector<float> t(reps);
+  auto time_of = [&](const mb_batch_opts &o, float *ms) -> mb_status {
+    MB_CHECK(batch_opts_check(o, "mb_engine_tune_batch"));
+    BatchPlanned P;
+    MB_CHECK(batch_plan(E, qs, n, o, P));
+    const mb_status w = batch_launch(E, qs, P, out, nq, n, nullptr);  // warm-up
+    if (w == MB_ERR_UNSUPPORTED) {  // the shape does not fit on an SM: not a candidate
+      MB_CUDA(cudaStreamSynchronize(E.stream));
+      *ms = 1e30f;
+      return MB_OK;
+    }
+    MB_CHECK(w);
+    for (uint32_t r = 0; r < reps; ++r) {
+      MB_CUDA(cudaEventRecord(E.ev0, E.stream));
+      MB_CHECK(batch_launch(E, qs, P, out, nq, n, nullptr));
+      MB_CUDA(cudaEventRecord(E.ev1, E.stream));
+      MB_CUDA(cudaEventSynchronize(E.ev1));
+      MB_CUDA(cudaEventElapsedTime(&t[r], E.ev0, E.ev1));
+    }
+    MB_CHECK(check_device_error(E.stream));
+    std::sort(t.begin(), t.end());
+    *ms = t[reps / 2];
+    ++count;
+    return MB_OK;
+  };
+  mb_batch_opts b;
+  memset(&b, 0, sizeof(b));
+  float bms = 1e30f;
+  auto consider = [&](const mb_batch_opts &o) -> mb_status {
+    float ms = 0;
+    MB_CHECK(time_of(o, &ms));
+    if (ms < bms) bms = ms, b = o;
+    return MB_OK;
+  };
+  // tile width x warps (default drain warps: about a fifth)
+  for (uint32_t V : {4u, 2u, 1u})
+    for (uint32_t w : {16u, 12u, 8u}) {
+      mb_batch_opts o;
+      memset(&o, 0, sizeof(o));
+      o.words_per_lane = V;
+      o.warps = w;
+      MB_CHECK(consider(o));
+    }
+  // drain warps
+  const mb_batch_opts b1 = b;
+  for (uint32_t d = 1; d <= 6 && d < b1.warps; ++d) {
+    mb_batch_opts o = b1;
+    o.drain_warps = d;
+    MB_CHECK(consider(o));
+  }
+  // L2 prefetch of the payload
+  const mb_batch_opts b2 = b;
+  for (uint32_t pf : {(uint32_t)MB_PREFETCH_NONE, (uint32_t)MB_PREFETCH_ALL}) {
+    mb_batch_opts o = b2;
+    o.prefetch = pf;
+    MB_CHECK(consider(o));
+  }
+  *best = b;
+  if (best_ms) *best_ms = bms;
+  if (tried) *tried = count;
+  return MB_OK;
 }
 
 // ------------------------------------------------------------ learned planner

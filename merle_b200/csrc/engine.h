@@ -85,6 +85,7 @@ struct Engine {
   // with one 2-D tensor copy.
   uint32_t *islab = nullptr;
   uint32_t nbm = 0;  // bitmaps in the slab
+  void *bmaps[3] = {};  // the slab's tensor maps for tiles of 32, 64, 128 words (device)
   bool indexed = false;
   float index_build_ms = 0;
   // query scratch
@@ -122,6 +123,7 @@ struct Engine {
   mb_status alloc(void **p, size_t bytes);
   void free_star();
   void free_denorm();
+  void free_bmaps();
   mb_status setup_index_cols();
   // Customer city / part mfgr of a row: the denormalised column when built,
   // else a probe of the dimension through the foreign key.

@@ -229,6 +229,70 @@ def test_engine_batch_invalid_options(eng, mb):
         assert L.mb_engine_query_batch(eng.handle, qarr, 2, C.byref(o), out.ctypes.data, None) == abi.MB_ERR_INVALID
 
 
+def _batch_info(eng, mb, qs, opts=None):
+    L = mb.lib()
+    n = len(qs)
+    qarr = (abi.mb_query * n)(*qs)
+    infos = (abi.mb_batch_launch_info * 8)()
+    nl, na = C.c_uint32(0), C.c_uint32(0)
+    mb.check(L.mb_engine_batch_info(eng.handle, qarr, n, C.byref(opts) if opts else None, infos, 8,
+                                    C.byref(nl), C.byref(na)))
+    return list(infos)[:nl.value], na.value
+
+
+def test_engine_batch_stages_only_rows_it_reads(eng, mb):
+    """A batch stages the union of the rows its queries read (plus gaps of at
+    most two rows between runs), one tensor copy per run."""
+    q = abi.query(1, 366, 731, 1, 4, 0, 25)  # one year bin, three discount bins, quantity bins
+    li, na = _batch_info(eng, mb, [q])
+    assert na == 0 and len(li) == 1
+    assert li[0].queries == 1 and li[0].staged_rows <= 30 and 1 <= li[0].copies <= 4
+    qs = WL.random_mix(3, 64, narrow=0.3)
+    li, na = _batch_info(eng, mb, qs)
+    assert len(li) == 1 and li[0].queries + na == 64
+    assert li[0].staged_rows <= 242 and li[0].copies <= 48
+    assert li[0].words_per_lane in (1, 2, 4) and 1 <= li[0].drain_warps < li[0].warps
+
+
+def test_engine_batch_graph_replays(eng, star, orc, mb):
+    import torch
+    L = mb.lib()
+    qs = _mix_with_edges()
+    want, wn = _batch_oracle(orc, star, qs)
+    n = len(qs)
+    qarr = (abi.mb_query * n)(*qs)
+    out = torch.full((len(want),), -1, dtype=torch.int64, device="cuda")
+    nq = torch.zeros(n, dtype=torch.int64, device="cuda")
+    g = C.c_void_p()
+    mb.check(L.mb_batch_graph_create(eng.handle, qarr, n, None, out.data_ptr(), nq.data_ptr(), C.byref(g)))
+    try:
+        for _ in range(3):
+            out.fill_(-1)
+            torch.cuda.synchronize()
+            mb.check(L.mb_batch_graph_launch(g))
+            mb.check(L.mb_engine_sync(eng.handle, None, 0))
+            np.testing.assert_array_equal(out.cpu().numpy(), want)
+            np.testing.assert_array_equal(nq.cpu().numpy().astype(np.uint64), wn)
+    finally:
+        mb.check(L.mb_batch_graph_destroy(g))
+
+
+def test_engine_batch_autotune(eng, star, orc, mb):
+    L = mb.lib()
+    qs = WL.random_mix(5, 64, narrow=0.3)
+    n = len(qs)
+    qarr = (abi.mb_query * n)(*qs)
+    best = abi.mb_batch_opts()
+    ms, tried = C.c_float(0), C.c_uint32(0)
+    mb.check(L.mb_engine_tune_batch(eng.handle, qarr, n, 2, C.byref(best), C.byref(ms), C.byref(tried)))
+    assert tried.value >= 9 and 0 < ms.value < 1e3
+    assert best.words_per_lane in (1, 2, 4) and best.warps in (8, 12, 16)
+    want, wn = _batch_oracle(orc, star, qs)
+    out, nq = eng.query_batch(qs, best)
+    np.testing.assert_array_equal(out, want)
+    np.testing.assert_array_equal(nq, wn)
+
+
 def test_engine_denormalised_equals_probe(cuda, star, orc):
     """The index over denormalised dimension columns and the one that probes
     the dimensions through the foreign keys give the same results, on the
