@@ -254,7 +254,7 @@ def main():
     import torch.distributed as dist
 
     import merle_b200
-    from merle_b200 import abi, check, workload as WL
+    from merle_b200 import abi, check, shard, workload as WL
     from merle_b200.engine import Engine
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -267,7 +267,8 @@ def main():
     L = merle_b200.lib()
     n = args.rows or 6_000_000 * args.k
     eng = Engine(local)
-    eng.gen_star(SEED_DATA, args.k, n, width4=bool(args.width4), row0=rank * n)
+    row0, n = shard.row_range(rank, n)
+    eng.gen_star(SEED_DATA, args.k, n, width4=bool(args.width4), row0=row0)
     eng.build_index()
     info = eng.info()
     qs = WL.random_mix(SEED_QUERIES, args.queries, args.narrow)
@@ -282,7 +283,7 @@ def main():
     def allreduce():
         if world > 1:
             with torch.cuda.stream(ext):
-                dist.all_reduce(out)
+                shard.combine(out, nq)
 
     # the launch shape from the autotuner (timed on this mix, before the
     # measured steps), and the batch captured once as a CUDA graph

@@ -641,9 +641,11 @@ typedef struct mb_server_opts {
   uint32_t mode;            /* mb_serve_mode */
   uint32_t max_batch;       /* 1..MB_BATCH_MAX (0 = 64) */
   uint32_t max_inflight;    /* launches on the GPU at once, 1..8 (0 = 2) */
-  uint32_t use_planner;     /* plan with the engine's learned planner (mb_engine_set_planner) */
+  uint32_t use_planner;     /* plain-path launches plan with the engine's learned planner
+                               (mb_engine_set_planner) */
   uint32_t min_batch;       /* batched mode: launches of fewer queries run them on the plain
-                               path, one after another (0 = 6; 1 = always the batched scan) */
+                               path, one after another (1 = always the batched scan); 0 = an
+                               online cost model of both kinds decides per launch */
   uint32_t pad_;
   mb_batch_opts batch;      /* batched-scan launch shape */
 } mb_server_opts;
@@ -664,6 +666,7 @@ typedef struct mb_server_stats {
   uint64_t launches, launched_queries;
   uint64_t peak_reserved;   /* largest admission reservation in flight (bytes) */
   double gpu_ms;            /* sum of launch device times */
+  uint64_t scan_launches;   /* launches that took the batched scan */
 } mb_server_stats;
 MB_API mb_status mb_server_create(mb_engine *e, const mb_server_opts *opts, mb_server **out);
 /* Stops accepting requests, finishes the launches in flight (queued requests

@@ -166,7 +166,8 @@ class mb_request_info(C.Structure):
 
 class mb_server_stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "rejected", "cancelled", "failed", "launches",
-                                          "launched_queries", "peak_reserved")] + [("gpu_ms", C.c_double)]
+                                          "launched_queries", "peak_reserved")] + [("gpu_ms", C.c_double),
+                                                                                   ("scan_launches", C.c_uint64)]
 
 
 class mb_query_stats(C.Structure):

@@ -516,13 +516,17 @@ __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, co
 #pragma unroll
       for (int k = 0; k < V; ++k) cx[k] |= x[k];
     }
+    uint32_t any = 0;
     if (hd >> 15) {
 #pragma unroll
-      for (int k = 0; k < V; ++k) acc[k] &= ~(cm[k] | cx[k]);
+      for (int k = 0; k < V; ++k) acc[k] &= ~(cm[k] | cx[k]), any |= acc[k];
     } else {
 #pragma unroll
-      for (int k = 0; k < V; ++k) acc[k] &= cm[k] | cx[k], unc[k] |= cx[k];
+      for (int k = 0; k < V; ++k) acc[k] &= cm[k] | cx[k], unc[k] |= cx[k], any |= acc[k];
     }
+    // conjuncts come most selective first: once no row of the tile is
+    // left, the rest of the chain cannot bring one back
+    if (!__any_sync(0xffffffffu, any != 0)) break;
   }
   uint32_t p[V], u[V], pc = 0;
   if (w0 + T <= nwords && (tail == 0 || w0 + T < nwords)) {  // an interior tile: no mask
@@ -539,6 +543,7 @@ __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, co
       pc += __popc(p[k]);
     }
   }
+  if (!__any_sync(0xffffffffu, pc != 0)) return;  // no row of this tile
   const uint32_t lt = (1u << lane) - 1u;
   const uint32_t rowbase = (uint32_t)((w0 + lane * V) * 32);  // first row of the lane's words
   uint32_t qn = *qlen;

@@ -424,27 +424,21 @@ struct OpB {
   }
 };
 
-static void build_op(const Engine &E, const mb_query &q, mb_op &out) {
+void ssb_build_op(const SsbSrc &S, const mb_query &q, mb_op &out) {
   OpB b;
   const uint32_t *p = q.p;
-  const mb_src date = fact_src(E.orderdate, E.fact_width("orderdate"));
-  const mb_src scity = fact_src(E.suppcity, E.fact_width("suppcity"));
-  const mb_src ccity = E.ccity_src(), mfgr = E.mfgr_src();
-  const mb_src rev = fact_src(E.revenue, 4);
   if (q.tmpl == 1) {
-    uint32_t sd = b.src(date), sdi = b.src(fact_src(E.discount, E.fact_width("discount")));
-    uint32_t sq = b.src(fact_src(E.quantity, E.fact_width("quantity")));
-    uint32_t se = b.src(fact_src(E.extendedprice, 4));
+    uint32_t sd = b.src(S.date), sdi = b.src(S.disc), sq = b.src(S.qty), se = b.src(S.eprice);
     b.clause1(sd, p[0], p[1]), b.clause1(sdi, p[2], p[3]), b.clause1(sq, p[4], p[5]);
     b.o.vkind = MB_V_MUL, b.o.va = se, b.o.vb = sdi;
   } else if (q.tmpl == 2) {
-    uint32_t ss = b.src(scity), sm = b.src(mfgr), sd = b.src(date), sr = b.src(rev);
+    uint32_t ss = b.src(S.scity), sm = b.src(S.mfgr), sd = b.src(S.date), sr = b.src(S.rev);
     b.clause1(ss, p[2], p[3]), b.clause1(sm, p[0], p[1]);
     b.key(sm, MB_X_ID, 1, p[0], 1);
     b.key(sd, MB_X_YEAR, 1, 0, p[1] - p[0]);
     b.o.vkind = MB_V_COL, b.o.va = sr;
   } else if (q.tmpl == 3) {
-    uint32_t ss = b.src(scity), sd = b.src(date), sc = b.src(ccity), sr = b.src(rev);
+    uint32_t ss = b.src(S.scity), sd = b.src(S.date), sc = b.src(S.ccity), sr = b.src(S.rev);
     b.clause1(ss, p[2], p[3]), b.clause1(sd, p[4], p[5]), b.clause1(sc, p[0], p[1]);
     uint32_t cmn = p[0], cmx = p[1], smn = p[2], smx = p[3], xf = MB_X_ID, dv = 1;
     if (p[1] - p[0] >= 50) cmn /= 10, cmx /= 10, smn /= 10, smx /= 10, xf = MB_X_DIV, dv = 10;
@@ -454,8 +448,8 @@ static void build_op(const Engine &E, const mb_query &q, mb_op &out) {
     b.key(ss, xf, dv, smn, 1);
     b.o.vkind = MB_V_COL, b.o.va = sr;
   } else {
-    uint32_t ss = b.src(scity), sd = b.src(date), sc = b.src(ccity), sm = b.src(mfgr), sr = b.src(rev);
-    uint32_t sk = b.src(fact_src(E.supplycost, 4));
+    uint32_t ss = b.src(S.scity), sd = b.src(S.date), sc = b.src(S.ccity), sm = b.src(S.mfgr), sr = b.src(S.rev);
+    uint32_t sk = b.src(S.scost);
     b.clause1(ss, p[2], p[3]), b.clause1(sd, p[6], p[7]), b.clause1(sc, p[0], p[1]), b.clause1(sm, p[4], p[5]);
     uint32_t smn = p[2], smx = p[3], sxf = MB_X_ID, sdv = 1;
     if (p[3] - p[2] >= 50) smn /= 10, smx /= 10, sxf = MB_X_DIV, sdv = 10;
@@ -468,6 +462,20 @@ static void build_op(const Engine &E, const mb_query &q, mb_op &out) {
     b.o.vkind = MB_V_SUB, b.o.va = sr, b.o.vb = sk;
   }
   out = b.o;
+}
+
+static void build_op(const Engine &E, const mb_query &q, mb_op &out) {
+  SsbSrc S;
+  S.date = fact_src(E.orderdate, E.fact_width("orderdate"));
+  S.disc = fact_src(E.discount, E.fact_width("discount"));
+  S.qty = fact_src(E.quantity, E.fact_width("quantity"));
+  S.eprice = fact_src(E.extendedprice, 4);
+  S.rev = fact_src(E.revenue, 4);
+  S.scost = fact_src(E.supplycost, 4);
+  S.scity = fact_src(E.suppcity, E.fact_width("suppcity"));
+  S.ccity = E.ccity_src();
+  S.mfgr = E.mfgr_src();
+  ssb_build_op(S, q, out);
 }
 
 static void query_preds(const mb_query &q, std::vector<Pred> &preds) {

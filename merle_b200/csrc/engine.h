@@ -132,6 +132,13 @@ struct Engine {
   mb_status build_denorm();
 };
 
+// The op functors s1op..s4op (ssb/lambdas.cuh:19-152) of a template query as
+// an mb_op over the given sources (engine.cu).
+struct SsbSrc {
+  mb_src date, disc, qty, eprice, rev, scost, scity, ccity, mfgr;
+};
+void ssb_build_op(const SsbSrc &S, const mb_query &q, mb_op &out);
+
 // Planner and lowering (engine.cu).
 Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t W, int nchk_sources);
 mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered &L);

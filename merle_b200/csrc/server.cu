@@ -7,9 +7,11 @@
 // (mb_engine_enqueue_batch) and plain path (run_lowered), so every answer is
 // the one the engine gives the query alone.
 //
-// A batched-mode launch of fewer than min_batch queries runs them on the
-// plain path instead: below that the persistent scan's per-tile cost, paid
-// by one warp per query, outweighs the bitmap reads it shares.
+// A batched-mode launch runs its queries either through the persistent
+// batched scan or one after another on the plain path: a launch of few
+// queries pays the scan's per-tile cost (one warp per query and tile) for
+// little shared reading.  An online cost model of both kinds (device times of
+// completed launches) picks the cheaper for each launch's size.
 //
 // Life of a request: submit (queued, t_submit) -> admitted into a launch by
 // the dispatcher (reservation taken, group table carved from the arena,
@@ -48,12 +50,47 @@ struct Request {
 
 struct Launch {
   std::vector<Request *> reqs;
+  bool scan = false;  // the batched scan (else the plain path, query by query)
   uint64_t off = 0, bytes = 0;  // arena bytes [off, off + bytes)
   uint64_t reserved = 0;
   uint32_t index = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   mb_status st = MB_OK;
   uint32_t *err = nullptr;  // pinned copy of the device error word
+};
+
+// Online cost model of the batched server's two launch kinds, from the
+// device times of completed launches: the plain path as a time per query
+// (exponentially weighted mean), the batched scan as a + b * queries (a
+// least-squares fit with exponentially decaying weights).  A launch of n
+// queries takes the batched scan when a + b * n < n * plain.
+struct CostModel {
+  double p_ms = 0;  // plain: ms per query
+  uint32_t p_cnt = 0;
+  double w = 0, wn = 0, wt = 0, wnn = 0, wnt = 0;  // weighted sums over scan launches
+  uint32_t b_cnt = 0;
+  static constexpr double DECAY = 0.97;
+  void add_plain(uint32_t n, float ms) {
+    const double per = ms / (double)(n ? n : 1);
+    p_ms = p_cnt ? 0.9 * p_ms + 0.1 * per : per;
+    ++p_cnt;
+  }
+  void add_scan(uint32_t n, float ms) {
+    w = DECAY * w + 1, wn = DECAY * wn + n, wt = DECAY * wt + ms;
+    wnn = DECAY * wnn + (double)n * n, wnt = DECAY * wnt + (double)n * ms;
+    ++b_cnt;
+  }
+  bool ready() const { return p_cnt >= 3 && b_cnt >= 3; }
+  bool scan_better(uint32_t n) const {
+    const double var = w * wnn - wn * wn;
+    double a = wt / w, b = 0;
+    if (var > 1e-9 * w * w) {  // two or more distinct batch sizes seen
+      b = (w * wnt - wn * wt) / var;
+      a = (wt - b * wn) / w;
+      if (b < 0) b = 0, a = wt / w;
+    }
+    return a + b * n < n * p_ms;
+  }
 };
 
 uint64_t splitmix(uint64_t z) {
@@ -87,6 +124,7 @@ struct mb_server {
   bool stop = false;
   std::thread th;
   mb_server_stats stats{};
+  CostModel cost;
   // injected faults (host side)
   uint32_t f_alloc = 0, f_launch = 0, f_slow = 0, f_slow_us = 0;
 
@@ -213,6 +251,12 @@ bool mb_server::launch_some(std::unique_lock<std::mutex> &lk) {
     }
   }
   L->reqs = take;
+  // batched mode: the batched scan or the plain path (a fixed min_batch, or
+  // the cost model once it has seen both kinds; until then 6 queries)
+  const uint32_t nt = (uint32_t)take.size();
+  if (o.mode == MB_SERVE_PLAIN) L->scan = false;
+  else if (o.min_batch) L->scan = nt >= o.min_batch;
+  else L->scan = cost.ready() ? nt >= 2 && cost.scan_better(nt) : nt >= 6;
   L->off = off;
   L->bytes = bytes;
   L->reserved = res;
@@ -247,13 +291,24 @@ bool mb_server::launch_some(std::unique_lock<std::mutex> &lk) {
   for (uint32_t i = 0; i < n; ++i) qs[i] = take[i]->q, total += take[i]->ngroups;
   int64_t *out_dev = reinterpret_cast<int64_t *>(arena + off);
   uint64_t *nq_dev = reinterpret_cast<uint64_t *>(out_dev + total);
+  // a batched-mode launch on the plain path plans with the learned planner
+  // when it is on (before the launch's first event: planning runs a sample
+  // pass and waits for it)
+  std::vector<mb_plan> pl;
+  bool learned = false;
+  if (o.mode == MB_SERVE_BATCHED && !L->scan && o.use_planner && E.planner && !f_a && !f_l) {
+    pl.resize(n);
+    std::vector<uint32_t> pick(n, 0);
+    learned = mb_engine_plan_learned(eng, qs.data(), n, pl.data(), pick.data()) == MB_OK;
+    for (uint32_t i = 0; i < n; ++i) take[i]->info.plan = learned ? pick[i] : 0;
+  }
   mb_status s = MB_OK;
   if (f_a) s = fail(MB_ERR_OOM, "serving: injected arena allocation failure");
   if (s == MB_OK && cudaEventRecord(L->ev0, st) != cudaSuccess) s = fail(MB_ERR_CUDA, "serving: event record");
   if (s == MB_OK && f_l) s = fail(MB_ERR_CUDA, "serving: injected launch failure");
   if (s == MB_OK) {
     if (o.mode == MB_SERVE_PLAIN) s = mb_engine_enqueue(eng, qs.data(), 1, &take[0]->plan, out_dev, nq_dev, 0);
-    else if (n < o.min_batch) s = mb_engine_enqueue(eng, qs.data(), n, nullptr, out_dev, nq_dev, 0);
+    else if (!L->scan) s = mb_engine_enqueue(eng, qs.data(), n, learned ? pl.data() : nullptr, out_dev, nq_dev, 0);
     else s = mb_engine_enqueue_batch(eng, qs.data(), n, &o.batch, out_dev, nq_dev);
   }
   if (s == MB_OK && cudaMemcpyAsync(mirror + off, arena + off, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
@@ -290,6 +345,11 @@ void mb_server::complete(Launch *L) {
     finish(r, s);
   }
   stats.gpu_ms += s == MB_OK ? ms : 0.0;
+  if (L->scan) ++stats.scan_launches;
+  if (s == MB_OK && o.mode == MB_SERVE_BATCHED) {
+    if (L->scan) cost.add_scan((uint32_t)L->reqs.size(), ms);
+    else cost.add_plain((uint32_t)L->reqs.size(), ms);
+  }
   reserved -= L->reserved;
   used -= L->bytes;
   // the caller popped L: the oldest live tables now start at the next launch
@@ -343,7 +403,6 @@ extern "C" mb_status mb_server_create(mb_engine *e, const mb_server_opts *opts, 
   if (o.mem_budget == 0) o.mem_budget = 256ull << 20;
   if (o.max_batch == 0) o.max_batch = 64;
   if (o.max_inflight == 0) o.max_inflight = 2;
-  if (o.min_batch == 0) o.min_batch = 6;
   if (o.mode > MB_SERVE_PLAIN || o.max_batch > MB_BATCH_MAX || o.max_inflight > 8 || o.mem_budget < 4096)
     return fail(MB_ERR_INVALID, "mb_server_create: options out of range");
   if (!e->E.indexed) return fail(MB_ERR_INVALID, "mb_server_create: the engine has no index");

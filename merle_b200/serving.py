@@ -118,13 +118,15 @@ def summarize(info, offered_qps: float | None = None) -> dict:
 
 
 def sweep(eng, qs, rates, modes=("batched", "plain"), seed: int = 5, mem_budget: int = 0,
-          max_batch: int = 0, max_inflight: int = 0) -> list[dict]:
+          max_batch: int = 0, max_inflight: int = 0, batch: abi.mb_batch_opts | None = None,
+          use_planner: bool = False) -> list[dict]:
     """The same arrival stream through each server mode at each rate."""
     recs = []
     for mode in modes:
         m = abi.SERVE_BATCHED if mode == "batched" else abi.SERVE_PLAIN
         for rate in rates:
-            with Server(eng, m, mem_budget=mem_budget, max_batch=max_batch, max_inflight=max_inflight) as s:
+            with Server(eng, m, mem_budget=mem_budget, max_batch=max_batch, max_inflight=max_inflight,
+                        batch=batch, use_planner=use_planner and mode == "batched") as s:
                 s.run_load(qs[:min(len(qs), 32)], rate, seed + 1)  # warm-up (untimed)
                 t = time.perf_counter()
                 out, info = s.run_load(qs, rate, seed)
@@ -145,19 +147,43 @@ def main(argv=None) -> None:
     ap.add_argument("--budget-mb", type=int, default=0)
     ap.add_argument("--max-batch", type=int, default=0)
     ap.add_argument("--max-inflight", type=int, default=0)
+    ap.add_argument("--width4", type=int, default=1, help="4-byte fact columns (0: ssb_schema widths)")
+    ap.add_argument("--planner", type=str, default="",
+                    help="weights of a trained planner network (merle_b200.planner): the batched server's "
+                         "plain-path launches use its plans")
+    ap.add_argument("--tune", type=int, default=1, help="autotune the batched scan's shape on a 64-query sample")
     ap.add_argument("--out", type=str, default="")
     a = ap.parse_args(argv)
     k = max(1, round(a.rows / 6_000_000))
     e = Engine()
     t0 = time.perf_counter()
-    e.gen_star(2, k, a.rows)
+    e.gen_star(2, k, a.rows, width4=bool(a.width4))
     e.build_index()
     info = e.info()
+    setup_s = time.perf_counter() - t0
     qs = random_mix(3, a.queries, narrow=0.3)
+    bopts, tune = None, None
+    if a.tune:
+        bopts = abi.mb_batch_opts()
+        ms, tried = C.c_float(0), C.c_uint32(0)
+        sample = (abi.mb_query * 64)(*qs[:64])
+        check(lib().mb_engine_tune_batch(e.handle, sample, min(64, len(qs)), 3, C.byref(bopts), C.byref(ms),
+                                         C.byref(tried)))
+        tune = {"opts": {f: getattr(bopts, f) for f, _ in bopts._fields_ if f != "pad_"}, "best_ms": ms.value}
+    mlp = None
+    if a.planner:
+        from .planner import MLP
+        mlp = MLP.load(a.planner)
+        check(lib().mb_engine_set_planner(e.handle, mlp.handle))
     recs = sweep(e, qs, [float(r) for r in a.rates.split(",")], tuple(a.modes.split(",")),
-                 mem_budget=a.budget_mb << 20, max_batch=a.max_batch, max_inflight=a.max_inflight)
-    head = {"rows": a.rows, "k": k, "queries": a.queries, "setup_s": time.perf_counter() - t0,
-            "resident_bytes": info["fact_bytes"] + info["dim_bytes"] + info["index_bytes"] + info["denorm_bytes"]}
+                 mem_budget=a.budget_mb << 20, max_batch=a.max_batch, max_inflight=a.max_inflight, batch=bopts,
+                 use_planner=mlp is not None)
+    if mlp is not None:
+        check(lib().mb_engine_set_planner(e.handle, None))
+        mlp.close()
+    head = {"rows": a.rows, "k": k, "width4": a.width4, "queries": a.queries, "setup_s": setup_s,
+            "resident_bytes": info["fact_bytes"] + info["dim_bytes"] + info["index_bytes"] + info["denorm_bytes"],
+            "index_build_ms": info["index_build_ms"], "batch_tune": tune, "planner": a.planner or None}
     lines = [json.dumps({**head, **r}) for r in recs]
     for ln in lines:
         print(ln, flush=True)

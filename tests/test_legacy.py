@@ -1,0 +1,56 @@
+"""The reference's own C entry points (include/merle_b200_legacy.h).
+
+CPU: the library exports them (and the bin tables) and window_zipf, a host
+function, equals the reference's outputs in tests/golden.  Where the
+reference tree is present, its unmodified main.c compiles and links against
+libmerleb200.so.  GPU (test_gpu_legacy.py): the SSB and synthetic demo drivers
+end to end."""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+GOLDEN = ROOT / "tests" / "golden"
+REF = Path("/root/reference")
+
+
+def test_bin_tables_exported(mb):
+    L = mb.lib()
+    tabs = {"dateSpBin": 8, "dateDeBin": 5, "discntSpBin": 5, "discntDeBin": 12, "qtySpBin": 6, "qtyDeBin": 11,
+            "mfgrSpBin": 6, "mfgrDeBin": 6, "sCitySpBin": 6, "sCityDeBin": 4}
+    for name, n in tabs.items():
+        a = (C.c_uint64 * n).in_dll(L, name)
+        assert list(a) == sorted(a) and len(set(a)) == n
+    assert list((C.c_uint64 * 8).in_dll(L, "dateSpBin")) == [0, 366, 731, 1096, 1461, 1827, 2192, 2557]
+
+
+def test_window_zipf_matches_reference(mb):
+    L = mb.lib()
+    L.window_zipf.restype = C.POINTER(C.c_double)
+    L.window_zipf.argtypes = [C.c_double, C.c_size_t, C.c_size_t]
+    g = json.loads((GOLDEN / "golden.json").read_text())["window_zipf"]
+    for skew, want in g.items():
+        p = L.window_zipf(float(skew), len(want), 60)
+        got = np.ctypeslib.as_array(p, shape=(len(want),)).copy()
+        np.testing.assert_allclose(got, want, rtol=1e-13, atol=0)
+    assert not L.window_zipf(1.0, 10, 60)  # skewness must exceed 1
+
+
+@pytest.mark.skipif(not (REF / "main.c").exists() or shutil.which("gcc") is None,
+                    reason="reference tree or gcc absent")
+def test_reference_main_links_unchanged(mb, tmp_path):
+    """The reference's driver (main.c, its headers) builds against this library
+    with no source change: every symbol it needs resolves in libmerleb200.so."""
+    exe = tmp_path / "mydemo"
+    r = subprocess.run(["gcc", "-fopenmp", str(REF / "main.c"), f"-I{REF}", "-I/usr/local/cuda/include",
+                        f"-L{mb.LIB_PATH.parent}", "-lmerleb200", f"-Wl,-rpath,{mb.LIB_PATH.parent}",
+                        "-Wl,--no-undefined", "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
