@@ -404,6 +404,20 @@ MB_API mb_status mb_engine_build_index(mb_engine *e);
 #define MB_INDEX_PROBE_DIMS 1u  /* keep probing the dimensions (no denormalised columns) */
 MB_API mb_status mb_engine_build_index_ex(mb_engine *e, uint32_t flags);
 
+/* Index files, so an index need not be rebuilt between runs.  No
+ * counterpart in the reference (whose on-disk state is the column files,
+ * ssb/cpuref.c:8-27).  Layout, little-endian: "MBIX", version 1, table rows,
+ * words per bitmap, bitmap count, then per indexed column and level the bin
+ * count, the bin bounds (u64) and the rows per bin (u64), then every bitmap
+ * of the slab (stride words each), then an FNV-1a 64 hash of everything
+ * before it.  Saving needs a built index. */
+MB_API mb_status mb_engine_save_index(mb_engine *e, const char *path);
+/* Loads an index file written for this engine's table (same rows, same
+ * levels; the caller vouches that the columns are the ones it was built
+ * over).  flags as mb_engine_build_index_ex.  MB_ERR_IO on a file error or a
+ * hash mismatch, MB_ERR_INVALID if the file does not fit the table. */
+MB_API mb_status mb_engine_load_index(mb_engine *e, const char *path, uint32_t flags);
+
 typedef struct mb_engine_info {
   uint64_t nrows, fact_bytes, dim_bytes, index_bytes;
   uint32_t k, width4, nbitmaps, sms;

@@ -215,6 +215,8 @@ SIGNATURES: dict[str, tuple] = {
     "mb_engine_load_star": (I32, [VOIDP, C.POINTER(mb_star_host)]),
     "mb_engine_build_index": (I32, [VOIDP]),
     "mb_engine_build_index_ex": (I32, [VOIDP, U32]),
+    "mb_engine_save_index": (I32, [VOIDP, C.c_char_p]),
+    "mb_engine_load_index": (I32, [VOIDP, C.c_char_p, U32]),
     "mb_engine_get_info": (I32, [VOIDP, C.POINTER(mb_engine_info)]),
     "mb_query_ngroups": (U32, [C.POINTER(mb_query)]),
     "mb_engine_plan_rule": (I32, [VOIDP, C.POINTER(mb_query), C.POINTER(mb_plan)]),

@@ -480,53 +480,42 @@ __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, co
   constexpr uint32_t T = 32 * V;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t ch = C.Qd[q * BQD_WORDS + 4], c0 = ch & 0xffffu, nc = ch >> 16;
-  // the chain: per conjunct a header (middle bins | edge bins << 8 | negated
-  // << 15) and the union indices of its middle bins, then of its edge bins
-  uint32_t acc[V], unc[V];
+  // the chain: one entry per bin, stage row | edge | last of its conjunct |
+  // conjunct negated (BCH_*); four entries per step, their loads issued
+  // together
+  uint32_t acc[V], unc[V], cm[V], cx[V];
 #pragma unroll
-  for (int k = 0; k < V; ++k) acc[k] = 0xffffffffu, unc[k] = 0;
+  for (int k = 0; k < V; ++k) acc[k] = 0xffffffffu, unc[k] = 0, cm[k] = 0, cx[k] = 0;
   const uint32_t *sl = stage + lane * V;
-  for (uint32_t i = 0; i < nc;) {
-    const uint32_t hd = chain[c0 + i++];
-    const uint32_t nm = hd & 0xffu, ne = (hd >> 8) & 0x7fu;
-    uint32_t cm[V], cx[V];
+  for (uint32_t i = 0; i < nc; i += 4) {
+    uint32_t e[4], x[4][V];
 #pragma unroll
-    for (int k = 0; k < V; ++k) cm[k] = cx[k] = 0;
-    // middle bins four at a time: the indices, then the words, then the ORs
-    uint32_t j = 0;
-    for (; j + 4 <= nm; j += 4, i += 4) {
-      const uint32_t b0 = chain[c0 + i], b1 = chain[c0 + i + 1], b2 = chain[c0 + i + 2], b3 = chain[c0 + i + 3];
-      uint32_t x0[V], x1[V], x2[V], x3[V];
-      lds_words<V>(sl + b0 * T, x0);
-      lds_words<V>(sl + b1 * T, x1);
-      lds_words<V>(sl + b2 * T, x2);
-      lds_words<V>(sl + b3 * T, x3);
+    for (int j = 0; j < 4; ++j) e[j] = i + j < nc ? chain[c0 + i + j] : 0u;
 #pragma unroll
-      for (int k = 0; k < V; ++k) cm[k] |= (x0[k] | x1[k]) | (x2[k] | x3[k]);
+    for (int j = 0; j < 4; ++j)
+      if (i + j < nc) lds_words<V>(sl + (e[j] & BCH_ROW) * T, x[j]);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (i + j >= nc) break;
+      if (e[j] & BCH_EDGE) {
+#pragma unroll
+        for (int k = 0; k < V; ++k) cx[k] |= x[j][k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < V; ++k) cm[k] |= x[j][k];
+      }
+      if (e[j] & BCH_LAST) {
+        if (e[j] & BCH_NEG) {
+#pragma unroll
+          for (int k = 0; k < V; ++k) acc[k] &= ~(cm[k] | cx[k]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < V; ++k) acc[k] &= cm[k] | cx[k], unc[k] |= cx[k];
+        }
+#pragma unroll
+        for (int k = 0; k < V; ++k) cm[k] = 0, cx[k] = 0;
+      }
     }
-    for (; j < nm; ++j) {
-      uint32_t x[V];
-      lds_words<V>(sl + chain[c0 + i++] * T, x);
-#pragma unroll
-      for (int k = 0; k < V; ++k) cm[k] |= x[k];
-    }
-    for (uint32_t j2 = 0; j2 < ne; ++j2) {
-      uint32_t x[V];
-      lds_words<V>(sl + chain[c0 + i++] * T, x);
-#pragma unroll
-      for (int k = 0; k < V; ++k) cx[k] |= x[k];
-    }
-    uint32_t any = 0;
-    if (hd >> 15) {
-#pragma unroll
-      for (int k = 0; k < V; ++k) acc[k] &= ~(cm[k] | cx[k]), any |= acc[k];
-    } else {
-#pragma unroll
-      for (int k = 0; k < V; ++k) acc[k] &= cm[k] | cx[k], unc[k] |= cx[k], any |= acc[k];
-    }
-    // conjuncts come most selective first: once no row of the tile is
-    // left, the rest of the chain cannot bring one back
-    if (!__any_sync(0xffffffffu, any != 0)) break;
   }
   uint32_t p[V], u[V], pc = 0;
   if (w0 + T <= nwords && (tail == 0 || w0 + T < nwords)) {  // an interior tile: no mask
@@ -543,7 +532,6 @@ __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, co
       pc += __popc(p[k]);
     }
   }
-  if (!__any_sync(0xffffffffu, pc != 0)) return;  // no row of this tile
   const uint32_t lt = (1u << lane) - 1u;
   const uint32_t rowbase = (uint32_t)((w0 + lane * V) * 32);  // first row of the lane's words
   uint32_t qn = *qlen;

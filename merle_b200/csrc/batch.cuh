@@ -87,8 +87,19 @@ struct BatchHdr {
   uint32_t copy[BCP_MAX];
   BatchSrc src[BS_MAX];
   uint32_t Qd[BQ_MAX * BQD_WORDS];
-  uint16_t chain[BC_MAX];  // per conjunct: header, then stage rows (batch_add, batch_flush)
+  uint16_t chain[BC_MAX];  // one entry per bin (BCH_*): stage row and flags
   uint8_t order[BQ_MAX];   // the order in which warps take the queries (costliest first)
+};
+
+// A chain entry: a bin of a query's conjunctive program.  Conjuncts are
+// consecutive runs of entries, the last one flagged; a conjunct is the OR of
+// its bins (edge bins also mark uncertain rows), the query the AND of its
+// conjuncts (of the complement of a negated one).  The host builds entries
+// with slab rows (BCH_SLAB_*) and rewrites them to stage rows when the batch
+// is complete.
+enum : uint32_t {
+  BCH_ROW = 0xffu, BCH_EDGE = 1u << 8, BCH_LAST = 1u << 9, BCH_NEG = 1u << 10,
+  BCH_SLAB_ROW = 0xfffu, BCH_SLAB_FLAGS = 12  // slab row | flags << 12 (flags as above, >> 8)
 };
 
 // Launch shape of the batched scan.

@@ -47,6 +47,16 @@ mb_status Engine::alloc(void **p, size_t bytes) {
 
 static void free_one(std::vector<void *> &allocs, void *p);
 
+void Engine::drop_index() {
+  for (auto &c : idx)
+    for (auto &l : c.levels) l.slab = nullptr;
+  free_one(allocs, islab);
+  islab = nullptr;
+  free_bmaps();
+  nbm = 0;
+  indexed = false;
+}
+
 void Engine::free_bmaps() {
   for (void *&m : bmaps) {
     free_one(allocs, m);
@@ -655,13 +665,7 @@ extern "C" mb_status mb_engine_build_index_ex(mb_engine *e, uint32_t flags) {
   Engine &E = e->E;
   if (!E.custkey) return fail(MB_ERR_INVALID, "mb_engine_build_index: no table");
   MB_CUDA(cudaSetDevice(E.device));
-  for (auto &c : E.idx)
-    for (auto &l : c.levels) l.slab = nullptr;
-  free_one(E.allocs, E.islab);
-  E.islab = nullptr;
-  E.free_bmaps();
-  E.nbm = 0;
-  E.indexed = false;
+  E.drop_index();
   MB_CUDA(cudaEventRecord(E.ev0, E.stream));
   if (flags & MB_INDEX_PROBE_DIMS) E.free_denorm();
   else MB_CHECK(E.build_denorm());
@@ -1071,7 +1075,7 @@ static int batch_add(BatchBuild &B, const Lowered &L, const DevPrg &P, uint64_t 
     for (uint32_t t = 0; t < s && !seen; ++t) seen = same_src(O.src[t], O.src[s]);
     if (!seen) ++newsrc;
   }
-  const uint32_t nch = P.ncnf + MB_MAXCOLS;  // entries + at most one header per operand
+  const uint32_t nch = P.ncnf;  // chain entries
   bool stages_ok = true;
   if (!fresh.empty()) {
     for (uint32_t r : fresh) B.used[r] = 1;
@@ -1106,17 +1110,17 @@ static int batch_add(BatchBuild &B, const Lowered &L, const DevPrg &P, uint64_t 
   d[1] = L.ngroups;
   d[2] = (uint32_t)out_off;
   d[3] = nq_slot;
-  // the chain: per conjunct a header (middle bins | edge bins << 8 | negated
-  // << 15), then the slab rows of its middle bins and of its edge bins (made
-  // stage rows by batch_flush)
+  // the chain: one entry per bin, slab row | flags (made stage rows by
+  // batch_finish)
   const uint32_t c0 = h.nchain;
   for (uint32_t i = 0; i < P.ncnf;) {
     uint32_t j = i;
-    while (!(P.cnf_flag[j] & CNF_END)) ++j;  // [i, j] is one conjunct, edges last
-    uint32_t nm = 0, ne = 0;
-    for (uint32_t k = i; k <= j; ++k) (P.cnf_flag[k] & CNF_EDGE) ? ++ne : ++nm;
-    h.chain[h.nchain++] = (uint16_t)(nm | (ne << 8) | ((P.cnf_flag[j] & CNF_NEG) ? 0x8000u : 0u));
-    for (uint32_t k = i; k <= j; ++k) h.chain[h.nchain++] = (uint16_t)slab_row(h, P.cnf_ptr[k]);
+    while (!(P.cnf_flag[j] & CNF_END)) ++j;  // [i, j] is one conjunct
+    for (uint32_t k = i; k <= j; ++k) {
+      uint32_t f = (P.cnf_flag[k] & CNF_EDGE) ? BCH_EDGE : 0u;
+      if (k == j) f |= BCH_LAST | ((P.cnf_flag[j] & CNF_NEG) ? BCH_NEG : 0u);
+      h.chain[h.nchain++] = (uint16_t)((uint32_t)slab_row(h, P.cnf_ptr[k]) | ((f >> 8) << BCH_SLAB_FLAGS));
+    }
     i = j + 1;
   }
   d[4] = c0 | ((h.nchain - c0) << 16);
@@ -1171,13 +1175,11 @@ static mb_status batch_finish(BatchBuild &B, const mb_batch_opts &o, BatchCfg *c
   if (h.nu == 0) return fail(MB_ERR_INVALID, "batch: staging plan over its limits");
   for (uint32_t q = 0; q < h.nq; ++q) {
     const uint32_t c0 = h.Qd[(size_t)q * BQD_WORDS + 4] & 0xffffu, n = h.Qd[(size_t)q * BQD_WORDS + 4] >> 16;
-    for (uint32_t i = c0; i < c0 + n;) {
-      const uint32_t hd = h.chain[i++], m = (hd & 0xffu) + ((hd >> 8) & 0x7fu);
-      for (uint32_t k = 0; k < m; ++k, ++i) {
-        const uint16_t t = h.chain[i] < h.nslab ? stage_of[h.chain[i]] : 0xffffu;
-        if (t >= h.nu) return fail(MB_ERR_INVALID, "batch: chain row %u not staged", (unsigned)h.chain[i]);
-        h.chain[i] = t;
-      }
+    for (uint32_t i = c0; i < c0 + n; ++i) {
+      const uint32_t e = h.chain[i], r = e & BCH_SLAB_ROW;
+      const uint16_t t = r < h.nslab ? stage_of[r] : 0xffffu;
+      if (t >= h.nu || t > BCH_ROW) return fail(MB_ERR_INVALID, "batch: chain row %u not staged", r);
+      h.chain[i] = (uint16_t)(t | ((e >> BCH_SLAB_FLAGS) << 8));
     }
   }
   h.pf_mask = 0;

@@ -124,6 +124,7 @@ struct Engine {
   void free_star();
   void free_denorm();
   void free_bmaps();
+  void drop_index();  // frees the slab and its tensor maps; the levels keep their bounds
   mb_status setup_index_cols();
   // Customer city / part mfgr of a row: the denormalised column when built,
   // else a probe of the dimension through the foreign key.

@@ -63,12 +63,13 @@ struct Launch {
 // device times of completed launches: the plain path as a time per query
 // (exponentially weighted mean), the batched scan as a + b * queries (a
 // least-squares fit with exponentially decaying weights).  A launch of n
-// queries takes the batched scan when a + b * n < n * plain.
+// queries takes the batched scan when a + b * n < n * plain, or when n is
+// beyond the batch sizes the fit has seen.
 struct CostModel {
   double p_ms = 0;  // plain: ms per query
   uint32_t p_cnt = 0;
   double w = 0, wn = 0, wt = 0, wnn = 0, wnt = 0;  // weighted sums over scan launches
-  uint32_t b_cnt = 0;
+  uint32_t b_cnt = 0, b_nmax = 0;                  // scan launches seen, their largest size
   static constexpr double DECAY = 0.97;
   void add_plain(uint32_t n, float ms) {
     const double per = ms / (double)(n ? n : 1);
@@ -79,9 +80,13 @@ struct CostModel {
     w = DECAY * w + 1, wn = DECAY * wn + n, wt = DECAY * wt + ms;
     wnn = DECAY * wnn + (double)n * n, wnt = DECAY * wnt + (double)n * ms;
     ++b_cnt;
+    if (n > b_nmax) b_nmax = n;
   }
   bool ready() const { return p_cnt >= 3 && b_cnt >= 3; }
   bool scan_better(uint32_t n) const {
+    // beyond the largest batch the fit has seen (and at least 8 queries) the
+    // scan is tried: a line fitted on small batches says little about large
+    if (n > b_nmax && n >= 8) return true;
     const double var = w * wnn - wn * wn;
     double a = wt / w, b = 0;
     if (var > 1e-9 * w * w) {  // two or more distinct batch sizes seen

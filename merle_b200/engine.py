@@ -41,6 +41,14 @@ class Engine:
         foreign keys instead of the denormalised per-row columns."""
         check(lib().mb_engine_build_index_ex(self._e, abi.MB_INDEX_PROBE_DIMS if probe_dims else 0))
 
+    def save_index(self, path) -> None:
+        check(lib().mb_engine_save_index(self._e, str(path).encode()))
+
+    def load_index(self, path, probe_dims: bool = False) -> None:
+        """Index file written for this table (mb_engine_save_index)."""
+        check(lib().mb_engine_load_index(self._e, str(path).encode(),
+                                         abi.MB_INDEX_PROBE_DIMS if probe_dims else 0))
+
     def info(self) -> dict:
         i = abi.mb_engine_info()
         check(lib().mb_engine_get_info(self._e, C.byref(i)))

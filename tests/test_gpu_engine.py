@@ -321,3 +321,43 @@ def test_engine_denormalised_equals_probe(cuda, star, orc):
         np.testing.assert_array_equal(nq, wn)
     ep.close()
     ed.close()
+
+
+def test_engine_index_file_roundtrip(cuda, mb, tmp_path):
+    """An index saved to a file and loaded into a fresh engine over the same
+    table answers every query as the built one; a damaged file or a file for
+    another table is refused."""
+    g = G["ssb13"]
+    a = Engine(0)
+    a.gen_star(g["seed"], g["k"], g["n"])
+    a.build_index()
+    f = tmp_path / "star.mbix"
+    a.save_index(f)
+    b = Engine(0)
+    b.gen_star(g["seed"], g["k"], g["n"])
+    b.load_index(f)
+    assert b.info()["nbitmaps"] == a.info()["nbitmaps"] and b.info()["index_bytes"] == a.info()["index_bytes"]
+    qs = WL.ssb13() + WL.random_mix(51, 30, narrow=0.4)
+    for q in qs:
+        oa, na, _ = a.query(q)
+        ob, nb, _ = b.query(q)
+        np.testing.assert_array_equal(oa, ob)
+        assert na == nb
+    ba, bna = a.query_batch(qs)
+    bb, bnb = b.query_batch(qs)
+    np.testing.assert_array_equal(ba, bb)
+    np.testing.assert_array_equal(bna, bnb)
+    raw = bytearray(f.read_bytes())
+    raw[len(raw) // 2] ^= 0x40
+    bad = tmp_path / "bad.mbix"
+    bad.write_bytes(bytes(raw))
+    with pytest.raises(mb.MbError) as ei:
+        b.load_index(bad)
+    assert ei.value.status == abi.MB_ERR_IO
+    c = Engine(0)
+    c.gen_star(g["seed"], g["k"], g["n"] + 1000)
+    with pytest.raises(mb.MbError) as ei:
+        c.load_index(f)
+    assert ei.value.status == abi.MB_ERR_INVALID
+    for e in (a, b, c):
+        e.close()
