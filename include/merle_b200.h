@@ -407,10 +407,10 @@ MB_API mb_status mb_engine_build_index_ex(mb_engine *e, uint32_t flags);
 /* Index files, so an index need not be rebuilt between runs.  No
  * counterpart in the reference (whose on-disk state is the column files,
  * ssb/cpuref.c:8-27).  Layout, little-endian: "MBIX", version 1, table rows,
- * words per bitmap, bitmap count, then per indexed column and level the bin
- * count, the bin bounds (u64) and the rows per bin (u64), then every bitmap
- * of the slab (stride words each), then an FNV-1a 64 hash of everything
- * before it.  Saving needs a built index. */
+ * words per bitmap, bitmap count, level mask, then per kept level its bin
+ * count, bin bounds (u64) and rows per bin (u64), then every bitmap of the
+ * slab (stride words each), then an FNV-1a 64 hash of everything before it.
+ * Saving needs a built index. */
 MB_API mb_status mb_engine_save_index(mb_engine *e, const char *path);
 /* Loads an index file written for this engine's table (same rows, same
  * levels; the caller vouches that the columns are the ones it was built
@@ -440,6 +440,28 @@ typedef struct mb_query {
 
 /* Group count of a query (the reference's NGRP_* formula, ssb/ssbdemo.h:79-87). */
 MB_API uint32_t mb_query_ngroups(const mb_query *q);
+
+/* The index-memory planner.  The canonical index has MB_INDEX_LEVELS
+ * levels; bit i of a level mask keeps level i (column order: date year,
+ * date month, discount, quantity, customer city region, customer city
+ * nation, supplier city region, supplier city nation, part mfgr, part
+ * category).  Every column keeps at least one level.  Generalises the
+ * reference's hand-picked sparse / dense / balanced bin sets
+ * (ssb/bmpidx-create.cu:120-215) into a choice under an HBM budget. */
+#define MB_INDEX_LEVELS 10
+#define MB_LEVELS_ALL 0x3ffu
+/* Builds the index with the levels of level_mask (flags as above). */
+MB_API mb_status mb_engine_build_index_levels(mb_engine *e, uint32_t flags, uint32_t level_mask);
+/* Chooses the levels to keep within budget_bytes for a workload: starting
+ * from every level, it drops the level whose loss raises the workload's
+ * cost least per byte freed (cost = the planner's cover cost: bitmap bytes
+ * read plus candidate-check bytes), until the index fits.  Needs a built
+ * index (its bin row counts).  *level_mask receives the choice;
+ * index_bytes / workload_bytes (may be NULL) its size and the workload's
+ * estimated bytes.  MB_ERR_INVALID if no choice fits the budget. */
+MB_API mb_status mb_engine_plan_index(mb_engine *e, const mb_query *qs, uint32_t n, uint64_t budget_bytes,
+                                      uint32_t *level_mask, uint64_t *index_bytes, uint64_t *workload_bytes);
+
 
 typedef enum mb_plan_kind {
   MB_PLAN_FUSED = 0,        /* virtual program + fused join-probe + group-by */

@@ -115,6 +115,8 @@ class mb_query(C.Structure):
 
 PLAN_FUSED, PLAN_SCAN, PLAN_MATERIALISED = range(3)
 MB_INDEX_PROBE_DIMS = 1
+MB_INDEX_LEVELS = 10
+MB_LEVELS_ALL = 0x3FF
 MB_BATCH_MAX = 128
 PREFETCH_AUTO, PREFETCH_NONE, PREFETCH_ALL = range(3)
 
@@ -216,6 +218,9 @@ SIGNATURES: dict[str, tuple] = {
     "mb_engine_build_index": (I32, [VOIDP]),
     "mb_engine_build_index_ex": (I32, [VOIDP, U32]),
     "mb_engine_save_index": (I32, [VOIDP, C.c_char_p]),
+    "mb_engine_build_index_levels": (I32, [VOIDP, U32, U32]),
+    "mb_engine_plan_index": (I32, [VOIDP, C.POINTER(mb_query), U32, U64, C.POINTER(U32), C.POINTER(U64),
+                                   C.POINTER(U64)]),
     "mb_engine_load_index": (I32, [VOIDP, C.c_char_p, U32]),
     "mb_engine_get_info": (I32, [VOIDP, C.POINTER(mb_engine_info)]),
     "mb_query_ngroups": (U32, [C.POINTER(mb_query)]),

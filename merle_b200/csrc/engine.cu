@@ -276,6 +276,15 @@ mb_status Engine::setup_index_cols() {
   m.src = mfgr_src();
   m.dom_lo = 0, m.dom_hi = 1000;
   m.levels = {lv(range_bounds(0, 1000, 200)), lv(range_bounds(0, 1000, 40))};
+  // keep the levels of level_mask (bit i: the i-th level in column order)
+  uint32_t bit = 0;
+  for (auto &c : idx) {
+    std::vector<Level> keep;
+    for (auto &l : c.levels)
+      if ((level_mask >> bit++) & 1u) keep.push_back(std::move(l));
+    if (keep.empty()) return fail(MB_ERR_INVALID, "index: level mask 0x%x keeps no level of %s", level_mask, c.name);
+    c.levels = std::move(keep);
+  }
   return MB_OK;
 }
 
@@ -312,8 +321,9 @@ static bool exact_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t stri
   return true;
 }
 
-Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t stride, int nchk_sources) {
+Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t stride, int nchk_sources, uint64_t *cost_out) {
   Cover best;
+  if (cost_out) *cost_out = 0;
   lo = std::max(lo, c.dom_lo);
   hi = std::min(hi, c.dom_hi);
   if (lo >= hi) {
@@ -385,7 +395,53 @@ Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t stride, int
       }
     }
   }
+  if (cost_out) *cost_out = best_cost;
   return best;
+}
+
+// ------------------------------------------------------------ index-memory planner
+// Cost in bytes of a workload's predicates under the levels of `mask` (the
+// planner's cover costs), with the bin row counts of the built index.
+static uint64_t workload_cost(const Engine &E, const std::vector<std::vector<Pred>> &preds, uint32_t mask,
+                              bool *ok) {
+  IdxCol cols[IC_N];
+  uint32_t bit = 0;
+  *ok = true;
+  for (int c = 0; c < IC_N; ++c)
+    cols[c].name = E.idx[c].name, cols[c].dom_lo = E.idx[c].dom_lo, cols[c].dom_hi = E.idx[c].dom_hi;
+  // the engine's levels are the kept subset of the canonical list: walk the
+  // canonical bits and pick the built levels in order
+  for (int c = 0; c < IC_N; ++c) {
+    const uint32_t nl = c == IC_DISC || c == IC_QTY ? 1u : 2u;  // canonical levels of the column
+    uint32_t li = 0;
+    for (uint32_t k = 0; k < nl; ++k, ++bit) {
+      const bool built = (E.level_mask >> bit) & 1u;
+      if (built && ((mask >> bit) & 1u)) cols[c].levels.push_back(E.idx[c].levels[li]);
+      if (built) ++li;
+    }
+    if (cols[c].levels.empty()) *ok = false;
+  }
+  if (!*ok) return UINT64_MAX;
+  uint64_t total = 0;
+  for (const auto &ps : preds)
+    for (const Pred &p : ps) {
+      uint64_t cst = 0;
+      plan_cover(cols[p.col], p.lo, p.hi, E.stride, 1, &cst);
+      if (cst == UINT64_MAX) {
+        *ok = false;
+        return UINT64_MAX;
+      }
+      total += cst;
+    }
+  return total;
+}
+
+static uint64_t mask_bytes(const Engine &E, uint32_t mask) {
+  static const uint32_t nbins[MB_INDEX_LEVELS] = {7, 84, 11, 50, 5, 25, 5, 25, 5, 25};
+  uint64_t b = 0;
+  for (uint32_t i = 0; i < MB_INDEX_LEVELS; ++i)
+    if ((mask >> i) & 1u) b += (uint64_t)nbins[i] * E.stride * 4;
+  return b;
 }
 
 uint32_t query_ngroups(const mb_query &q) {
@@ -660,9 +716,15 @@ extern "C" mb_status mb_engine_load_star(mb_engine *e, const mb_star_host *h) {
 extern "C" mb_status mb_engine_build_index(mb_engine *e) { return mb_engine_build_index_ex(e, 0); }
 
 extern "C" mb_status mb_engine_build_index_ex(mb_engine *e, uint32_t flags) {
+  return mb_engine_build_index_levels(e, flags, MB_LEVELS_ALL);
+}
+
+extern "C" mb_status mb_engine_build_index_levels(mb_engine *e, uint32_t flags, uint32_t level_mask) {
   if (!e) return fail(MB_ERR_INVALID, "mb_engine_build_index: NULL engine");
   if (flags & ~MB_INDEX_PROBE_DIMS) return fail(MB_ERR_INVALID, "mb_engine_build_index_ex: flags 0x%x", flags);
+  if (level_mask & ~MB_LEVELS_ALL) return fail(MB_ERR_INVALID, "mb_engine_build_index_levels: mask 0x%x", level_mask);
   Engine &E = e->E;
+  E.level_mask = level_mask;
   if (!E.custkey) return fail(MB_ERR_INVALID, "mb_engine_build_index: no table");
   MB_CUDA(cudaSetDevice(E.device));
   E.drop_index();
@@ -695,6 +757,43 @@ extern "C" mb_status mb_engine_build_index_ex(mb_engine *e, uint32_t flags) {
   cudaEventElapsedTime(&E.index_build_ms, E.ev0, E.ev1);
   free_one(E.allocs, d_pop);
   E.indexed = true;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_engine_plan_index(mb_engine *e, const mb_query *qs, uint32_t n, uint64_t budget,
+                                          uint32_t *level_mask, uint64_t *index_bytes, uint64_t *workload_bytes) {
+  if (!e || (!qs && n) || !level_mask) return fail(MB_ERR_INVALID, "mb_engine_plan_index: NULL argument");
+  Engine &E = e->E;
+  if (!E.indexed) return fail(MB_ERR_INVALID, "mb_engine_plan_index: build an index first (its bin row counts)");
+  std::vector<std::vector<Pred>> preds(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    if (qs[i].tmpl < 1 || qs[i].tmpl > 4) return fail(MB_ERR_INVALID, "mb_engine_plan_index: template %u", qs[i].tmpl);
+    query_preds(qs[i], preds[i]);
+  }
+  uint32_t mask = E.level_mask;
+  bool ok = false;
+  uint64_t cost = workload_cost(E, preds, mask, &ok);
+  if (!ok) return fail(MB_ERR_INVALID, "mb_engine_plan_index: the built index cannot cover the workload");
+  while (mask_bytes(E, mask) > budget) {
+    int best = -1;
+    double best_rate = 0;
+    uint64_t best_cost = 0;
+    for (uint32_t i = 0; i < MB_INDEX_LEVELS; ++i) {
+      if (!((mask >> i) & 1u)) continue;
+      bool ok2 = false;
+      const uint64_t c2 = workload_cost(E, preds, mask & ~(1u << i), &ok2);
+      if (!ok2) continue;
+      const double rate = ((double)c2 - (double)cost) / (double)mask_bytes(E, 1u << i);
+      if (best < 0 || rate < best_rate) best = (int)i, best_rate = rate, best_cost = c2;
+    }
+    if (best < 0)
+      return fail(MB_ERR_INVALID, "mb_engine_plan_index: no level set fits %llu bytes", (unsigned long long)budget);
+    mask &= ~(1u << best);
+    cost = best_cost;
+  }
+  *level_mask = mask;
+  if (index_bytes) *index_bytes = mask_bytes(E, mask);
+  if (workload_bytes) *workload_bytes = cost;
   return MB_OK;
 }
 

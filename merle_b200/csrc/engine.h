@@ -85,6 +85,10 @@ struct Engine {
   // with one 2-D tensor copy.
   uint32_t *islab = nullptr;
   uint32_t nbm = 0;  // bitmaps in the slab
+  // Levels the index keeps (bit i: the i-th level in column order; the
+  // canonical index has 10: date year/month, discount, quantity, customer
+  // and supplier city region/nation, part mfgr/category).
+  uint32_t level_mask = MB_LEVELS_ALL;
   void *bmaps[3] = {};  // the slab's tensor maps for tiles of 32, 64, 128 words (device)
   bool indexed = false;
   float index_build_ms = 0;
@@ -141,7 +145,9 @@ struct SsbSrc {
 void ssb_build_op(const SsbSrc &S, const mb_query &q, mb_op &out);
 
 // Planner and lowering (engine.cu).
-Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t W, int nchk_sources);
+// The cheapest cover of [lo, hi) with c's levels; *cost_out (if given) = its
+// cost in bytes (bitmap bytes + candidate-check sectors of its edge rows).
+Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t W, int nchk_sources, uint64_t *cost_out = nullptr);
 mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered &L);
 uint32_t query_ngroups(const mb_query &q);
 mb_status run_lowered(Engine &E, Lowered &L, const mb_plan &plan, int64_t *d_out, uint64_t *d_nq, bool zero);

@@ -59,7 +59,7 @@ extern "C" mb_status mb_engine_save_index(mb_engine *e, const char *path) {
   F.f = fopen(path, "wb");
   if (!F.f) return fail(MB_ERR_IO, "mb_engine_save_index: cannot create %s", path);
   bool ok = F.put("MBIX", 4) && F.put(&MBIX_VERSION, 4) && F.put(&E.nrows, 8) && F.put(&E.stride, 8) &&
-            F.put(&E.nbm, 4);
+            F.put(&E.nbm, 4) && F.put(&E.level_mask, 4);
   for (auto &c : E.idx)
     for (auto &l : c.levels) {
       const uint32_t nb = l.nbins();
@@ -90,18 +90,21 @@ extern "C" mb_status mb_engine_load_index(mb_engine *e, const char *path, uint32
   File F;
   F.f = fopen(path, "rb");
   if (!F.f) return fail(MB_ERR_IO, "mb_engine_load_index: cannot open %s", path);
+  char magic[4];
+  uint32_t ver = 0, nbm = 0, mask = 0;
+  uint64_t nrows = 0, stride = 0;
+  if (!F.get(magic, 4) || memcmp(magic, "MBIX", 4) != 0 || !F.get(&ver, 4) || ver != MBIX_VERSION)
+    return fail(MB_ERR_IO, "mb_engine_load_index: %s is not an index file (version %u)", path, MBIX_VERSION);
+  if (!F.get(&nrows, 8) || !F.get(&stride, 8) || !F.get(&nbm, 4) || !F.get(&mask, 4))
+    return fail(MB_ERR_IO, "mb_engine_load_index: %s: short header", path);
+  if (mask == 0 || (mask & ~MB_LEVELS_ALL))
+    return fail(MB_ERR_INVALID, "mb_engine_load_index: %s: level mask 0x%x", path, mask);
   E.drop_index();
   MB_CUDA(cudaEventRecord(E.ev0, E.stream));
   if (flags & MB_INDEX_PROBE_DIMS) E.free_denorm();
   else MB_CHECK(E.build_denorm());
-  MB_CHECK(E.setup_index_cols());  // the levels this table's index has
-  char magic[4];
-  uint32_t ver = 0, nbm = 0;
-  uint64_t nrows = 0, stride = 0;
-  if (!F.get(magic, 4) || memcmp(magic, "MBIX", 4) != 0 || !F.get(&ver, 4) || ver != MBIX_VERSION)
-    return fail(MB_ERR_IO, "mb_engine_load_index: %s is not an index file (version %u)", path, MBIX_VERSION);
-  if (!F.get(&nrows, 8) || !F.get(&stride, 8) || !F.get(&nbm, 4))
-    return fail(MB_ERR_IO, "mb_engine_load_index: %s: short header", path);
+  E.level_mask = mask;
+  MB_CHECK(E.setup_index_cols());  // the levels the file's index has
   uint32_t want = 0;
   for (auto &c : E.idx)
     for (auto &l : c.levels) want += l.nbins();

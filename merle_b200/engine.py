@@ -41,6 +41,20 @@ class Engine:
         foreign keys instead of the denormalised per-row columns."""
         check(lib().mb_engine_build_index_ex(self._e, abi.MB_INDEX_PROBE_DIMS if probe_dims else 0))
 
+    def build_index_levels(self, level_mask: int, probe_dims: bool = False) -> None:
+        """The index with only the levels of level_mask (mb_engine_plan_index)."""
+        check(lib().mb_engine_build_index_levels(self._e, abi.MB_INDEX_PROBE_DIMS if probe_dims else 0,
+                                                 level_mask))
+
+    def plan_index(self, qs, budget_bytes: int) -> tuple[int, int, int]:
+        """(level mask, index bytes, workload bytes) of the levels to keep
+        within budget_bytes for the workload qs."""
+        n = len(qs)
+        qarr = (abi.mb_query * max(n, 1))(*qs)
+        m, ib, wb = C.c_uint32(0), C.c_uint64(0), C.c_uint64(0)
+        check(lib().mb_engine_plan_index(self._e, qarr, n, budget_bytes, C.byref(m), C.byref(ib), C.byref(wb)))
+        return m.value, ib.value, wb.value
+
     def save_index(self, path) -> None:
         check(lib().mb_engine_save_index(self._e, str(path).encode()))
 

@@ -361,3 +361,44 @@ def test_engine_index_file_roundtrip(cuda, mb, tmp_path):
     assert ei.value.status == abi.MB_ERR_INVALID
     for e in (a, b, c):
         e.close()
+
+
+def test_engine_index_planner(cuda, mb, tmp_path):
+    """The index-memory planner drops levels to fit a budget (the workload's
+    estimated bytes rise), an index built with its choice answers every query
+    as the full one, and an index file keeps the choice."""
+    g = G["ssb13"]
+    e = Engine(0)
+    e.gen_star(g["seed"], g["k"], g["n"])
+    e.build_index()
+    full = e.info()["index_bytes"]
+    qs = WL.random_mix(61, 200, narrow=0.3)
+    m_all, b_all, w_all = e.plan_index(qs, full)
+    assert m_all == abi.MB_LEVELS_ALL and b_all == full
+    m, b, w = e.plan_index(qs, int(full * 0.6))
+    assert b <= full * 0.6 and m != abi.MB_LEVELS_ALL and w >= w_all
+    want = [e.query(q)[:2] for q in qs[:40]]
+    wb = e.query_batch(qs[:40])
+    e.build_index_levels(m)
+    assert e.info()["index_bytes"] == b
+    for q, (o, n) in zip(qs[:40], want):
+        out, nq, _ = e.query(q)
+        np.testing.assert_array_equal(out, o)
+        assert nq == n
+    ob, nb = e.query_batch(qs[:40])
+    np.testing.assert_array_equal(ob, wb[0])
+    np.testing.assert_array_equal(nb, wb[1])
+    f = tmp_path / "small.mbix"
+    e.save_index(f)
+    e2 = Engine(0)
+    e2.gen_star(g["seed"], g["k"], g["n"])
+    e2.load_index(f)
+    assert e2.info()["index_bytes"] == b
+    out, nq, _ = e2.query(qs[0])
+    np.testing.assert_array_equal(out, want[0][0])
+    with pytest.raises(mb.MbError):
+        e.plan_index(qs, full // 10)  # below the smallest index (one level per column)
+    with pytest.raises(mb.MbError):
+        e.build_index_levels(0x3fe & ~0x3)  # no date level
+    e.close()
+    e2.close()
