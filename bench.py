@@ -191,7 +191,7 @@ def reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-            "data": "synthetic", "config": config_of(args, n),
+            "data": "synthetic", "config": config_of(args, args.rows or 6_000_000 * args.k),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": f"{len(qs)}-query mix over the first {n:,} rows (ssb_schema widths), "
                                        f"one query per thread"},
