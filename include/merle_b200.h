@@ -537,8 +537,8 @@ typedef enum mb_prefetch {
   MB_PREFETCH_ALL = 2       /* every column an op reads for every selected row */
 } mb_prefetch;
 typedef struct mb_batch_opts {
-  uint32_t words_per_lane;  /* 1, 2 or 4 (0 = 4, narrower if a tile does not fit): a tile is
-                               1024 * words_per_lane rows */
+  uint32_t words_per_lane;  /* 1, 2, 4 or 6 (0 = 4, narrower if a tile does not fit): a tile
+                               is 1024 * words_per_lane rows */
   uint32_t warps;           /* warps per CTA, 2..16 (0 = 16) */
   uint32_t stages;          /* at most this many staged tiles in flight per CTA, 1..4
                                (0 = 4); fewer if they do not fit in shared memory */

@@ -459,7 +459,11 @@ __device__ __forceinline__ bool job_run(const BCtx &C) {
 
 template <int V>
 __device__ __forceinline__ void lds_words(const uint32_t *p, uint32_t (&x)[V]) {
-  if (V == 4) {
+  if (V == 6) {  // 24 bytes a lane: three 8-byte loads
+    const uint2 a = reinterpret_cast<const uint2 *>(p)[0], b = reinterpret_cast<const uint2 *>(p)[1],
+                c = reinterpret_cast<const uint2 *>(p)[2];
+    x[0] = a.x, x[1] = a.y, x[2 % V] = b.x, x[3 % V] = b.y, x[4 % V] = c.x, x[5 % V] = c.y;
+  } else if (V == 4) {
     const uint4 t = *reinterpret_cast<const uint4 *>(p);
     x[0] = t.x, x[1] = t.y, x[2] = t.z, x[3] = t.w;
   } else if (V == 2) {
@@ -761,7 +765,7 @@ batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParam
 }  // namespace
 
 size_t batch_smem(const BatchHdr &h, const BatchCfg &c) {
-  if (c.V != 1 && c.V != 2 && c.V != 4) return 0;
+  if (c.V != 1 && c.V != 2 && c.V != 4 && c.V != 6) return 0;
   if (c.warps < 2 || c.warps > BW_MAX || c.stages == 0 || c.stages > 4 || c.drainers == 0 || c.drainers >= c.warps)
     return 0;
   return blayout(h.nq, h.nchain, h.nu, c.warps, c.stages, 32 * c.V).total;
@@ -858,6 +862,7 @@ mb_status batch_scan(const BatchHdr &h, const BatchHdr *dh, const BatchCfg &c, c
   if (batch_smem(h, c) == 0) return fail(MB_ERR_INVALID, "batch: launch shape V=%u warps=%u stages=%u", c.V,
                                          c.warps, c.stages);
   switch (c.V) {
+  case 6: return launch_bs<6>(h, dh, c, maps, out, nqual, st);
   case 4: return launch_bs<4>(h, dh, c, maps, out, nqual, st);
   case 2: return launch_bs<2>(h, dh, c, maps, out, nqual, st);
   default: return launch_bs<1>(h, dh, c, maps, out, nqual, st);

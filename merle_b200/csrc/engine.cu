@@ -1255,7 +1255,7 @@ static BatchCfg batch_cfg(const BatchHdr &h, const mb_batch_opts &o) {
       if (batch_smem(h, c) && batch_smem(h, c) <= cap) break;
     if (batch_smem(h, c) && batch_smem(h, c) <= cap) break;  // (one stage, if that is all that fits)
     if (c.V == 1 || o.words_per_lane) break;
-    c.V >>= 1;  // not even one stage of this tile fits: narrower tiles
+    c.V = c.V == 6 ? 4 : c.V >> 1;  // not even one stage of this tile fits: narrower tiles
   }
   return c;
 }
@@ -1350,7 +1350,7 @@ static mb_status batch_plan(Engine &E, const mb_query *qs, uint32_t n, const mb_
 // The slab's tensor maps for tile width T, in device memory (encoded once
 // per index).
 static mb_status batch_maps(Engine &E, uint32_t V, const void **out) {
-  const int k = V == 4 ? 2 : V == 2 ? 1 : 0;
+  const int k = V == 6 ? 3 : V == 4 ? 2 : V == 2 ? 1 : 0;
   if (!E.bmaps[k]) {
     std::vector<uint8_t> host(BMAP_COUNT * BMAP_BYTES);
     MB_CHECK(batch_encode_maps(E.islab, E.stride, E.nbm, 32 * V, host.data()));
@@ -1366,7 +1366,8 @@ static mb_status batch_maps(Engine &E, uint32_t V, const void **out) {
 static mb_status batch_staging(Engine &E, BatchHdr **out, uint32_t *slot);
 
 static mb_status batch_opts_check(const mb_batch_opts &o, const char *who) {
-  if ((o.words_per_lane && o.words_per_lane != 1 && o.words_per_lane != 2 && o.words_per_lane != 4) ||
+  if ((o.words_per_lane && o.words_per_lane != 1 && o.words_per_lane != 2 && o.words_per_lane != 4 &&
+       o.words_per_lane != 6) ||
       o.warps == 1 || o.warps > 16 || o.stages > 4 || o.prefetch > MB_PREFETCH_ALL ||
       o.drain_warps >= (o.warps ? o.warps : 16u))
     return fail(MB_ERR_INVALID, "%s: options out of range", who);
@@ -1610,7 +1611,7 @@ extern "C" mb_status mb_engine_tune_batch(mb_engine *e, const mb_query *qs, uint
     return MB_OK;
   };
   // tile width x warps (default drain warps: about a fifth)
-  for (uint32_t V : {4u, 2u, 1u})
+  for (uint32_t V : {6u, 4u, 2u, 1u})
     for (uint32_t w : {16u, 12u, 8u}) {
       mb_batch_opts o;
       memset(&o, 0, sizeof(o));

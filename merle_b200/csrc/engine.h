@@ -89,7 +89,7 @@ struct Engine {
   // canonical index has 10: date year/month, discount, quantity, customer
   // and supplier city region/nation, part mfgr/category).
   uint32_t level_mask = MB_LEVELS_ALL;
-  void *bmaps[3] = {};  // the slab's tensor maps for tiles of 32, 64, 128 words (device)
+  void *bmaps[4] = {};  // the slab's tensor maps for tiles of 32, 64, 128, 192 words (device)
   bool indexed = false;
   float index_build_ms = 0;
   // query scratch

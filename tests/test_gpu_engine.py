@@ -165,6 +165,8 @@ BATCH_OPTS = [
     (4, 16, 0, 0, abi.PREFETCH_AUTO),
     (2, 4, 1, 2, abi.PREFETCH_AUTO),
     (2, 12, 0, 0, abi.PREFETCH_AUTO),
+    (6, 16, 0, 0, abi.PREFETCH_AUTO),
+    (6, 12, 1, 3, abi.PREFETCH_NONE),
 ]
 
 
