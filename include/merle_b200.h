@@ -418,6 +418,18 @@ MB_API mb_status mb_engine_save_index(mb_engine *e, const char *path);
  * hash mismatch, MB_ERR_INVALID if the file does not fit the table. */
 MB_API mb_status mb_engine_load_index(mb_engine *e, const char *path, uint32_t flags);
 
+/* Column files in the reference's format (ssb/cpuref.c:8-27: a 4-byte
+ * element-width header, then the n elements): one host array written to
+ * path.  MB_ERR_IO on a file error. */
+MB_API mb_status mb_write_column(const char *path, const void *host, uint64_t n, uint32_t width);
+/* The engine's table as the reference's SSB column files in dir (the files
+ * ssb_load reads: the nine fact columns in ssb_schema widths, custCity and
+ * partMfgr with zero-filled custMktSegment, partName, partColor, partType,
+ * partSize and partContainer of the same lengths), so the reference's own
+ * drivers can run on data generated here.  The table must hold ssb_schema
+ * widths or 4-byte columns whose values fit them. */
+MB_API mb_status mb_engine_save_ssb(mb_engine *e, const char *dir);
+
 typedef struct mb_engine_info {
   uint64_t nrows, fact_bytes, dim_bytes, index_bytes;
   uint32_t k, width4, nbitmaps, sms;
@@ -586,7 +598,8 @@ MB_API mb_status mb_batch_graph_destroy(mb_batch_graph *g);
  * mix (median of reps launches, CUDA events on the engine stream) over tile
  * widths x warps, then drain warps, then L2 prefetch, each stage keeping the
  * best so far; *best receives the fastest options, *best_ms its time,
- * *tried the shapes timed. */
+ * *tried the shapes timed.  The engine keeps the result: later batches
+ * enqueued with opts == NULL use it (a new index forgets it). */
 MB_API mb_status mb_engine_tune_batch(mb_engine *e, const mb_query *qs, uint32_t n, uint32_t reps,
                                       mb_batch_opts *best, float *best_ms, uint32_t *tried);
 

@@ -218,6 +218,8 @@ SIGNATURES: dict[str, tuple] = {
     "mb_engine_build_index": (I32, [VOIDP]),
     "mb_engine_build_index_ex": (I32, [VOIDP, U32]),
     "mb_engine_save_index": (I32, [VOIDP, C.c_char_p]),
+    "mb_write_column": (I32, [C.c_char_p, VOIDP, U64, U32]),
+    "mb_engine_save_ssb": (I32, [VOIDP, C.c_char_p]),
     "mb_engine_build_index_levels": (I32, [VOIDP, U32, U32]),
     "mb_engine_plan_index": (I32, [VOIDP, C.POINTER(mb_query), U32, U64, C.POINTER(U32), C.POINTER(U64),
                                    C.POINTER(U64)]),

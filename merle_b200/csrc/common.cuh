@@ -4,9 +4,19 @@
 #include <stdint.h>
 #include <stdio.h>
 #include <string>
+#include <nvtx3/nvToolsExt.h>
 #include "merle_b200.h"
 
 namespace mb {
+
+// An NVTX range over a scope (engine phases show up by name in Nsight
+// Systems; without a profiler attached the calls do nothing).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // ---------------------------------------------------------------- errors
 // Thread-local message of the last failing call (mb_last_error()).

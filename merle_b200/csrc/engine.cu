@@ -48,6 +48,7 @@ mb_status Engine::alloc(void **p, size_t bytes) {
 static void free_one(std::vector<void *> &allocs, void *p);
 
 void Engine::drop_index() {
+  have_tuned = false;
   for (auto &c : idx)
     for (auto &l : c.levels) l.slab = nullptr;
   free_one(allocs, islab);
@@ -720,6 +721,7 @@ extern "C" mb_status mb_engine_build_index_ex(mb_engine *e, uint32_t flags) {
 }
 
 extern "C" mb_status mb_engine_build_index_levels(mb_engine *e, uint32_t flags, uint32_t level_mask) {
+  NvtxRange nvtx_("mb_engine_build_index");
   if (!e) return fail(MB_ERR_INVALID, "mb_engine_build_index: NULL engine");
   if (flags & ~MB_INDEX_PROBE_DIMS) return fail(MB_ERR_INVALID, "mb_engine_build_index_ex: flags 0x%x", flags);
   if (level_mask & ~MB_LEVELS_ALL) return fail(MB_ERR_INVALID, "mb_engine_build_index_levels: mask 0x%x", level_mask);
@@ -883,6 +885,7 @@ mb_status run_lowered(Engine &E, Lowered &L, const mb_plan &plan, int64_t *d_out
 
 extern "C" mb_status mb_engine_query(mb_engine *e, const mb_query *q, const mb_plan *plan, int64_t *out_host,
                                      uint64_t *nqual_host, mb_query_stats *stats) {
+  NvtxRange nvtx_("mb_engine_query");
   if (!e || !q || !out_host) return fail(MB_ERR_INVALID, "mb_engine_query: NULL argument");
   Engine &E = e->E;
   MB_CUDA(cudaSetDevice(E.device));
@@ -921,6 +924,7 @@ extern "C" uint64_t mb_queries_layout(const mb_query *qs, uint32_t n, uint64_t *
 
 extern "C" mb_status mb_engine_enqueue(mb_engine *e, const mb_query *qs, uint32_t n, const mb_plan *plans,
                                        int64_t *out_dev, uint64_t *nqual_dev, int record_times) {
+  NvtxRange nvtx_("mb_engine_enqueue");
   if (!e || (!qs && n) || !out_dev || !nqual_dev) return fail(MB_ERR_INVALID, "mb_engine_enqueue: NULL argument");
   Engine &E = e->E;
   MB_CUDA(cudaSetDevice(E.device));
@@ -1435,11 +1439,13 @@ static mb_status batch_staging(Engine &E, BatchHdr **out, uint32_t *slot) {
 
 extern "C" mb_status mb_engine_enqueue_batch(mb_engine *e, const mb_query *qs, uint32_t n, const mb_batch_opts *opts,
                                              int64_t *out_dev, uint64_t *nqual_dev) {
+  NvtxRange nvtx_("mb_engine_enqueue_batch");
   if (!e || (!qs && n) || !out_dev || !nqual_dev) return fail(MB_ERR_INVALID, "mb_engine_enqueue_batch: NULL argument");
   Engine &E = e->E;
   MB_CUDA(cudaSetDevice(E.device));
   mb_batch_opts o;
   if (opts) o = *opts;
+  else if (E.have_tuned) o = E.tuned;  // the autotuner's last choice
   else memset(&o, 0, sizeof(o));
   MB_CHECK(batch_opts_check(o, "mb_engine_enqueue_batch"));
   BatchPlanned P;
@@ -1455,6 +1461,7 @@ extern "C" mb_status mb_engine_batch_info(mb_engine *e, const mb_query *qs, uint
   MB_CUDA(cudaSetDevice(E.device));
   mb_batch_opts o;
   if (opts) o = *opts;
+  else if (E.have_tuned) o = E.tuned;  // the autotuner's last choice
   else memset(&o, 0, sizeof(o));
   MB_CHECK(batch_opts_check(o, "mb_engine_batch_info"));
   BatchPlanned P;
@@ -1521,6 +1528,7 @@ extern "C" mb_status mb_batch_graph_create(mb_engine *e, const mb_query *qs, uin
   MB_CUDA(cudaSetDevice(E.device));
   mb_batch_opts o;
   if (opts) o = *opts;
+  else if (E.have_tuned) o = E.tuned;  // the autotuner's last choice
   else memset(&o, 0, sizeof(o));
   MB_CHECK(batch_opts_check(o, "mb_batch_graph_create"));
   BatchPlanned P;
@@ -1562,6 +1570,7 @@ extern "C" mb_status mb_batch_graph_launch(mb_batch_graph *g) {
 // ------------------------------------------------------------ autotuner
 extern "C" mb_status mb_engine_tune_batch(mb_engine *e, const mb_query *qs, uint32_t n, uint32_t reps,
                                           mb_batch_opts *best, float *best_ms, uint32_t *tried) {
+  NvtxRange nvtx_("mb_engine_tune_batch");
   if (!e || !qs || n == 0 || !best) return fail(MB_ERR_INVALID, "mb_engine_tune_batch: bad argument");
   Engine &E = e->E;
   MB_CUDA(cudaSetDevice(E.device));
@@ -1634,6 +1643,8 @@ extern "C" mb_status mb_engine_tune_batch(mb_engine *e, const mb_query *qs, uint
     MB_CHECK(consider(o));
   }
   *best = b;
+  E.tuned = b;
+  E.have_tuned = true;
   if (best_ms) *best_ms = bms;
   if (tried) *tried = count;
   return MB_OK;
@@ -1795,6 +1806,7 @@ extern "C" mb_status mb_engine_set_planner(mb_engine *e, mb_mlp *m) {
 
 extern "C" mb_status mb_engine_plan_learned(mb_engine *e, const mb_query *qs, uint32_t n, mb_plan *plans,
                                            uint32_t *chosen) {
+  NvtxRange nvtx_("mb_engine_plan_learned");
   if (!e || (n && (!qs || !plans))) return fail(MB_ERR_INVALID, "mb_engine_plan_learned: NULL argument");
   Engine &E = e->E;
   MB_CUDA(cudaSetDevice(E.device));

@@ -112,6 +112,9 @@ struct Engine {
   void *bq_host[BQ_RING] = {}, *bq_dev = nullptr;
   cudaEvent_t bq_copied[BQ_RING] = {};
   uint32_t bq_next = 0;
+  // the autotuner's last launch shape, used by batches enqueued without options
+  mb_batch_opts tuned{};
+  bool have_tuned = false;
   int64_t *bout = nullptr;  // device results of mb_engine_query_batch
   uint64_t bout_cap = 0;
   // timing: per-query event pairs of the last enqueue, and markers

@@ -312,6 +312,7 @@ extern "C" mb_status mb_mlp_gradients(mb_mlp *M, const float *x, const float *t,
 
 extern "C" mb_status mb_mlp_train(mb_mlp *M, const float *x, const float *t, const float *mask, uint32_t n,
                                   const mb_mlp_train_opts *o, float *final_loss) {
+  NvtxRange nvtx_("mb_mlp_train");
   if (!M || !x || !t || !mask || !o || n == 0) return fail(MB_ERR_INVALID, "mb_mlp_train: bad argument");
   if (o->batch == 0 || o->epochs == 0) return fail(MB_ERR_INVALID, "mb_mlp_train: batch and epochs must be > 0");
   MB_CUDA(cudaSetDevice(M->device));

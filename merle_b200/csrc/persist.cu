@@ -51,6 +51,7 @@ struct Pinned {
 using namespace mb;
 
 extern "C" mb_status mb_engine_save_index(mb_engine *e, const char *path) {
+  NvtxRange nvtx_("mb_engine_save_index");
   if (!e || !path) return fail(MB_ERR_INVALID, "mb_engine_save_index: NULL argument");
   Engine &E = e->E;
   if (!E.indexed) return fail(MB_ERR_INVALID, "mb_engine_save_index: no index built");
@@ -82,6 +83,7 @@ extern "C" mb_status mb_engine_save_index(mb_engine *e, const char *path) {
 }
 
 extern "C" mb_status mb_engine_load_index(mb_engine *e, const char *path, uint32_t flags) {
+  NvtxRange nvtx_("mb_engine_load_index");
   if (!e || !path) return fail(MB_ERR_INVALID, "mb_engine_load_index: NULL argument");
   if (flags & ~MB_INDEX_PROBE_DIMS) return fail(MB_ERR_INVALID, "mb_engine_load_index: flags 0x%x", flags);
   Engine &E = e->E;
@@ -152,5 +154,101 @@ extern "C" mb_status mb_engine_load_index(mb_engine *e, const char *path, uint32
   MB_CUDA(cudaStreamSynchronize(E.stream));
   cudaEventElapsedTime(&E.index_build_ms, E.ev0, E.ev1);
   E.indexed = true;
+  return MB_OK;
+}
+
+// ------------------------------------------------------------ column files
+extern "C" mb_status mb_write_column(const char *path, const void *host, uint64_t n, uint32_t width) {
+  if (!path || (!host && n)) return fail(MB_ERR_INVALID, "mb_write_column: NULL argument");
+  if (width != 1 && width != 2 && width != 4 && width != 8) return fail(MB_ERR_INVALID, "mb_write_column: width %u", width);
+  FILE *f = fopen(path, "wb");
+  if (!f) return fail(MB_ERR_IO, "mb_write_column: cannot create %s", path);
+  bool ok = fwrite(&width, 4, 1, f) == 1 && (n == 0 || fwrite(host, width, n, f) == n);
+  ok = (fclose(f) == 0) && ok;
+  if (!ok) return fail(MB_ERR_IO, "mb_write_column: writing %s failed", path);
+  return MB_OK;
+}
+
+namespace mb {
+namespace {
+
+// A device column of n elements of width `from` written as a column file of
+// width `to` (values narrowed; the caller checked they fit), in pieces
+// through a pinned buffer.
+mb_status write_dev_column(Engine &E, const char *dir, const char *name, const void *dev, uint64_t n, uint32_t from,
+                           uint32_t to) {
+  char path[1024];
+  snprintf(path, sizeof(path), "%s/%s", dir, name);
+  FILE *f = fopen(path, "wb");
+  if (!f) return fail(MB_ERR_IO, "mb_engine_save_ssb: cannot create %s", path);
+  struct Closer {
+    FILE *f;
+    ~Closer() {
+      if (f) fclose(f);
+    }
+  } closer{f};
+  Pinned buf;
+  MB_CUDA(cudaMallocHost(&buf.p, CHUNK));
+  std::vector<uint8_t> out(CHUNK / from * to);
+  bool ok = fwrite(&to, 4, 1, f) == 1;
+  const uint64_t per = CHUNK / from;
+  for (uint64_t i = 0; ok && i < n; i += per) {
+    const uint64_t m = n - i < per ? n - i : per;
+    MB_CUDA(cudaMemcpyAsync(buf.p, static_cast<const uint8_t *>(dev) + i * from, m * from, cudaMemcpyDeviceToHost,
+                            E.stream));
+    MB_CUDA(cudaStreamSynchronize(E.stream));
+    const uint8_t *src = static_cast<const uint8_t *>(buf.p);
+    if (from == to) {
+      ok = fwrite(src, 1, m * to, f) == m * to;
+      continue;
+    }
+    for (uint64_t j = 0; j < m; ++j) {
+      uint64_t v = 0;
+      memcpy(&v, src + j * from, from);
+      memcpy(out.data() + j * to, &v, to);  // little-endian: the low bytes
+    }
+    ok = fwrite(out.data(), 1, m * to, f) == m * to;
+  }
+  closer.f = nullptr;
+  ok = (fclose(f) == 0) && ok;
+  if (!ok) return fail(MB_ERR_IO, "mb_engine_save_ssb: writing %s failed", path);
+  return MB_OK;
+}
+
+}  // namespace
+}  // namespace mb
+
+extern "C" mb_status mb_engine_save_ssb(mb_engine *e, const char *dir) {
+  if (!e || !dir) return fail(MB_ERR_INVALID, "mb_engine_save_ssb: NULL argument");
+  Engine &E = e->E;
+  if (!E.custkey) return fail(MB_ERR_INVALID, "mb_engine_save_ssb: no table");
+  MB_CUDA(cudaSetDevice(E.device));
+  // the reference's ssb_schema widths (ssb/ssbdemo.h:41-49)
+  struct {
+    const char *file, *col;
+    const void *dev;
+    uint32_t to;
+  } fact[] = {{"loCustKey", "custkey", E.custkey, 4},         {"loPartKey", "partkey", E.partkey, 4},
+              {"loOrderDate", "orderdate", E.orderdate, 2},   {"loExtendedPrice", "extendedprice", E.extendedprice, 4},
+              {"loRevenue", "revenue", E.revenue, 4},         {"loSupplyCost", "supplycost", E.supplycost, 4},
+              {"loSuppCity", "suppcity", E.suppcity, 1},      {"loQuantity", "quantity", E.quantity, 1},
+              {"loDiscount", "discount", E.discount, 1}};
+  for (auto &c : fact) MB_CHECK(write_dev_column(E, dir, c.file, c.dev, E.nrows, E.fact_width(c.col), c.to));
+  const uint64_t nc = E.ncust + 1, np = E.npart + 1;
+  MB_CHECK(write_dev_column(E, dir, "custCity", E.custcity, nc, 1, 1));
+  MB_CHECK(write_dev_column(E, dir, "partMfgr", E.partmfgr, np, 2, 2));
+  // the dimension attributes no query here reads: zeros of the same lengths
+  std::vector<uint8_t> z(np * 2 > nc ? np * 2 : nc, 0);
+  char path[1024];
+  struct {
+    const char *file;
+    uint64_t n;
+    uint32_t w;
+  } zeros[] = {{"custMktSegment", nc, 1}, {"partName", np, 2},     {"partColor", np, 1},
+               {"partType", np, 1},       {"partSize", np, 1},     {"partContainer", np, 1}};
+  for (auto &c : zeros) {
+    snprintf(path, sizeof(path), "%s/%s", dir, c.file);
+    MB_CHECK(mb_write_column(path, z.data(), c.n, c.w));
+  }
   return MB_OK;
 }

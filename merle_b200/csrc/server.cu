@@ -187,6 +187,7 @@ void mb_server::finish(Request *r, int32_t status) {
 // lock held; the lock is released around the engine calls).  Returns false
 // if nothing could launch.
 bool mb_server::launch_some(std::unique_lock<std::mutex> &lk) {
+  NvtxRange nvtx_("mb_server launch");
   const uint32_t maxb = o.mode == MB_SERVE_PLAIN ? 1 : o.max_batch;
   if (o.mode == MB_SERVE_PLAIN && !pending.front()->planned) {
     // a plain-mode request is planned when it reaches the front: its plan

@@ -55,6 +55,10 @@ class Engine:
         check(lib().mb_engine_plan_index(self._e, qarr, n, budget_bytes, C.byref(m), C.byref(ib), C.byref(wb)))
         return m.value, ib.value, wb.value
 
+    def save_ssb(self, dirname) -> None:
+        """The table as the reference's SSB column files (ssb_load's format)."""
+        check(lib().mb_engine_save_ssb(self._e, str(dirname).encode()))
+
     def save_index(self, path) -> None:
         check(lib().mb_engine_save_index(self._e, str(path).encode()))
 

@@ -150,3 +150,26 @@ def test_synth_demoall(cuda, mb, synth_dir):
     (the reference's own driver flow, synth/cpuref.c:180-253)."""
     L = _lib(mb)
     assert L.synth_demoall(str(synth_dir).encode())
+
+
+def test_engine_table_exported_for_the_reference_drivers(cuda, mb, tmp_path):
+    """A table generated here, written as the reference's column files
+    (mb_engine_save_ssb), runs through the reference's driver flow and gives
+    the reference's golden results."""
+    from merle_b200.engine import Engine
+    g = G["ssb13"]
+    e = Engine(0)
+    e.gen_star(g["seed"], g["k"], g["n"], width4=True)
+    e.save_ssb(tmp_path)
+    e.close()
+    L = _lib(mb)
+    h = SsbSchema()
+    n = L.ssb_load(C.byref(h), None, str(tmp_path).encode())
+    assert n == g["n"]
+    try:
+        r = L.ssb_cpujoin(C.byref(h), n)
+        got = np.ctypeslib.as_array(r, shape=(SUMGRP_ALL,)).copy()
+        np.testing.assert_array_equal(got, np.load(GOLDEN / "ssb13_ref_u32.npy"))
+    finally:
+        L.ssb_free(C.byref(h), None)
+    assert L.ssb_demoall(str(tmp_path).encode())
