@@ -645,17 +645,21 @@ MB_API mb_status mb_mlp_train(mb_mlp *m, const float *x, const float *t, const f
                               const mb_mlp_train_opts *opts, float *final_loss);
 
 #define MB_PLAN_FEATURES 32
-#define MB_PLAN_CANDIDATES 12
+#define MB_PLAN_CANDIDATES 16
 /* A query's planner features (MB_PLAN_FEATURES floats): template, per
  * predicate its bins, edge bins and estimated selectivity (bin popcounts),
  * the popcount of the whole program on the first 1% of the rows (a GPU
- * pass), column and group-domain sizes. */
+ * pass), group-domain size, bitmap count (slot 28, once the table size, is
+ * zero: planning must not depend on a size the network was not trained
+ * over). */
 MB_API mb_status mb_engine_query_features(mb_engine *e, const mb_query *q, float *features);
 /* Candidate plan idx (0 = the rule plan) of a query: fused or materialised
- * predicates, predicate order, group-by strategy, tile width, staging, scan. */
+ * predicates, predicate order, group-by strategy, tile width, staging, scan,
+ * and four pairs of these (tile width with group-by strategy or order). */
 MB_API mb_status mb_engine_plan_candidate(mb_engine *e, const mb_query *q, uint32_t idx, mb_plan *out);
 /* The network the engine plans with (borrowed: it must outlive its use);
- * NULL returns to the rule planner. */
+ * NULL returns to the rule planner.  It must map MB_PLAN_FEATURES inputs to
+ * MB_PLAN_CANDIDATES outputs (MB_ERR_INVALID otherwise). */
 MB_API mb_status mb_engine_set_planner(mb_engine *e, mb_mlp *m);
 /* Plans n queries with the network (one BF16 forward pass for all of them):
  * plans[i] = the candidate with the least predicted time, chosen[i] its

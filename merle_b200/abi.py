@@ -138,7 +138,7 @@ class mb_plan(C.Structure):
 
 
 MB_PLAN_FEATURES = 32
-MB_PLAN_CANDIDATES = 12
+MB_PLAN_CANDIDATES = 16
 
 
 class mb_mlp_config(C.Structure):

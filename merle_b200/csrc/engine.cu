@@ -1739,7 +1739,7 @@ static mb_status features_of(Engine &E, const mb_query &q, QueryFacts &F, float 
   f[25] = nlog10(ssel, 1e-7, 7.0);
   f[26] = (float)sunc;
   f[27] = log2f((float)std::max<uint32_t>(1, F.L.ngroups)) / 16.f;
-  f[28] = (float)log10((double)std::max<uint64_t>(1, E.nrows)) / 10.f;
+  f[28] = 0.f;  // the table size is left out: trained at one size, planning at another must not extrapolate it
   f[29] = F.L.chk ? 1.f : 0.f;
   f[30] = (float)F.L.nbitmaps / 64.f;
   f[31] = 1.f;
@@ -1775,6 +1775,14 @@ static void candidate_of(const QueryFacts &F, uint32_t idx, mb_plan &p) {
   case 9: p.launch.grp_strategy = MB_GRP_GLOBAL; break;
   case 10: p.launch.grp_strategy = MB_GRP_HASH; break;
   case 11: p.launch.staging = MB_STAGE_TMA; break;
+  // pairs of the single changes that were most often best on their own
+  case 12: p.launch.words_per_lane = 4, p.launch.grp_strategy = MB_GRP_GLOBAL; break;
+  case 13: p.launch.words_per_lane = 1, p.launch.grp_strategy = MB_GRP_GLOBAL; break;
+  case 14: p.order_mode = 1, p.launch.words_per_lane = 4; break;
+  case 15:
+    p.launch.words_per_lane = 4;
+    if (F.L.ngroups <= 4096) p.launch.grp_strategy = MB_GRP_SHARED;
+    break;
   default: break;  // 0: the rule plan
   }
 }
@@ -1800,6 +1808,10 @@ extern "C" mb_status mb_engine_plan_candidate(mb_engine *e, const mb_query *q, u
 
 extern "C" mb_status mb_engine_set_planner(mb_engine *e, mb_mlp *m) {
   if (!e) return fail(MB_ERR_INVALID, "mb_engine_set_planner: NULL engine");
+  uint32_t in = 0, out = 0;
+  if (m && (!mlp_shape(m, &in, &out) || in != MB_PLAN_FEATURES || out != MB_PLAN_CANDIDATES))
+    return fail(MB_ERR_INVALID, "mb_engine_set_planner: the network maps %u features to %u plans, the engine needs "
+                "%u to %u", in, out, MB_PLAN_FEATURES, MB_PLAN_CANDIDATES);
   e->E.planner = m;
   return MB_OK;
 }

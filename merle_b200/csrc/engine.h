@@ -147,6 +147,9 @@ struct SsbSrc {
 };
 void ssb_build_op(const SsbSrc &S, const mb_query &q, mb_op &out);
 
+// The layer widths of a planner network (mlp.cu); false for NULL.
+bool mlp_shape(const mb_mlp *m, uint32_t *in, uint32_t *out);
+
 // Planner and lowering (engine.cu).
 // The cheapest cover of [lo, hi) with c's levels; *cost_out (if given) = its
 // cost in bytes (bitmap bytes + candidate-check sectors of its edge rows).

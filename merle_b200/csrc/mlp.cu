@@ -216,6 +216,14 @@ float init_weight(uint64_t seed, uint32_t i, uint32_t fan_in) {
 }  // namespace
 }  // namespace mb
 
+namespace mb {
+bool mlp_shape(const mb_mlp *m, uint32_t *in, uint32_t *out) {
+  if (!m) return false;
+  *in = m->cfg.in, *out = m->cfg.out;
+  return true;
+}
+}  // namespace mb
+
 using namespace mb;
 
 extern "C" mb_status mb_mlp_create(int device, const mb_mlp_config *cfg, mb_mlp **out) {

@@ -1,6 +1,6 @@
-"""The learned planner: a 3-layer perceptron (32 -> 64 -> 64 -> 12) that
+"""The learned planner: a 3-layer perceptron (32 -> 64 -> 64 -> 16) that
 predicts, from a query's features, the log slowdown of each of the engine's
-12 candidate plans against the fastest of them; the engine runs the candidate
+16 candidate plans against the fastest of them; the engine runs the candidate
 with the least prediction.
 
 Everything numeric runs in libmerleb200.so: the features (bin counts and
@@ -35,7 +35,8 @@ NF = abi.MB_PLAN_FEATURES
 NC = abi.MB_PLAN_CANDIDATES
 CANDIDATE_NAMES = ["rule", "template-order", "tile-4", "tile-1", "materialise-most-selective",
                    "materialise-all-but-least", "materialised-plan", "scan", "grp-shared", "grp-global",
-                   "grp-hash", "stage-tma"]
+                   "grp-hash", "stage-tma", "tile-4+grp-global", "tile-1+grp-global", "template-order+tile-4",
+                   "tile-4+grp-shared"]
 
 
 def _f32p(a: np.ndarray):

@@ -145,3 +145,16 @@ def test_learned_planner_gains_over_rule(eng24):
     print("learned planner, 200 held-out queries at 24M rows:", r)
     assert r["regret_total"] <= 1.15
     assert r["speedup_vs_rule_total"] >= 1.0
+
+
+def test_planner_network_shape_checked(net, eng24, mb):
+    """A network whose outputs are not one per candidate plan is refused."""
+    from merle_b200 import lib
+    assert net.nout != P.NC
+    assert lib().mb_engine_set_planner(eng24.handle, net.handle) == mb.abi.MB_ERR_INVALID
+    m = P.MLP(seed=1)
+    try:
+        assert lib().mb_engine_set_planner(eng24.handle, m.handle) == mb.abi.MB_OK
+        assert lib().mb_engine_set_planner(eng24.handle, None) == mb.abi.MB_OK
+    finally:
+        m.close()
