@@ -696,9 +696,11 @@ typedef struct mb_server_opts {
   uint32_t max_inflight;    /* launches on the GPU at once, 1..8 (0 = 2) */
   uint32_t use_planner;     /* plain-path launches plan with the engine's learned planner
                                (mb_engine_set_planner) */
-  uint32_t min_batch;       /* batched mode: launches of fewer queries run them on the plain
-                               path, one after another (1 = always the batched scan); 0 = an
-                               online cost model of both kinds decides per launch */
+  uint32_t min_batch;       /* batched mode: fewer queued queries than this run on the plain
+                               path, one query per launch (1 = always the batched scan); 0 = an
+                               online cost model decides per launch: while the plain path keeps
+                               up with the arrival rate, the scan only when it lowers the queued
+                               queries' summed completion time; past that, the cheaper per query */
   uint32_t pad_;
   mb_batch_opts batch;      /* batched-scan launch shape */
 } mb_server_opts;

@@ -61,19 +61,41 @@ struct Launch {
 
 // Online cost model of the batched server's two launch kinds, from the
 // device times of completed launches: the plain path as a time per query
-// (exponentially weighted mean), the batched scan as a + b * queries (a
-// least-squares fit with exponentially decaying weights).  A launch of n
-// queries takes the batched scan when a + b * n < n * plain, or when n is
-// beyond the batch sizes the fit has seen.
+// (decayed mean over about the last 128 queries), the batched scan as
+// a + b * queries (a least-squares fit with exponentially decaying weights),
+// and the arrival rate (decayed mean gap between submits).
+//
+// While the plain path alone keeps up with the arrivals (plain time per query
+// below OVERLOAD of the mean gap) the queue stays short and what matters is
+// latency: n queued queries take the batched scan only when that lowers the
+// sum of their completion times, a + b * n < plain * (n + 1) / 2 (one after
+// another they complete at plain, 2 plain, ..., n plain).  Past that load
+// the queue grows and throughput decides: the scan when a + b * n < n * plain,
+// or when n is beyond the batch sizes the fit has seen.
 struct CostModel {
-  double p_ms = 0;  // plain: ms per query
+  // plain: ms per query, a decayed mean over the recent plain queries (the
+  // load is the mean service time over the mean gap, not the latest query's)
+  double p_ms = 0, p_sum = 0, p_w = 0;
   uint32_t p_cnt = 0;
   double w = 0, wn = 0, wt = 0, wnn = 0, wnt = 0;  // weighted sums over scan launches
   uint32_t b_cnt = 0, b_nmax = 0;                  // scan launches seen, their largest size
-  static constexpr double DECAY = 0.97;
+  // mean gap between arrivals: decayed sums of gaps and of weights, so that
+  // the first few gaps give their plain mean rather than the first alone
+  double g_sum = 0, g_w = 0, last_us = -1;
+  static constexpr double DECAY = 0.97, GAP_DECAY = 1 - 1.0 / 128, OVERLOAD = 0.95;
+  void add_arrival(double t_us) {
+    if (last_us >= 0) {
+      g_sum = GAP_DECAY * g_sum + (t_us - last_us) * 1e-3;
+      g_w = GAP_DECAY * g_w + 1;
+    }
+    last_us = t_us;
+  }
+  bool overloaded() const { return p_cnt && g_w >= 8 && p_ms * g_w >= OVERLOAD * g_sum; }
   void add_plain(uint32_t n, float ms) {
-    const double per = ms / (double)(n ? n : 1);
-    p_ms = p_cnt ? 0.9 * p_ms + 0.1 * per : per;
+    const double k = (double)(n ? n : 1), d = pow(GAP_DECAY, k);
+    p_sum = d * p_sum + ms;
+    p_w = d * p_w + k;
+    p_ms = p_sum / p_w;
     ++p_cnt;
   }
   void add_scan(uint32_t n, float ms) {
@@ -84,9 +106,11 @@ struct CostModel {
   }
   bool ready() const { return p_cnt >= 3 && b_cnt >= 3; }
   bool scan_better(uint32_t n) const {
-    // beyond the largest batch the fit has seen (and at least 8 queries) the
-    // scan is tried: a line fitted on small batches says little about large
-    if (n > b_nmax && n >= 8) return true;
+    const bool over = overloaded();
+    // under overload, beyond the largest batch the fit has seen (and at
+    // least 8 queries) the scan is tried: a line fitted on small batches
+    // says little about large
+    if (over && n > b_nmax && n >= 8) return true;
     const double var = w * wnn - wn * wn;
     double a = wt / w, b = 0;
     if (var > 1e-9 * w * w) {  // two or more distinct batch sizes seen
@@ -94,7 +118,7 @@ struct CostModel {
       a = (wt - b * wn) / w;
       if (b < 0) b = 0, a = wt / w;
     }
-    return a + b * n < n * p_ms;
+    return over ? a + b * n < n * p_ms : a + b * n < 0.5 * (n + 1) * p_ms;
   }
 };
 
@@ -225,6 +249,25 @@ bool mb_server::launch_some(std::unique_lock<std::mutex> &lk) {
     bytes += tb;
   }
   if (take.empty()) return false;
+  // batched mode: the batched scan takes the whole lot (a fixed min_batch,
+  // or the cost model once it has seen both kinds; until then 6 queries
+  // when the plain path falls behind the arrivals);
+  // otherwise the plain path runs one query per launch and the rest stay
+  // queued for the next launches, so each answer returns when its own query
+  // is done rather than when the last of the lot is
+  const uint32_t nt = (uint32_t)take.size();
+  bool scan;
+  if (o.mode == MB_SERVE_PLAIN) scan = false;
+  else if (o.min_batch) scan = nt >= o.min_batch;
+  else scan = cost.ready() ? nt >= 2 && cost.scan_better(nt) : nt >= 6 && cost.overloaded();
+  if (!scan && nt > 1) {
+    for (size_t i = take.size(); i-- > 1;) {
+      pending.push_front(take[i]);
+      res -= take[i]->foot;
+      bytes -= 8ull * (take[i]->ngroups + 1);
+    }
+    take.resize(1);
+  }
   // Arena space, contiguous.  Launches complete in stream order, so the live
   // tables are [tail, head) or, once the head wrapped, [tail, end) + [0, head).
   uint64_t off = 0;
@@ -257,12 +300,7 @@ bool mb_server::launch_some(std::unique_lock<std::mutex> &lk) {
     }
   }
   L->reqs = take;
-  // batched mode: the batched scan or the plain path (a fixed min_batch, or
-  // the cost model once it has seen both kinds; until then 6 queries)
-  const uint32_t nt = (uint32_t)take.size();
-  if (o.mode == MB_SERVE_PLAIN) L->scan = false;
-  else if (o.min_batch) L->scan = nt >= o.min_batch;
-  else L->scan = cost.ready() ? nt >= 2 && cost.scan_better(nt) : nt >= 6;
+  L->scan = scan;
   L->off = off;
   L->bytes = bytes;
   L->reserved = res;
@@ -481,6 +519,7 @@ extern "C" mb_status mb_server_submit(mb_server *s, const mb_query *q, int64_t *
     r->foot = 8ull * (r->ngroups + 1);
     r->id = s->next_id++;
     r->info.t_submit_us = s->now_us();
+    s->cost.add_arrival(r->info.t_submit_us);
     s->reqs[r->id] = r;
     s->pending.push_back(r);
     ++s->stats.submitted;

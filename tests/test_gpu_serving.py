@@ -45,7 +45,8 @@ def _layout(qs):
 
 
 @pytest.mark.parametrize("mode,rate,min_batch", [(abi.SERVE_BATCHED, 20000.0, 0), (abi.SERVE_BATCHED, 2000.0, 0),
-                                                 (abi.SERVE_BATCHED, 2000.0, 1), (abi.SERVE_PLAIN, 20000.0, 0)])
+                                                 (abi.SERVE_BATCHED, 20000.0, 1), (abi.SERVE_BATCHED, 2000.0, 1),
+                                                 (abi.SERVE_PLAIN, 20000.0, 0)])
 def test_serving_results_equal_alone(eng, mix, alone, mode, rate, min_batch):
     with SV.Server(eng, mode, min_batch=min_batch) as s:
         out, info = s.run_load(mix, rate, seed=3)
@@ -57,8 +58,10 @@ def test_serving_results_equal_alone(eng, mix, alone, mode, rate, min_batch):
         assert info[i].nqual == alone[i][1]
         assert info[i].t_submit_us <= info[i].t_launch_us <= info[i].t_done_us
     assert st["completed"] == len(mix) and st["failed"] == 0
-    if mode == abi.SERVE_BATCHED and rate >= 20000:
-        assert st["launches"] < len(mix)  # requests shared launches
+    if mode == abi.SERVE_BATCHED and rate >= 20000 and min_batch == 1:
+        assert st["launches"] < len(mix) and st["scan_launches"] == st["launches"]  # requests shared launches
+    if mode == abi.SERVE_BATCHED:
+        assert st["launched_queries"] == len(mix)
     if mode == abi.SERVE_PLAIN:
         assert st["launches"] == len(mix)
     r = SV.summarize(info, rate)
