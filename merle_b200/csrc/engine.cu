@@ -37,6 +37,7 @@ Engine::~Engine() {
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (stream) cudaStreamDestroy(stream);
+  if (pstream) cudaStreamDestroy(pstream);
 }
 
 mb_status Engine::alloc(void **p, size_t bytes) {
@@ -1702,47 +1703,68 @@ static float nlog10(double x, double floor_, double span) {  // log10 scaled int
   return (float)((log10(std::max(x, floor_)) - log10(floor_)) / span);
 }
 
-static mb_status features_of(Engine &E, const mb_query &q, QueryFacts &F, float *f) {
-  MB_CHECK(query_facts(E, q, F));
-  memset(f, 0, MB_PLAN_FEATURES * sizeof(float));
-  if (q.tmpl >= 1 && q.tmpl <= 4) f[q.tmpl - 1] = 1.f;
-  double sel = 1;
-  for (uint32_t i = 0; i < F.npred; ++i) {
-    float *g = f + 4 + 5 * i;
-    g[0] = log2f(1.f + (float)F.nb[i]) / 6.f;
-    g[1] = (float)F.ne[i] * 0.5f;
-    g[2] = nlog10(F.est[i], 1e-7, 7.0);
-    g[3] = F.comp[i] ? 1.f : 0.f;
-    g[4] = F.full[i] ? 1.f : 0.f;
-    sel *= F.est[i];
+// Features of n queries.  Each query's program is popcounted over the first
+// 1% of the rows (its possible and uncertain bits): the sample passes of a
+// chunk of queries are launched back to back and waited for once.
+static constexpr uint32_t FEAT_CHUNK = 64;
+
+static mb_status features_of(Engine &E, const mb_query *qs, uint32_t n, QueryFacts *F, float *x) {
+  if (!E.d_feat) MB_CHECK(E.alloc((void **)&E.d_feat, 16 * FEAT_CHUNK));
+  if (!E.pstream) MB_CUDA(cudaStreamCreateWithFlags(&E.pstream, cudaStreamNonBlocking));
+  std::vector<unsigned long long> h(2 * FEAT_CHUNK);
+  std::vector<uint64_t> sampled(FEAT_CHUNK);
+  for (uint32_t c0 = 0; c0 < n; c0 += FEAT_CHUNK) {
+    const uint32_t m = std::min(FEAT_CHUNK, n - c0);
+    MB_CUDA(cudaMemsetAsync(E.d_feat, 0, 16 * m, E.pstream));
+    for (uint32_t j = 0; j < m; ++j) {
+      QueryFacts &Fi = F[c0 + j];
+      MB_CHECK(query_facts(E, qs[c0 + j], Fi));
+      sampled[j] = 0;
+      if (Fi.L.empty || Fi.L.prg.ncols + Fi.L.prg.instrs[0].opcode == 0) continue;
+      DevPrg P;
+      bool v4 = false;
+      MB_CHECK(flatten_prg(&Fi.L.prg, 1, &P, &v4));
+      const uint64_t nw = std::max<uint64_t>(1, P.nwords / 100);
+      const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(nw, 256), 148ull * 4);
+      sample_popc_kernel<<<grid, 256, 0, E.pstream>>>(P, nw, E.d_feat + 2 * j);
+      MB_LAUNCH_CHECK("sample_popc_kernel");
+      sampled[j] = nw;
+    }
+    MB_CUDA(cudaMemcpyAsync(h.data(), E.d_feat, 16 * m, cudaMemcpyDeviceToHost, E.pstream));
+    MB_CUDA(cudaStreamSynchronize(E.pstream));
+    for (uint32_t j = 0; j < m; ++j) {
+      const QueryFacts &Fi = F[c0 + j];
+      const mb_query &q = qs[c0 + j];
+      float *f = x + (size_t)(c0 + j) * MB_PLAN_FEATURES;
+      memset(f, 0, MB_PLAN_FEATURES * sizeof(float));
+      if (q.tmpl >= 1 && q.tmpl <= 4) f[q.tmpl - 1] = 1.f;
+      double sel = 1;
+      for (uint32_t i = 0; i < Fi.npred; ++i) {
+        float *g = f + 4 + 5 * i;
+        g[0] = log2f(1.f + (float)Fi.nb[i]) / 6.f;
+        g[1] = (float)Fi.ne[i] * 0.5f;
+        g[2] = nlog10(Fi.est[i], 1e-7, 7.0);
+        g[3] = Fi.comp[i] ? 1.f : 0.f;
+        g[4] = Fi.full[i] ? 1.f : 0.f;
+        sel *= Fi.est[i];
+      }
+      f[24] = nlog10(sel, 1e-9, 9.0);
+      double ssel = 0, sunc = 0;
+      if (sampled[j]) {
+        const unsigned long long pc = h[2 * j], uc = h[2 * j + 1];
+        const double rows = (double)std::min<uint64_t>(E.nrows, sampled[j] * 32);
+        ssel = (double)pc / std::max(1.0, rows);
+        sunc = pc ? (double)uc / (double)pc : 0.0;
+      }
+      f[25] = nlog10(ssel, 1e-7, 7.0);
+      f[26] = (float)sunc;
+      f[27] = log2f((float)std::max<uint32_t>(1, Fi.L.ngroups)) / 16.f;
+      f[28] = 0.f;  // the table size is left out: trained at one size, planning at another must not extrapolate it
+      f[29] = Fi.L.chk ? 1.f : 0.f;
+      f[30] = (float)Fi.L.nbitmaps / 64.f;
+      f[31] = 1.f;
+    }
   }
-  f[24] = nlog10(sel, 1e-9, 9.0);
-  // popcount of the whole program on the first 1% of the rows
-  double ssel = 0, sunc = 0;
-  if (!F.L.empty && F.L.prg.ncols + F.L.prg.instrs[0].opcode > 0) {
-    DevPrg P;
-    bool v4 = false;
-    MB_CHECK(flatten_prg(&F.L.prg, 1, &P, &v4));
-    const uint64_t nw = std::max<uint64_t>(1, P.nwords / 100);
-    if (!E.d_feat) MB_CHECK(E.alloc((void **)&E.d_feat, 16));
-    MB_CUDA(cudaMemsetAsync(E.d_feat, 0, 16, E.stream));
-    const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(nw, 256), 148ull * 4);
-    sample_popc_kernel<<<grid, 256, 0, E.stream>>>(P, nw, E.d_feat);
-    MB_LAUNCH_CHECK("sample_popc_kernel");
-    unsigned long long h[2] = {0, 0};
-    MB_CUDA(cudaMemcpyAsync(h, E.d_feat, 16, cudaMemcpyDeviceToHost, E.stream));
-    MB_CUDA(cudaStreamSynchronize(E.stream));
-    const double rows = (double)std::min<uint64_t>(E.nrows, nw * 32);
-    ssel = (double)h[0] / std::max(1.0, rows);
-    sunc = h[0] ? (double)h[1] / (double)h[0] : 0.0;
-  }
-  f[25] = nlog10(ssel, 1e-7, 7.0);
-  f[26] = (float)sunc;
-  f[27] = log2f((float)std::max<uint32_t>(1, F.L.ngroups)) / 16.f;
-  f[28] = 0.f;  // the table size is left out: trained at one size, planning at another must not extrapolate it
-  f[29] = F.L.chk ? 1.f : 0.f;
-  f[30] = (float)F.L.nbitmaps / 64.f;
-  f[31] = 1.f;
   return MB_OK;
 }
 
@@ -1794,7 +1816,7 @@ extern "C" mb_status mb_engine_query_features(mb_engine *e, const mb_query *q, f
   Engine &E = e->E;
   MB_CUDA(cudaSetDevice(E.device));
   QueryFacts F;
-  return features_of(E, *q, F, features);
+  return features_of(E, q, 1, &F, features);
 }
 
 extern "C" mb_status mb_engine_plan_candidate(mb_engine *e, const mb_query *q, uint32_t idx, mb_plan *out) {
@@ -1824,7 +1846,7 @@ extern "C" mb_status mb_engine_plan_learned(mb_engine *e, const mb_query *qs, ui
   MB_CUDA(cudaSetDevice(E.device));
   std::vector<QueryFacts> F(n);
   std::vector<float> x((size_t)n * MB_PLAN_FEATURES);
-  for (uint32_t i = 0; i < n; ++i) MB_CHECK(features_of(E, qs[i], F[i], &x[(size_t)i * MB_PLAN_FEATURES]));
+  if (n) MB_CHECK(features_of(E, qs, n, F.data(), x.data()));
   std::vector<uint32_t> pick(n, 0);
   if (E.planner && n) {
     const uint32_t no = mb_mlp_nparams(E.planner) ? MB_PLAN_CANDIDATES : 0;

@@ -104,7 +104,11 @@ struct Engine {
   uint64_t rows_cap = 0;
   uint64_t *d_rowcnt = nullptr;  // row count of the materialised plan
   std::vector<void *> allocs;
-  unsigned long long *d_feat = nullptr;  // the planner's sample popcounts
+  unsigned long long *d_feat = nullptr;  // the planner's sample popcounts, a pair per query
+  // the planner's sample pass runs on its own stream: it reads only the index
+  // slab, complete once indexed is set, and waiting for it must not wait for
+  // queries in flight on the engine stream
+  cudaStream_t pstream = nullptr;
   mb_mlp *planner = nullptr;             // borrowed (mb_engine_set_planner)
   // batch descriptors: a ring of pinned host staging headers (each reusable
   // once its copy event completed) and the device copy

@@ -48,6 +48,10 @@ struct Request {
   mb_request_info info{};
 };
 
+// a batched-mode plain launch plans its query and up to this many queued
+// ones in one learned-planner call
+constexpr size_t PLAN_AHEAD = 15;
+
 struct Launch {
   std::vector<Request *> reqs;
   bool scan = false;  // the batched scan (else the plain path, query by query)
@@ -316,6 +320,20 @@ bool mb_server::launch_some(std::unique_lock<std::mutex> &lk) {
   if (f_slow) --f_slow, slow = f_slow_us;
   if (f_alloc) --f_alloc, f_a = true;
   else if (f_launch) --f_launch, f_l = true;
+  // a batched-mode launch on the plain path plans with the learned planner
+  // when it is on: its query together with up to PLAN_AHEAD queued ones not
+  // yet planned, so that one sample wait and one network pass serve several
+  // launches (cancel leaves a request alone while it is being planned)
+  std::vector<Request *> ahead;
+  const bool learn = o.mode == MB_SERVE_BATCHED && !scan && o.use_planner && eng->E.planner && !f_a && !f_l;
+  if (learn && !take[0]->planned) {
+    ahead.push_back(take[0]);
+    for (Request *r : pending) {
+      if (ahead.size() > PLAN_AHEAD) break;
+      if (!r->planned && !r->planning) ahead.push_back(r);
+    }
+    for (Request *r : ahead) r->planning = true;
+  }
   inflight.push_back(L);
   ++stats.launches;
   stats.launched_queries += take.size();
@@ -335,24 +353,27 @@ bool mb_server::launch_some(std::unique_lock<std::mutex> &lk) {
   for (uint32_t i = 0; i < n; ++i) qs[i] = take[i]->q, total += take[i]->ngroups;
   int64_t *out_dev = reinterpret_cast<int64_t *>(arena + off);
   uint64_t *nq_dev = reinterpret_cast<uint64_t *>(out_dev + total);
-  // a batched-mode launch on the plain path plans with the learned planner
-  // when it is on (before the launch's first event: planning runs a sample
-  // pass and waits for it)
-  std::vector<mb_plan> pl;
-  bool learned = false;
-  if (o.mode == MB_SERVE_BATCHED && !L->scan && o.use_planner && E.planner && !f_a && !f_l) {
-    pl.resize(n);
-    std::vector<uint32_t> pick(n, 0);
-    learned = mb_engine_plan_learned(eng, qs.data(), n, pl.data(), pick.data()) == MB_OK;
-    for (uint32_t i = 0; i < n; ++i) take[i]->info.plan = learned ? pick[i] : 0;
+  // planning comes before the launch's first event (it waits for its sample
+  // pass, on the planner's own stream)
+  std::vector<mb_plan> ahead_plans(ahead.size());
+  std::vector<uint32_t> ahead_pick(ahead.size(), 0);
+  bool ahead_ok = false;
+  if (!ahead.empty()) {
+    std::vector<mb_query> aq(ahead.size());
+    for (size_t i = 0; i < ahead.size(); ++i) aq[i] = ahead[i]->q;
+    ahead_ok = mb_engine_plan_learned(eng, aq.data(), (uint32_t)aq.size(), ahead_plans.data(), ahead_pick.data()) ==
+               MB_OK;
   }
+  const bool learned = learn && (take[0]->planned || ahead_ok);
+  const mb_plan *lplan = take[0]->planned ? &take[0]->plan : ahead_ok ? &ahead_plans[0] : nullptr;
+  if (learn) take[0]->info.plan = take[0]->planned ? take[0]->info.plan : ahead_ok ? ahead_pick[0] : 0;
   mb_status s = MB_OK;
   if (f_a) s = fail(MB_ERR_OOM, "serving: injected arena allocation failure");
   if (s == MB_OK && cudaEventRecord(L->ev0, st) != cudaSuccess) s = fail(MB_ERR_CUDA, "serving: event record");
   if (s == MB_OK && f_l) s = fail(MB_ERR_CUDA, "serving: injected launch failure");
   if (s == MB_OK) {
     if (o.mode == MB_SERVE_PLAIN) s = mb_engine_enqueue(eng, qs.data(), 1, &take[0]->plan, out_dev, nq_dev, 0);
-    else if (!L->scan) s = mb_engine_enqueue(eng, qs.data(), n, learned ? pl.data() : nullptr, out_dev, nq_dev, 0);
+    else if (!L->scan) s = mb_engine_enqueue(eng, qs.data(), n, learned ? lplan : nullptr, out_dev, nq_dev, 0);
     else s = mb_engine_enqueue_batch(eng, qs.data(), n, &o.batch, out_dev, nq_dev);
   }
   if (s == MB_OK && cudaMemcpyAsync(mirror + off, arena + off, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
@@ -361,6 +382,11 @@ bool mb_server::launch_some(std::unique_lock<std::mutex> &lk) {
     s = fail(MB_ERR_CUDA, "serving: error word copy");
   cudaEventRecord(L->ev1, st);
   lk.lock();
+  for (size_t i = 0; i < ahead.size(); ++i) {
+    Request *r = ahead[i];
+    r->planning = false;
+    if (ahead_ok) r->plan = ahead_plans[i], r->info.plan = ahead_pick[i], r->planned = true;
+  }
   L->st = s;
   return true;
 }

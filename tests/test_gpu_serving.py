@@ -134,18 +134,28 @@ def test_wait_timeout_and_unknown_id(eng, mb):
             s.wait(rid, 1)  # already handed out
 
 
-def test_plain_mode_with_learned_planner(eng, mix, alone):
+@pytest.mark.parametrize("mode,min_batch,rate", [(abi.SERVE_PLAIN, 0, 5000.0), (abi.SERVE_BATCHED, 65, 50000.0)])
+def test_learned_planner_in_the_serving_loop(eng, mix, alone, mode, min_batch, rate):
+    """Plain mode plans each request at the front of the queue; batched mode
+    held to the plain path (min_batch above max_batch) plans a launch's query
+    with the queued ones ahead of it in one planner call."""
     from merle_b200 import planner as P
     m = P.MLP(seed=5)  # untrained: any candidate may come out, answers must not change
     try:
         from merle_b200 import lib, check
         check(lib().mb_engine_set_planner(eng.handle, m.handle))
-        with SV.Server(eng, abi.SERVE_PLAIN, use_planner=True, mem_budget=1 << 30) as s:
-            out, info = s.run_load(mix[:60], 5000.0, seed=6)
+        with SV.Server(eng, mode, use_planner=True, mem_budget=1 << 30, min_batch=min_batch) as s:
+            out, info = s.run_load(mix[:60], rate, seed=6)
+            st = s.stats()
         check(lib().mb_engine_set_planner(eng.handle, None))
     finally:
         m.close()
     offs = _layout(mix[:60])
+    plans = set()
     for i in range(60):
         assert info[i].status == abi.MB_OK
         np.testing.assert_array_equal(out[offs[i]:offs[i + 1]], alone[i][0])
+        assert info[i].nqual == alone[i][1] and info[i].batch_size == 1
+        plans.add(info[i].plan)
+    assert plans <= set(range(P.NC))
+    assert st["launches"] == 60 and st["scan_launches"] == 0
