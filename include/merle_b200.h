@@ -759,6 +759,59 @@ typedef enum mb_fault {
 } mb_fault;
 MB_API mb_status mb_server_inject(mb_server *s, uint32_t fault, uint32_t count, uint32_t arg_us);
 
+/* ------------------------------------------------------------------------
+ * WAH compressed bitmaps: interop with the reference's compressed-bitmap
+ * baseline (merle/wahGpu.cuh:5-44, merle/host/wahCpu.h, ssb/wah-demo.cu).
+ *
+ * A WAH stream cuts the rows into 31-bit groups: a literal word (bit 31 clear)
+ * holds one group in bits 0..30; a fill word (bit 31 set) stands for a run of
+ * all-0 (bit 30 clear) or all-1 (bit 30 set) groups, the run length in bits
+ * 0..29 (merle/host/wahCpu.c:20-24).  Row 31g + j of group g is bit j
+ * (MB_WAH_LSB, as the reference's loadArrayFile sets them,
+ * merle/host/wahConv.c:85-87) or bit 30 - j (MB_WAH_MSB, as its simpleJoin and
+ * dbjoinFlatWah build them, wahConv.c:142-144, wahGpuCmprs.cu:215-226).
+ * Streams written here are canonical (maximal runs: wahCmprsCPU's output,
+ * wahConv.c:36-57).  All pointers are device pointers except in
+ * mb_wah_save / mb_wah_load; scratch is stream-ordered (cudaMallocAsync).
+ *
+ * A decoded stream is an ordinary bitmap of this library (stride
+ * mb_bitmap_stride words, padding zeroed), so it can be a bin of any mb_col
+ * operand of a virtual bitmap program: this is the compressed-operand hook
+ * the reference declares but never defines (vprg::_cmprs_adapt_run,
+ * primitive.cuh:334-337). */
+typedef enum mb_wah_order { MB_WAH_LSB = 0, MB_WAH_MSB = 1 } mb_wah_order;
+typedef enum mb_wah_opcode { MB_WAH_AND = 0, MB_WAH_OR = 1, MB_WAH_XOR = 2 } mb_wah_opcode;
+
+/* Groups of n rows: ceil(n / 31) (the reference's decmprsNrWord). */
+MB_API uint64_t mb_wah_groups(uint64_t nrows);
+/* Compresses a bitmap of nrows rows (rows < 31 * (2^30 - 1)) into `wah`
+ * (capacity words; mb_wah_groups(nrows) always suffice).  *nwords = the
+ * stream's words.  wah NULL: a size query.  MB_ERR_INVALID if the stream does
+ * not fit (nothing written, *nwords still set).  Waits for the stream once
+ * (to learn the size); wahCompress / wahCmprsCPU (wahGpuCmprs.cu:172-198). */
+MB_API mb_status mb_wah_encode(const uint32_t *bitmap, uint64_t nrows, uint32_t order, uint32_t *wah,
+                               uint64_t capacity, uint64_t *nwords, void *stream);
+/* Expands a stream into a bitmap of nrows rows (mb_bitmap_stride(nrows) words
+ * written): groups past the stream and rows >= nrows are 0.  No host wait.
+ * wahCntExcScan + wahDecomp (wahGpuCmprs.cu:6-14, 34-47). */
+MB_API mb_status mb_wah_decode(const uint32_t *wah, uint64_t nwords, uint32_t order, uint64_t nrows,
+                               uint32_t *bitmap, void *stream);
+/* *ngroups = the groups a stream stands for (the sum of its run counts). */
+MB_API mb_status mb_wah_ngroups(const uint32_t *wah, uint64_t nwords, uint64_t *ngroups, void *stream);
+/* op (mb_wah_opcode) of two streams over ngroups groups (shorter streams are
+ * extended with 0 groups) into a canonical stream; capacity and *nwords as in
+ * mb_wah_encode.  The reference's wahAnd / wahOr / wahXor and their explicit
+ * forms (wahGpu.cuh:11-30; wahAndCPU, wahCpu.c:27-79). */
+MB_API mb_status mb_wah_op(uint32_t op, const uint32_t *a, uint64_t na, const uint32_t *b, uint64_t nb,
+                           uint64_t ngroups, uint32_t *out, uint64_t capacity, uint64_t *nwords, void *stream);
+/* The reference's WAH file (struct wahHost_s, wahCpu.h:10-15; read by
+ * loadWahFile, wahConv.c:93-109): 24-byte header (has1Fill, magic 0x44f8a1ef,
+ * cmprsNrWord, decmprsNrWord) then the words.  HOST buffers.  Load with
+ * words NULL returns the sizes only; MB_ERR_IO on a bad magic or size. */
+MB_API mb_status mb_wah_save(const char *path, const uint32_t *words, uint64_t nwords, uint64_t ngroups);
+MB_API mb_status mb_wah_load(const char *path, uint32_t *words, uint64_t capacity, uint64_t *nwords,
+                             uint64_t *ngroups);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

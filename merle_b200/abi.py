@@ -270,7 +270,17 @@ SIGNATURES: dict[str, tuple] = {
     "mb_gen_flat": (I32, [U64, U64, U64, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP, VOIDP]),
     "mb_gen_star": (I32, [U64, U32, U64, U64, I32, C.POINTER(mb_star_cols), VOIDP]),
     "mb_gen_star_dims": (I32, [U64, U32, VOIDP, VOIDP, VOIDP, VOIDP]),
+    "mb_wah_groups": (U64, [U64]),
+    "mb_wah_encode": (I32, [VOIDP, U64, U32, VOIDP, U64, C.POINTER(U64), VOIDP]),
+    "mb_wah_decode": (I32, [VOIDP, U64, U32, U64, VOIDP, VOIDP]),
+    "mb_wah_ngroups": (I32, [VOIDP, U64, C.POINTER(U64), VOIDP]),
+    "mb_wah_op": (I32, [U32, VOIDP, U64, VOIDP, U64, U64, VOIDP, U64, C.POINTER(U64), VOIDP]),
+    "mb_wah_save": (I32, [C.c_char_p, VOIDP, U64, U64]),
+    "mb_wah_load": (I32, [C.c_char_p, VOIDP, U64, C.POINTER(U64), C.POINTER(U64)]),
 }
+
+WAH_LSB, WAH_MSB = 0, 1
+WAH_AND, WAH_OR, WAH_XOR = 0, 1, 2
 
 
 def bind(lib: C.CDLL, sigs: dict[str, tuple]) -> None:

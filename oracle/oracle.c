@@ -466,3 +466,84 @@ int orc_is_nochk(const mb_vprg *p) {
     if (p->cols[i].leftmost || p->cols[i].rightmost) return 0;
   return 1;
 }
+
+/* ------------------------------------------------------- WAH interop */
+
+/* 31-bit group g of a bitmap in this library's layout (row r is bit r % 32 of
+ * word r / 32): rows 31g .. 31g + 30, row 31g + j at bit j (order 0, as
+ * loadArrayFile sets bits, merle/host/wahConv.c:85-87) or at bit 30 - j
+ * (order 1, as simpleJoin shifts them in, merle/host/wahConv.c:142-144,
+ * and dbjoinFlatWah ballots them, merle/wahGpuCmprs.cu:215-226).
+ * Rows >= nrows are 0. */
+static uint32_t wah_group(const uint32_t *bm, uint64_t nrows, uint64_t g, uint32_t order) {
+  uint32_t v = 0;
+  for (uint32_t j = 0; j < 31; ++j) {
+    uint64_t r = 31 * g + j;
+    if (r >= nrows) break;
+    if ((bm[r / 32] >> (r % 32)) & 1u) v |= 1u << (order ? 30 - j : j);
+  }
+  return v;
+}
+
+uint64_t orc_wah_encode(const uint32_t *bm, uint64_t nrows, uint32_t order, uint32_t *out) {
+  /* wahCmprsCPU (merle/host/wahConv.c:36-57) over the groups: a group that is
+   * neither 0 nor 0x7fffffff is a literal word; a maximal run of 0 groups is
+   * 0x80000000 + run, a maximal run of 0x7fffffff groups 0xc0000000 + run. */
+  uint64_t G = (nrows + 30) / 31, n = 0, g = 0;
+  while (g < G) {
+    uint32_t v = wah_group(bm, nrows, g, order);
+    if (v != 0 && v != 0x7fffffffu) {
+      out[n++] = v;
+      ++g;
+      continue;
+    }
+    uint64_t run = 0;
+    while (g < G && wah_group(bm, nrows, g, order) == v) ++run, ++g;
+    out[n++] = (v ? 0xc0000000u : 0x80000000u) + (uint32_t)run;
+  }
+  return n;
+}
+
+void orc_wah_decode(const uint32_t *wah, uint64_t nwords, uint32_t order, uint64_t nrows, uint32_t *bm,
+                    uint64_t stride) {
+  /* wahDecomp (merle/wahGpuCmprs.cu:34-47): word k expands to its group count
+   * (a fill's 30-bit count, a literal's 1) of 31-bit groups, a fill to its
+   * value repeated, a literal to its low 31 bits; the groups are then laid
+   * out as rows.  Groups past the stream, rows >= nrows and the words up to
+   * the stride are 0. */
+  memset(bm, 0, stride * sizeof(uint32_t));
+  uint64_t g = 0;
+  for (uint64_t k = 0; k < nwords; ++k) {
+    uint32_t w = wah[k];
+    uint64_t cnt = (w & 0x80000000u) ? (w & 0x3fffffffu) : 1;
+    uint32_t v = (w & 0x80000000u) ? ((w & 0x40000000u) ? 0x7fffffffu : 0u) : (w & 0x7fffffffu);
+    if (v == 0) {
+      g += cnt;
+      continue;
+    }
+    for (uint64_t c = 0; c < cnt; ++c, ++g)
+      for (uint32_t j = 0; j < 31; ++j) {
+        uint64_t r = 31 * g + j;
+        if (r >= nrows) return;
+        if ((v >> (order ? 30 - j : j)) & 1u) bm[r / 32] |= 1u << (r % 32);
+      }
+  }
+}
+
+uint64_t orc_wah_op(uint32_t op, const uint32_t *a, uint64_t na, const uint32_t *b, uint64_t nb,
+                    uint64_t ngroups, uint32_t *out) {
+  /* The explicit operations wahAndExpl / wahOrExpl / wahXorExpl
+   * (merle/wahGpuCmprs.cu:16-33) between the two decompressed streams, the
+   * result compressed as wahCompress does (merle/wahGpuCmprs.cu:172-198,
+   * the same words as wahCmprsCPU).  Streams shorter than ngroups groups are
+   * extended with 0 groups. */
+  uint64_t nrows = 31 * ngroups, W = (nrows + 31) / 32;
+  uint32_t *x = (uint32_t *)calloc(W + 1, 4), *y = (uint32_t *)calloc(W + 1, 4);
+  orc_wah_decode(a, na, 0, nrows, x, W + 1);
+  orc_wah_decode(b, nb, 0, nrows, y, W + 1);
+  for (uint64_t i = 0; i < W; ++i) x[i] = op == 0 ? x[i] & y[i] : op == 1 ? x[i] | y[i] : x[i] ^ y[i];
+  uint64_t n = orc_wah_encode(x, nrows, 0, out);
+  free(x);
+  free(y);
+  return n;
+}

@@ -105,6 +105,16 @@ int64_t orc_flat_query(const int32_t *a, const int32_t *b, const int32_t *c,
                        int32_t ahi, const int32_t *bset, uint32_t nb, int32_t clo,
                        int32_t chi, uint64_t *count);
 
+/* WAH (word-aligned hybrid) streams of the reference's compressed-bitmap
+ * baseline (merle/host/wahCpu.h, merle/wahGpu.cuh).  order 0: row 31g + j of
+ * group g at bit j; order 1: at bit 30 - j. */
+uint64_t orc_wah_encode(const uint32_t *bitmap, uint64_t nrows, uint32_t order, uint32_t *out);
+void orc_wah_decode(const uint32_t *wah, uint64_t nwords, uint32_t order, uint64_t nrows, uint32_t *bitmap,
+                    uint64_t stride);
+/* op 0 AND, 1 OR, 2 XOR over ngroups groups; returns the words written. */
+uint64_t orc_wah_op(uint32_t op, const uint32_t *a, uint64_t na, const uint32_t *b, uint64_t nb,
+                    uint64_t ngroups, uint32_t *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,6 +18,7 @@ from merle_b200 import abi
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libcpuref.so"
+WAH_REF_LIB = HERE / "_ref" / "libwahref.so"
 
 P = C.c_void_p
 U32, U64, I64, I32 = C.c_uint32, C.c_uint64, C.c_int64, C.c_int32
@@ -41,10 +42,14 @@ SIGS = {
     "orc_s4": (None, [P, U64, U32, U32, U32, U32, U32, U32, U32, U32, P, U32, P]),
     "orc_synth": (None, [P, P, U32, P, P, P, U64, U64, U64, U64, U64, U64, U64, P, P]),
     "orc_flat_query": (I64, [P, P, P, P, P, U64, I32, I32, P, U32, I32, I32, P]),
+    "orc_wah_encode": (U64, [P, U64, U32, P]),
+    "orc_wah_decode": (None, [P, U64, U32, U64, P, U64]),
+    "orc_wah_op": (U64, [U32, P, U64, P, U64, U64, P]),
 }
 
 _lib = None
 _ref = None
+_wahref = None
 
 
 def build() -> None:
@@ -84,6 +89,21 @@ def ref() -> C.CDLL | None:
         _ref.window_zipf.restype = C.POINTER(C.c_double)
         _ref.window_zipf.argtypes = [C.c_double, C.c_size_t, C.c_size_t]
     return _ref
+
+
+def wah_ref() -> C.CDLL | None:
+    """The reference's CPU WAH code (merle/host/wahCpu.c, wahConv.c), or None
+    if not built."""
+    global _wahref
+    if _wahref is None and WAH_REF_LIB.exists():
+        _wahref = C.CDLL(str(WAH_REF_LIB), mode=os.RTLD_NOW | os.RTLD_LOCAL)
+        _wahref.wahCmprsCPU.restype = C.c_size_t
+        _wahref.wahCmprsCPU.argtypes = [P, C.c_size_t, P]
+        _wahref.wahAndCPU.restype = C.c_void_p
+        _wahref.wahAndCPU.argtypes = [P, P, P, P, P, P]
+        _wahref.loadWahFile.restype = C.c_void_p
+        _wahref.loadWahFile.argtypes = [C.c_char_p]
+    return _wahref
 
 
 def ptr(a: np.ndarray) -> int:
@@ -367,3 +387,29 @@ def algo_bytes(star: "StarHost", scale: float, nrows: int, tmpl: int, p, ngroups
     dims = sum(len(getattr(star, d)) * getattr(star, d).dtype.itemsize for d in DIMS[tmpl])
     return {"bitmap": bm, "gather": int(sec * scale), "dims": dims, "out": 8 * ngroups,
             "total": int(bm + sec * scale + dims + 8 * ngroups), "rows": int(len(rows) * scale)}
+
+
+# ---------------------------------------------------------------- WAH streams
+def wah_encode(bitmap: np.ndarray, nrows: int, order: int = 0) -> np.ndarray:
+    bm = np.ascontiguousarray(bitmap, dtype=np.uint32)
+    G = (nrows + 30) // 31
+    out = np.zeros(max(1, G), np.uint32)
+    n = lib().orc_wah_encode(ptr(bm), nrows, order, ptr(out))
+    return out[:n].copy()
+
+
+def wah_decode(wah: np.ndarray, nrows: int, order: int = 0) -> np.ndarray:
+    w = np.ascontiguousarray(wah, dtype=np.uint32)
+    stride = ((nrows + 31) // 32 + 31) // 32 * 32
+    bm = np.zeros(max(1, stride), np.uint32)
+    lib().orc_wah_decode(ptr(w) if len(w) else None, len(w), order, nrows, ptr(bm), stride)
+    return bm[:stride]
+
+
+def wah_op(op: int, a: np.ndarray, b: np.ndarray, ngroups: int) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    b = np.ascontiguousarray(b, dtype=np.uint32)
+    out = np.zeros(max(1, ngroups), np.uint32)
+    n = lib().orc_wah_op(op, ptr(a) if len(a) else None, len(a), ptr(b) if len(b) else None, len(b), ngroups,
+                         ptr(out))
+    return out[:n].copy()

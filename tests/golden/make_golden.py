@@ -9,7 +9,7 @@ oracle/Makefile):
 Inputs are the seeded synthetic tables of include/merle_b200_gen.h; outputs
 are produced by the REFERENCE's functions (ssb_cpujoin / s1ref..s4ref of
 ssb/cpuref.c, synth_ref of synth/cpuref.c, window_zipf of
-synth/window_zipf.c), so the fixtures pin our oracle to the reference even on
+synth/window_zipf.c, wahCmprsCPU / wahAndCPU of merle/host/), so the fixtures pin our oracle to the reference even on
 a machine without the reference tree.
 """
 from __future__ import annotations
@@ -72,6 +72,52 @@ SYNTH_CASES = [(0, 60, 100, 160, 0, 2000), (200, 260, 30, 90, 500, 1500), (900, 
                (0, 997, 0, 0, 1000, 1001)]
 
 
+def wah_inputs(seed: int, ngroups: int) -> np.ndarray:
+    """31-bit groups (values < 2^31) mixing literals with runs of 0 and of
+    0x7fffffff groups of random lengths, 1 included."""
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < ngroups:
+        kind = rng.integers(0, 3)
+        run = int(rng.choice([1, 1, 2, 3, 7, 40]))
+        if kind == 0:
+            out += [0] * run
+        elif kind == 1:
+            out += [0x7fffffff] * run
+        else:
+            out += rng.integers(1, 0x7fffffff, run).tolist()
+    return np.array(out[:ngroups], np.uint32)
+
+
+WAH_CASES = [(11, 600), (12, 1), (13, 257), (14, 1000)]
+
+
+def wah_golden(wref) -> dict:
+    """wahCmprsCPU of seeded group arrays, and wahAndCPU of consecutive pairs
+    of the compressed streams (merle/host/wahConv.c:36-57, wahCpu.c:27-79)."""
+    arrays = {}
+    for seed, g in WAH_CASES:
+        dec = wah_inputs(seed, g)
+        # in place: wahCmprsCPU returns its output end minus its INPUT start
+        # (wahConv.c:56), a word count only when the two are the same buffer
+        buf = dec.copy()
+        n = wref.wahCmprsCPU(O.ptr(buf), g, O.ptr(buf))
+        assert 1 <= n <= g
+        arrays[f"dec_{seed}"] = dec
+        arrays[f"wah_{seed}"] = buf[:n].copy()
+    seeds = [s for s, _ in WAH_CASES]
+    for a, b in zip(seeds, seeds[1:] + seeds[:1]):
+        x = np.concatenate([arrays[f"wah_{a}"], np.zeros(2, np.uint32)])
+        y = np.concatenate([arrays[f"wah_{b}"], np.zeros(2, np.uint32)])
+        na, nb = len(arrays[f"wah_{a}"]), len(arrays[f"wah_{b}"])
+        out = np.zeros(na + nb + 4, np.uint32)
+        base = O.ptr(out)
+        end = wref.wahAndCPU(O.ptr(x), O.ptr(x) + 4 * na, O.ptr(y), O.ptr(y) + 4 * nb, base, base + 4 * len(out))
+        arrays[f"and_{a}_{b}"] = out[:(end - base) // 4].copy()
+    np.savez_compressed(HERE / "wah_ref.npz", **arrays)
+    return {"cases": WAH_CASES, "pairs": [[a, b] for a, b in zip(seeds, seeds[1:] + seeds[:1])]}
+
+
 def main() -> None:
     ref = O.ref()
     if ref is None:
@@ -111,8 +157,14 @@ def main() -> None:
         p = ref.window_zipf(skew, 64, 60)
         wz[str(skew)] = [p[i] for i in range(64)]
     out["window_zipf"] = wz
+    # 5. the reference's CPU WAH compression and compressed AND
+    wref = O.wah_ref()
+    if wref is None:
+        raise SystemExit("oracle/_ref/libwahref.so is missing: run `make -C oracle` with the reference tree")
+    out["wah"] = wah_golden(wref)
     (HERE / "golden.json").write_text(json.dumps(out, indent=1))
-    print("wrote", HERE / "golden.json", HERE / "ssb13_ref_u32.npy", HERE / "synth_ref_u32.npy")
+    print("wrote", HERE / "golden.json", HERE / "ssb13_ref_u32.npy", HERE / "synth_ref_u32.npy",
+          HERE / "wah_ref.npz")
 
 
 if __name__ == "__main__":
