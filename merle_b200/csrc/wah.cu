@@ -27,6 +27,7 @@
 // All passes are HBM-bound integer work: no tensor cores.
 #include <string.h>
 #include <stdio.h>
+#include <mutex>
 #include <vector>
 #include "common.cuh"
 
@@ -36,8 +37,13 @@ namespace {
 constexpr uint32_t WT = 256;          // threads of the counting / writing passes
 constexpr uint32_t WI = 8;            // groups (encode) or stream words (decode) per thread
 constexpr uint32_t WB = WT * WI;      // per block
-constexpr uint32_t DT = 256;          // output words per decode block (one per thread)
-constexpr uint32_t DCAP = 1024;       // stream words a decode block stages
+constexpr uint32_t EW = WB * 31 / 32;  // bitmap words an encode block covers (2048 groups = 1984 words)
+constexpr uint32_t DT = 256;          // threads of a decode block
+constexpr uint32_t DV = 8;            // output words a decode thread writes
+constexpr uint32_t DW = DT * DV;      // output words a decode block writes
+constexpr uint32_t DCAP = 2304;       // stream words a decode block stages
+constexpr uint32_t DGRP = DW * 32 / 31 + 3;  // groups a decode block's words span
+constexpr uint32_t DLONG = 64;        // runs longer than 32 groups a decode block fills together
 constexpr uint32_t FILL = 0x80000000u, ONES = 0x40000000u, CNT = 0x3fffffffu, LIT = 0x7fffffffu;
 constexpr uint64_t MAX_GROUPS = CNT;  // a run must fit the 30-bit count
 constexpr uint32_t WAH_MAGIC = 0x44f8a1efu;
@@ -56,19 +62,6 @@ __device__ __forceinline__ uint32_t enc_word(const EncSrc &S, uint64_t i) {
     const uint32_t u = __ldg(S.b + i);
     v = S.op == 0 ? v & u : S.op == 1 ? v | u : v ^ u;
   }
-  return v;
-}
-
-// Group g (< ceil(nrows / 31)) as stored in a stream: row 31g + j at bit j
-// (order 0) or at bit 30 - j (order 1); rows >= nrows are 0.
-__device__ __forceinline__ uint32_t group_of(const EncSrc &S, uint64_t g) {
-  const uint64_t r0 = 31 * g, w = r0 >> 5;
-  const uint32_t s = (uint32_t)(r0 & 31);
-  const uint64_t two = (uint64_t)enc_word(S, w) | ((uint64_t)enc_word(S, w + 1) << 32);
-  uint32_t v = (uint32_t)(two >> s) & LIT;
-  const uint64_t left = S.nrows - r0;
-  if (left < 31) v &= (1u << left) - 1u;
-  if (S.order) v = __brev(v) >> 1;
   return v;
 }
 
@@ -99,37 +92,105 @@ __device__ __forceinline__ T block_excl_scan(T x, T *total) {
   return before + inc - x;
 }
 
+// Stages the bitmap words of encode block b (groups [WB b, WB (b + 1)) are
+// rows [63488 b, 63488 (b + 1)) = words [EW b, EW (b + 1))) in shared memory:
+// st[0] = word EW b - 1 (the group before the block ends in it), st[1 + i] =
+// word EW b + i, st[EW + 1] = the word after.  Rows >= nrows read as 0.
+__device__ __forceinline__ void enc_stage(const EncSrc &S, uint64_t b, uint32_t *st) {
+  constexpr uint32_t R = (EW + 2 + WT - 1) / WT;
+  const int64_t base = (int64_t)(b * EW) - 1;
+  uint32_t v[R];
+#pragma unroll
+  for (uint32_t r = 0; r < R; ++r) {  // every load issued before the first store
+    const uint32_t i = r * WT + threadIdx.x;
+    const int64_t w = base + i;
+    v[r] = i < EW + 2 && w >= 0 && (uint64_t)w < S.nw ? enc_word(S, (uint64_t)w) : 0u;
+  }
+#pragma unroll
+  for (uint32_t r = 0; r < R; ++r) {
+    const uint32_t i = r * WT + threadIdx.x;
+    if (i >= EW + 2) break;
+    const int64_t w = base + i;
+    const uint64_t r0 = (uint64_t)w * 32;
+    if (w >= 0 && (uint64_t)w < S.nw && r0 + 32 > S.nrows) v[r] &= (1u << (S.nrows - r0)) - 1u;
+    st[i] = v[r];
+  }
+  __syncthreads();
+}
+
+// Local group j (-1 = the group before the block) from the staged words.
+__device__ __forceinline__ uint32_t enc_group(const uint32_t *st, int32_t j, uint32_t order) {
+  const uint32_t bit = (uint32_t)(32 + 31 * j), w = bit >> 5;
+  uint32_t v = __funnelshift_r(st[w], st[w + 1], bit & 31) & LIT;
+  if (order) v = __brev(v) >> 1;
+  return v;
+}
+
+// Whether local group j (global gbase + j < G) starts a stream word: a
+// literal, the first group, or a kind unlike the group before.  Threads take
+// groups j = i * WT + t in round i, so neighbouring lanes read neighbouring
+// shared-memory words.
+__device__ __forceinline__ uint32_t enc_flag(const uint32_t *st, int32_t j, uint64_t gbase, uint64_t G,
+                                             uint32_t order, uint32_t *v) {
+  *v = enc_group(st, j, order);
+  const uint32_t k = kind_of(*v);
+  // the kind of group j - 1: lane - 1 holds it; lane 0 extracts it
+  uint32_t kp = __shfl_up_sync(0xffffffffu, k, 1);
+  if ((threadIdx.x & 31) == 0) kp = kind_of(enc_group(st, j - 1, order));
+  const uint64_t g = gbase + (uint64_t)j;
+  if (g >= G) return 0u;
+  if (k == 2u || g == 0) return 1u;
+  return k != kp ? 1u : 0u;
+}
+
+// Exclusive prefix of one flag per thread over the block (lane order within
+// warps, warps in order); *total = the block's flags.  All WT threads call it.
+__device__ __forceinline__ uint32_t block_flag_scan(uint32_t f, uint32_t *total) {
+  __shared__ uint32_t wsum[WT / 32];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t bal = __ballot_sync(0xffffffffu, f);
+  if (lane == 0) wsum[warp] = __popc(bal);
+  __syncthreads();
+  uint32_t before = 0, all = 0;
+#pragma unroll
+  for (uint32_t i = 0; i < WT / 32; ++i) {
+    if (i < warp) before += wsum[i];
+    all += wsum[i];
+  }
+  __syncthreads();
+  *total = all;
+  return before + __popc(bal & ((1u << lane) - 1u));
+}
+
 // (1) stream words each block of WB groups starts.
 __global__ void __launch_bounds__(WT) wah_enc_count(const EncSrc S, uint64_t G, uint64_t *bcnt) {
-  const uint64_t g0 = (uint64_t)blockIdx.x * WB + (uint64_t)threadIdx.x * WI;
-  uint32_t c = 0;
-  if (g0 < G) {
-    uint32_t prev = g0 ? kind_of(group_of(S, g0 - 1)) : 3u;
+  __shared__ uint32_t st[EW + 2];
+  enc_stage(S, blockIdx.x, st);
+  const uint64_t gbase = (uint64_t)blockIdx.x * WB;
+  uint32_t c = 0, v;
 #pragma unroll
-    for (uint32_t i = 0; i < WI; ++i) {
-      const uint64_t g = g0 + i;
-      if (g >= G) break;
-      const uint32_t k = kind_of(group_of(S, g));
-      c += (k == 2u || k != prev) ? 1u : 0u;
-      prev = k;
-    }
-  }
+  for (uint32_t i = 0; i < WI; ++i) c += enc_flag(st, (int32_t)(i * WT + threadIdx.x), gbase, G, S.order, &v);
   uint64_t total;
   block_excl_scan<uint64_t>(c, &total);
   if (threadIdx.x == 0) bcnt[blockIdx.x] = total;
 }
 
-// (2) exclusive scan of n block values in place (one CTA); v[n] = total.
+// (2) exclusive scan of n block values in place (one CTA, four values a
+// thread per round); v[n] = total.
 __global__ void __launch_bounds__(1024) wah_scan_blocks(uint64_t *v, uint64_t n) {
   __shared__ uint64_t part[32];
   __shared__ uint64_t carry;
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
-  for (uint64_t base = 0; base < n; base += 1024) {
-    const uint64_t i = base + threadIdx.x;
-    const uint64_t x = i < n ? v[i] : 0;
-    uint64_t inc = x;
+  for (uint64_t base = 0; base < n; base += 4096) {
+    const uint64_t i0 = base + 4ull * threadIdx.x;
+    uint64_t x[4], sum = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) x[j] = i0 + j < n ? v[i0 + j] : 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sum += x[j];
+    uint64_t inc = sum;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
       const uint64_t y = __shfl_up_sync(0xffffffffu, inc, d);
@@ -137,12 +198,15 @@ __global__ void __launch_bounds__(1024) wah_scan_blocks(uint64_t *v, uint64_t n)
     }
     if (lane == 31) part[warp] = inc;
     __syncthreads();
-    uint64_t before = carry, all = 0;
+    uint64_t at = carry, all = 0;
     for (uint32_t k = 0; k < 32; ++k) {
-      if (k < warp) before += part[k];
+      if (k < warp) at += part[k];
       all += part[k];
     }
-    if (i < n) v[i] = before + inc - x;
+    at += inc - sum;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (i0 + j < n) v[i0 + j] = at, at += x[j];
     __syncthreads();
     if (threadIdx.x == 0) carry += all;
     __syncthreads();
@@ -154,29 +218,23 @@ __global__ void __launch_bounds__(1024) wah_scan_blocks(uint64_t *v, uint64_t n)
 // word's starting group into pos.
 __global__ void __launch_bounds__(WT) wah_enc_write(const EncSrc S, uint64_t G, const uint64_t *boff, uint32_t *out,
                                                     uint32_t *pos) {
-  const uint64_t g0 = (uint64_t)blockIdx.x * WB + (uint64_t)threadIdx.x * WI;
-  uint32_t v[WI], head = 0, c = 0;
-  if (g0 < G) {
-    uint32_t prev = g0 ? kind_of(group_of(S, g0 - 1)) : 3u;
-#pragma unroll
-    for (uint32_t i = 0; i < WI; ++i) {
-      const uint64_t g = g0 + i;
-      v[i] = g < G ? group_of(S, g) : 0u;
-      const uint32_t k = kind_of(v[i]);
-      if (g < G && (k == 2u || k != prev)) head |= 1u << i, ++c;
-      prev = k;
+  __shared__ uint32_t st[EW + 2];
+  enc_stage(S, blockIdx.x, st);
+  const uint64_t gbase = (uint64_t)blockIdx.x * WB;
+  uint64_t at = boff[blockIdx.x];
+#pragma unroll 1
+  for (uint32_t i = 0; i < WI; ++i) {
+    const int32_t j = (int32_t)(i * WT + threadIdx.x);
+    uint32_t v, total;
+    const uint32_t f = enc_flag(st, j, gbase, G, S.order, &v);
+    const uint32_t ex = block_flag_scan(f, &total);
+    if (f) {
+      const uint32_t k = kind_of(v);
+      out[at + ex] = k == 2u ? v : (k == 1u ? FILL | ONES : FILL);
+      pos[at + ex] = (uint32_t)(gbase + (uint64_t)j);
     }
+    at += total;
   }
-  uint64_t total;
-  uint64_t at = boff[blockIdx.x] + block_excl_scan<uint64_t>(c, &total);
-#pragma unroll
-  for (uint32_t i = 0; i < WI; ++i)
-    if (head >> i & 1u) {
-      const uint32_t k = kind_of(v[i]);
-      out[at] = k == 2u ? v[i] : (k == 1u ? FILL | ONES : FILL);
-      pos[at] = (uint32_t)(g0 + i);
-      ++at;
-    }
 }
 
 // (4) fill runs.
@@ -192,39 +250,71 @@ __global__ void wah_enc_fills(uint32_t *out, const uint32_t *pos, uint64_t K, ui
 
 __device__ __forceinline__ uint64_t word_groups(uint32_t w) { return (w & FILL) ? (w & CNT) : 1u; }
 
-// decode (1): group counts per block of WB stream words.
+// decode (1): group counts per block of WB stream words (word i * WT + t of
+// the block in round i: coalesced).
 __global__ void __launch_bounds__(WT) wah_dec_count(const uint32_t *wah, uint64_t n, uint64_t *bsum) {
-  const uint64_t k0 = (uint64_t)blockIdx.x * WB + (uint64_t)threadIdx.x * WI;
+  const uint64_t kbase = (uint64_t)blockIdx.x * WB;
   uint64_t c = 0;
 #pragma unroll
-  for (uint32_t i = 0; i < WI; ++i)
-    if (k0 + i < n) c += word_groups(__ldg(wah + k0 + i));
+  for (uint32_t i = 0; i < WI; ++i) {
+    const uint64_t k = kbase + i * WT + threadIdx.x;
+    if (k < n) c += word_groups(__ldg(wah + k));
+  }
   uint64_t total;
   block_excl_scan<uint64_t>(c, &total);
   if (threadIdx.x == 0) bsum[blockIdx.x] = total;
 }
 
 // decode (2b): the exclusive scan of every word's group count; S[n] = total.
+// S is stored saturated at 2^32 - 1: decoding looks up groups below 2^30
+// only, and min(x, cap) keeps the order of every prefix below the cap.
+__device__ __forceinline__ uint32_t sat32(uint64_t x) { return x > 0xffffffffull ? 0xffffffffu : (uint32_t)x; }
+
 __global__ void __launch_bounds__(WT) wah_dec_scan(const uint32_t *wah, uint64_t n, const uint64_t *boff,
-                                                   uint64_t nblk, uint64_t *S) {
-  const uint64_t k0 = (uint64_t)blockIdx.x * WB + (uint64_t)threadIdx.x * WI;
+                                                   uint64_t nblk, uint32_t *S) {
+  // counts in round order (coalesced loads), regrouped through shared
+  // memory so that each thread owns WI consecutive words: one block scan
+  __shared__ uint32_t xs[WB + WB / 32];  // padded: index i at i + i / 32
+  const uint64_t kbase = (uint64_t)blockIdx.x * WB;
   uint32_t c[WI];
+#pragma unroll
+  for (uint32_t i = 0; i < WI; ++i) {
+    const uint64_t k = kbase + i * WT + threadIdx.x;
+    c[i] = k < n ? (uint32_t)word_groups(__ldg(wah + k)) : 0u;
+  }
+#pragma unroll
+  for (uint32_t i = 0; i < WI; ++i) {
+    const uint32_t l = i * WT + threadIdx.x;
+    xs[l + l / 32] = c[i];
+  }
+  __syncthreads();
   uint64_t sum = 0;
 #pragma unroll
   for (uint32_t i = 0; i < WI; ++i) {
-    c[i] = k0 + i < n ? (uint32_t)word_groups(__ldg(wah + k0 + i)) : 0u;
+    const uint32_t l = threadIdx.x * WI + i;
+    c[i] = xs[l + l / 32];
     sum += c[i];
   }
   uint64_t total;
   uint64_t at = boff[blockIdx.x] + block_excl_scan<uint64_t>(sum, &total);
 #pragma unroll
-  for (uint32_t i = 0; i < WI; ++i)
-    if (k0 + i < n) S[k0 + i] = at, at += c[i];
-  if (blockIdx.x == 0 && threadIdx.x == 0) S[n] = boff[nblk];
+  for (uint32_t i = 0; i < WI; ++i) {
+    const uint32_t l = threadIdx.x * WI + i;
+    xs[l + l / 32] = sat32(at);
+    at += c[i];
+  }
+  __syncthreads();
+#pragma unroll
+  for (uint32_t i = 0; i < WI; ++i) {
+    const uint32_t l = i * WT + threadIdx.x;
+    const uint64_t k = kbase + l;
+    if (k < n) S[k] = xs[l + l / 32];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) S[n] = sat32(boff[nblk]);
 }
 
 // Largest k in [lo, hi] with S[k] <= g (S ascending, S[lo] <= g).
-__device__ __forceinline__ uint64_t last_le(const uint64_t *S, uint64_t lo, uint64_t hi, uint64_t g) {
+__device__ __forceinline__ uint64_t last_le(const uint32_t *S, uint64_t lo, uint64_t hi, uint64_t g) {
   while (lo < hi) {
     const uint64_t mid = lo + (hi - lo + 1) / 2;
     if (S[mid] <= g) lo = mid;
@@ -233,12 +323,13 @@ __device__ __forceinline__ uint64_t last_le(const uint64_t *S, uint64_t lo, uint
   return lo;
 }
 
-// decode (3): for output block b, the stream words covering its groups.
-__global__ void wah_dec_partition(const uint64_t *S, uint64_t n, uint64_t nblk, uint64_t *kb, uint64_t *ke) {
+// decode (3): for output block b (words [DW b, DW (b + 1))), the stream
+// words covering its groups.
+__global__ void wah_dec_partition(const uint32_t *S, uint64_t n, uint64_t nblk, uint64_t *kb, uint64_t *ke) {
   const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nblk) return;
   const uint64_t total = S[n];
-  const uint64_t w0 = b * DT, w1 = w0 + DT - 1;
+  const uint64_t w0 = b * DW, w1 = w0 + DW - 1;
   const uint64_t ga = (32 * w0) / 31, gz = (32 * w1) / 31 + 1;
   if (ga >= total) {
     kb[b] = 1, ke[b] = 0;  // past the stream: an empty range
@@ -249,54 +340,126 @@ __global__ void wah_dec_partition(const uint64_t *S, uint64_t n, uint64_t nblk, 
   ke[b] = last_le(S, s, n - 1, gz < total ? gz : total - 1);
 }
 
-// decode (4): output words, one per thread.
-__global__ void __launch_bounds__(DT) wah_dec_emit(const uint32_t *wah, const uint64_t *S, uint64_t n,
-                                                   const uint64_t *kb, const uint64_t *ke, uint32_t order,
-                                                   uint64_t nrows, uint64_t nw, uint64_t stride, uint32_t *bm) {
-  __shared__ uint64_t s_S[DCAP];
-  __shared__ uint32_t s_w[DCAP];
-  const uint64_t b = blockIdx.x, w = b * DT + threadIdx.x;
-  const uint64_t lo = kb[b], hi = ke[b], total = S[n];
-  const bool empty = lo > hi, staged = !empty && hi - lo + 1 <= DCAP;
-  if (staged)
-    for (uint64_t i = threadIdx.x; i <= hi - lo; i += DT) s_S[i] = S[lo + i], s_w[i] = __ldg(wah + lo + i);
-  __syncthreads();
-  if (w >= stride) return;
-  uint32_t out = 0;
-  if (!empty && w < nw) {
-    const uint64_t ga = (32 * w) / 31;
-    const uint32_t sa = (uint32_t)(32 * w - 31 * ga);
-    uint32_t v[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const uint64_t g = ga + h;
-      uint32_t x = 0;
-      if (g < total) {
-        uint32_t word;
-        if (staged) {
-          uint32_t l = 0, r = (uint32_t)(hi - lo);
-          while (l < r) {
-            const uint32_t m = l + (r - l + 1) / 2;
-            if (s_S[m] <= g) l = m;
-            else r = m - 1;
-          }
-          word = s_w[l];
-        } else {
-          word = __ldg(wah + last_le(S, lo, hi, g));
-        }
-        x = (word & FILL) ? ((word & ONES) ? LIT : 0u) : (word & LIT);
-        if (order) x = __brev(x) >> 1;
-      }
-      v[h] = x;
-    }
-    out = (v[0] >> sa) | (v[1] << (31 - sa));
-    const uint64_t r0 = 32 * w;
-    if (r0 + 32 > nrows) out &= nrows > r0 ? (1u << (nrows - r0)) - 1u : 0u;
-  }
-  bm[w] = out;
+__device__ __forceinline__ uint32_t group_value(uint32_t word, uint32_t order) {
+  uint32_t x = (word & FILL) ? ((word & ONES) ? LIT : 0u) : (word & LIT);
+  return order ? __brev(x) >> 1 : x;
 }
 
-// Device scratch freed on scope exit (stream-ordered).
+// decode (4): the block expands its staged stream words into its groups in
+// shared memory (0 groups are the default; runs longer than 32 groups are
+// filled by all threads together), then each thread composes output words
+// w = DW b + i DT + t from the two groups each spans.
+__global__ void __launch_bounds__(DT) wah_dec_emit(const uint32_t *wah, const uint32_t *S, uint64_t n,
+                                                   const uint64_t *kb, const uint64_t *ke, uint32_t order,
+                                                   uint64_t nrows, uint64_t nw, uint64_t stride, uint32_t *bm) {
+  __shared__ uint32_t s_S[DCAP + 1];
+  __shared__ uint32_t s_w[DCAP];
+  __shared__ uint32_t grp[DGRP];
+  __shared__ uint32_t long_lo[DLONG], long_hi[DLONG], long_v[DLONG];
+  __shared__ uint32_t nlong;
+  const uint32_t t = threadIdx.x;
+  const uint64_t b = blockIdx.x, wbase = b * DW;
+  const uint64_t ga0 = (32 * wbase) / 31;
+  const uint64_t lo = kb[b], hi = ke[b], total = S[n];
+  const bool empty = lo > hi, staged = !empty && hi - lo + 1 <= DCAP;
+  const uint32_t cnt = staged ? (uint32_t)(hi - lo + 1) : 0u;
+  const uint64_t wend = wbase + DW < nw ? wbase + DW : nw;
+  const uint32_t ng = wend > wbase ? (uint32_t)((32 * (wend - 1)) / 31 + 2 - ga0) : 0u;
+  const uint64_t gcap = ga0 + ng < total ? ga0 + ng : total;  // groups with a value: [ga0, gcap)
+  for (uint32_t j = t; j < ng; j += DT) grp[j] = 0;
+  if (t == 0) nlong = 0;
+  if (staged) {
+    constexpr uint32_t R = (DCAP + DT - 1) / DT;
+    uint32_t a[R], c[R];
+#pragma unroll
+    for (uint32_t r = 0; r < R; ++r) {  // every load issued before the first store
+      const uint32_t i = r * DT + t;
+      if (i < cnt) a[r] = S[lo + i], c[r] = __ldg(wah + lo + i);
+    }
+#pragma unroll
+    for (uint32_t r = 0; r < R; ++r) {
+      const uint32_t i = r * DT + t;
+      if (i < cnt) s_S[i] = a[r], s_w[i] = c[r];
+    }
+    if (t == 0) s_S[cnt] = S[hi + 1];
+  }
+  __syncthreads();
+  if (staged) {
+    // local group range of the block: [0, lcap); S values are < 2^32 here
+    const uint32_t g_lo = (uint32_t)ga0, lcap = (uint32_t)(gcap > ga0 ? gcap - ga0 : 0);
+    for (uint32_t i = t; i < cnt; i += DT) {
+      const uint32_t x = group_value(s_w[i], order);
+      if (!x) continue;
+      const uint32_t a = s_S[i] > g_lo ? s_S[i] - g_lo : 0u, e0 = s_S[i + 1] > g_lo ? s_S[i + 1] - g_lo : 0u;
+      const uint32_t e = e0 < lcap ? e0 : lcap;
+      if (a >= e) continue;
+      if (e - a <= 32) {
+        for (uint32_t j = a; j < e; ++j) grp[j] = x;
+      } else {
+        const uint32_t r = atomicAdd(&nlong, 1u);
+        if (r < DLONG) long_lo[r] = a, long_hi[r] = e, long_v[r] = x;
+        else
+          for (uint32_t j = a; j < e; ++j) grp[j] = x;
+      }
+    }
+  }
+  __syncthreads();
+  const uint32_t nl = nlong < DLONG ? nlong : DLONG;
+  for (uint32_t r = 0; r < nl; ++r)
+    for (uint32_t j = long_lo[r] + t; j < long_hi[r]; j += DT) grp[j] = long_v[r];
+  __syncthreads();
+  // word wbase + l holds rows from local group (rb + 32 l) / 31 at bit
+  // (rb + 32 l) % 31 on, rb = 32 wbase - 31 ga0 (< 31): 32-bit arithmetic
+  const uint32_t rb = (uint32_t)(32 * wbase - 31 * ga0);
+#pragma unroll 1
+  for (uint32_t i = 0; i < DV; ++i) {
+    const uint32_t l = i * DT + t;
+    const uint64_t w = wbase + l;
+    if (w >= stride) break;
+    uint32_t o = 0;
+    if (!empty && w < nw) {
+      const uint32_t q = rb + 32 * l, la = q / 31, sa = q - 31 * la;
+      uint32_t va, vb;
+      if (staged) {
+        va = grp[la];
+        vb = grp[la + 1];
+      } else {  // more stream words than the stage holds (runs of 0 groups): search
+        const uint64_t ga = ga0 + la;
+        va = ga < total ? group_value(__ldg(wah + last_le(S, lo, hi, ga)), order) : 0u;
+        vb = ga + 1 < total ? group_value(__ldg(wah + last_le(S, lo, hi, ga + 1)), order) : 0u;
+      }
+      o = (va >> sa) | (vb << (31 - sa));
+      const uint64_t r0 = 32 * w;
+      if (r0 + 32 > nrows) o &= nrows > r0 ? (1u << (nrows - r0)) - 1u : 0u;
+    }
+    bm[w] = o;
+  }
+}
+
+// A stream-ordered memory pool per device for the passes' scratch, which
+// keeps what it was given (release threshold: unlimited) so that repeated
+// calls reuse it instead of mapping fresh memory each time.
+cudaMemPool_t scratch_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+
+// Device scratch from that pool, freed on scope exit (stream-ordered).
 struct Scratch {
   cudaStream_t st;
   std::vector<void *> ptrs;
@@ -306,8 +469,10 @@ struct Scratch {
   }
   template <typename T>
   mb_status get(T **p, uint64_t count) {
+    cudaMemPool_t pool = scratch_pool();
+    if (!pool) return fail(MB_ERR_CUDA, "wah: no scratch memory pool");
     void *q = nullptr;
-    const cudaError_t e = cudaMallocAsync(&q, count ? count * sizeof(T) : sizeof(T), st);
+    const cudaError_t e = cudaMallocFromPoolAsync(&q, count ? count * sizeof(T) : sizeof(T), pool, st);
     if (e != cudaSuccess) return cuda_fail(e, "wah: scratch allocation");
     ptrs.push_back(q);
     *p = static_cast<T *>(q);
@@ -349,9 +514,10 @@ mb_status encode(const EncSrc &S, uint32_t *out, uint64_t capacity, uint64_t *nw
 
 // The exclusive scan of the stream's group counts into a new scratch array
 // S[0..n] (S[n] = the groups the stream stands for).
-mb_status group_scan(const uint32_t *wah, uint64_t n, Scratch &sc, uint64_t **S_out, cudaStream_t st) {
+mb_status group_scan(const uint32_t *wah, uint64_t n, Scratch &sc, uint32_t **S_out, cudaStream_t st) {
   const uint64_t nblk = ceil_div(n, WB);
-  uint64_t *boff, *S;
+  uint64_t *boff;
+  uint32_t *S;
   MB_CHECK(sc.get(&boff, nblk + 1));
   MB_CHECK(sc.get(&S, n + 1));
   wah_dec_count<<<(unsigned)nblk, WT, 0, st>>>(wah, n, boff);
@@ -372,9 +538,9 @@ mb_status decode(const uint32_t *wah, uint64_t n, uint32_t order, uint64_t nrows
     return MB_OK;
   }
   Scratch sc(st);
-  uint64_t *S;
+  uint32_t *S;
   MB_CHECK(group_scan(wah, n, sc, &S, st));
-  const uint64_t nblk = ceil_div(stride, DT);
+  const uint64_t nblk = ceil_div(stride, DW);
   uint64_t *kb, *ke;
   MB_CHECK(sc.get(&kb, nblk));
   MB_CHECK(sc.get(&ke, nblk));
@@ -424,9 +590,14 @@ extern "C" mb_status mb_wah_ngroups(const uint32_t *wah, uint64_t nwords, uint64
   if (nwords == 0) return MB_OK;
   cudaStream_t st = as_stream(stream);
   Scratch sc(st);
-  uint64_t *S;
-  MB_CHECK(group_scan(wah, nwords, sc, &S, st));
-  MB_CUDA(cudaMemcpyAsync(ngroups, S + nwords, 8, cudaMemcpyDeviceToHost, st));
+  const uint64_t nblk = ceil_div(nwords, WB);
+  uint64_t *boff;
+  MB_CHECK(sc.get(&boff, nblk + 1));
+  wah_dec_count<<<(unsigned)nblk, WT, 0, st>>>(wah, nwords, boff);
+  MB_LAUNCH_CHECK("wah_dec_count");
+  wah_scan_blocks<<<1, 1024, 0, st>>>(boff, nblk);
+  MB_LAUNCH_CHECK("wah_scan_blocks");
+  MB_CUDA(cudaMemcpyAsync(ngroups, boff + nblk, 8, cudaMemcpyDeviceToHost, st));
   MB_CUDA(cudaStreamSynchronize(st));
   return MB_OK;
 }

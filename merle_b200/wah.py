@@ -50,14 +50,15 @@ def wah_groups(nrows: int) -> int:
 
 def wah_compress(bitmap, nrows: int, order: int = abi.WAH_LSB, stream=None):
     """Device bitmap (int32 tensor, >= ceil(nrows/32) words) -> device WAH
-    stream (int32 tensor of exactly the stream's words)."""
+    stream (an int32 tensor of the stream's words: a view of a buffer of
+    ceil(nrows/31) words, the bound on any stream's length)."""
     torch = _torch()
     cap = max(1, wah_groups(nrows))
     out = torch.empty(cap, dtype=torch.int32, device=bitmap.device if nrows else "cuda")
     n = C.c_uint64()
     check(lib().mb_wah_encode(_ptr(bitmap) if nrows else None, nrows, order, _ptr(out), cap, C.byref(n),
                               _stream(stream)))
-    return out[:n.value].clone()
+    return out[:n.value]
 
 
 def wah_decompress(wah, nrows: int, order: int = abi.WAH_LSB, stream=None):
@@ -84,7 +85,7 @@ def _op(op: int, a, b, ngroups: int | None, stream=None):
     n = C.c_uint64()
     check(lib().mb_wah_op(op, _ptr(a), a.numel(), _ptr(b), b.numel(), ngroups, _ptr(out), cap, C.byref(n),
                           _stream(stream)))
-    return out[:n.value].clone()
+    return out[:n.value]
 
 
 def wah_and(a, b, ngroups: int | None = None, stream=None):
@@ -111,3 +112,123 @@ def load_wah_file(path: str | Path) -> tuple[np.ndarray, int]:
     w = np.zeros(max(1, n.value), np.uint32)
     check(lib().mb_wah_load(str(path).encode(), w.ctypes.data, len(w), C.byref(n), C.byref(g)))
     return w[:n.value], g.value
+
+
+# ---------------------------------------------------------------- measurement
+def _predicates(star, tmpl: int, p) -> list:
+    """(source, lo, hi) of each predicate of an SSB template, as the
+    reference's WAH baseline builds its bitmaps (s1wah .. s4wah,
+    ssb/wah-demo.cu:22-240): fact-column ranges and dimension attributes
+    reached through the foreign key."""
+    from . import device as D
+    date = (D.src_of(star["orderdate"]), p[-2], p[-1])
+    scity = lambda lo, hi: (D.src_of(star["suppcity"]), lo, hi)  # noqa: E731
+    ccity = lambda lo, hi: (D.src_of(star.custcity, star["custkey"]), lo, hi)  # noqa: E731
+    pmfgr = lambda lo, hi: (D.src_of(star.partmfgr, star["partkey"]), lo, hi)  # noqa: E731
+    if tmpl == 1:
+        return [(D.src_of(star["orderdate"]), p[0], p[1]), (D.src_of(star["discount"]), p[2], p[3]),
+                (D.src_of(star["quantity"]), p[4], p[5])]
+    if tmpl == 2:
+        return [pmfgr(p[0], p[1]), scity(p[2], p[3])]
+    if tmpl == 3:
+        return [ccity(p[0], p[1]), scity(p[2], p[3]), date]
+    return [ccity(p[0], p[1]), scity(p[2], p[3]), pmfgr(p[4], p[5]), date]
+
+
+def main(argv=None) -> None:
+    """Times the reference's WAH baseline pipeline on this library's kernels
+    for the 13 SSB queries (per query: the AND of the predicates' compressed
+    streams, then decompression, the region ssb/wah-demo.cu times), the fused
+    plain path on the same queries, and compression / decompression
+    throughput.  One JSON line per measurement."""
+    import argparse
+    import json
+    import time
+
+    from . import device as D, workload as WL
+    from .engine import Engine
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--k", type=int, default=20)
+    ap.add_argument("--rows", type=int, default=120_000_000)
+    ap.add_argument("--codec-rows", type=int, default=1_800_000_000)
+    ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--codec-only", action="store_true", help="skip the SSB pipeline")
+    ap.add_argument("--out", type=str, default="")
+    a = ap.parse_args(argv)
+    torch = _torch()
+    lines = []
+
+    def emit(d):
+        print(json.dumps(d), flush=True)
+        lines.append(d)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    n = a.rows
+    star = D.DevStar(2, a.k, n) if not a.codec_only else None
+    G = wah_groups(n)
+    eng = Engine(0)
+    if not a.codec_only:
+        eng.gen_star(2, a.k, n)
+        eng.build_index()
+    seen = {}
+    for tmpl, p in ([] if a.codec_only else WL.SSB13):
+        seen[tmpl] = seen.get(tmpl, 0) + 1
+        bms = [D.bitmap_create(src, n, [lo], [hi])[0][0] for src, lo, hi in _predicates(star, tmpl, p)]
+        t0 = time.perf_counter()
+        streams = [wah_compress(b, n, abi.WAH_MSB) for b in bms]
+        torch.cuda.synchronize()
+        comp_ms = (time.perf_counter() - t0) * 1e3
+
+        def pipeline():
+            r = streams[0]
+            for s in streams[1:]:
+                r = wah_and(r, s, G)
+            return wah_decompress(r, n, abi.WAH_MSB)
+
+        want = bms[0]
+        for b in bms[1:]:
+            want = want & b
+        assert torch.equal(pipeline()[:want.numel()], want)
+        wah_ms = timed(pipeline, a.reps)
+        q = abi.query(tmpl, *p)
+        eng.query(q)
+        fused = sorted(eng.query(q)[2].ms for _ in range(a.reps))[a.reps // 2]
+        emit({"what": "wah_pipeline", "query": f"Q{tmpl}.{seen[tmpl]}", "rows": n, "wah_and_decode_ms": wah_ms,
+              "wah_compress_ms_wall": comp_ms, "stream_words": [int(s.numel()) for s in streams],
+              "fused_plain_ms": fused})
+    eng.close()
+    # compression / decompression throughput on bitmaps of three densities
+    n = a.codec_rows
+    words = (n + 31) // 32
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    for name, bm in (("dense", torch.randint(-2**31, 2**31 - 1, (words,), dtype=torch.int32, device="cuda",
+                                              generator=g)),
+                     ("runs", torch.repeat_interleave(torch.tensor([0, -1, 0x5555], dtype=torch.int32,
+                                                                   device="cuda").repeat(words // 3000 + 1),
+                                                      1000)[:words].contiguous()),
+                     ("sparse", (torch.rand(words, device="cuda", generator=g) < 0.01).to(torch.int32))):
+        w = wah_compress(bm, n)
+        enc_ms = timed(lambda: wah_compress(bm, n), a.reps)
+        dec_ms = timed(lambda: wah_decompress(w, n), a.reps)
+        bm_bytes, st_bytes = 4 * words, 4 * int(w.numel())
+        emit({"what": "wah_codec", "bitmap": name, "rows": n, "stream_words": int(w.numel()),
+              "encode_ms": enc_ms, "decode_ms": dec_ms,
+              "encode_gbs": (bm_bytes + st_bytes) / enc_ms / 1e6, "decode_gbs": (bm_bytes + st_bytes) / dec_ms / 1e6})
+    if a.out:
+        Path(a.out).write_text("".join(json.dumps(d) + "\n" for d in lines))
+
+
+if __name__ == "__main__":
+    main()
