@@ -280,6 +280,20 @@ MB_API mb_status mb_vprg_grpby(const mb_vprg *p, const mb_op *op, uint32_t nr_gr
 MB_API mb_status mb_join_grpby(uint64_t nrows, const mb_op *op, uint32_t nr_grp,
                         int64_t *out, uint64_t *nqual, void *stream);
 
+/* The same result through Crystal-style hash joins (the reference's comparison
+ * system, crystal/src/ssb/q21.cu and siblings): for each foreign key whose
+ * dimension attributes carry clauses of their own (every term of the clause
+ * reads that key's dimension, whose size dimsz must be set), the dimension
+ * rows passing them go into an open-addressing table keyed by dimension key
+ * and carrying the op's attributes on that key (up to 3, each <= 4 bytes; up
+ * to 4 keys); one pass over the fact rows then evaluates the fact-column
+ * clauses, probes the tables (a miss eliminates the row) and aggregates.
+ * Tables up to 48 KB are copied into each CTA's shared memory.  Waits for
+ * the stream once (the table sizes).  An op without such clauses runs as
+ * mb_join_grpby. */
+MB_API mb_status mb_hash_join_grpby(uint64_t nrows, const mb_op *op, uint32_t nr_grp,
+                                    int64_t *out, uint64_t *nqual, void *stream);
+
 /* ------------------------------------------------------------------------- */
 /* Host planning helpers of the reference's operator API                     */
 /* ------------------------------------------------------------------------- */
@@ -478,7 +492,10 @@ MB_API mb_status mb_engine_plan_index(mb_engine *e, const mb_query *qs, uint32_t
 typedef enum mb_plan_kind {
   MB_PLAN_FUSED = 0,        /* virtual program + fused join-probe + group-by */
   MB_PLAN_SCAN = 1,         /* no index: every row through the op */
-  MB_PLAN_MATERIALISED = 2  /* stage 1 -> row list -> stage 3 */
+  MB_PLAN_MATERIALISED = 2, /* stage 1 -> row list -> stage 3 */
+  MB_PLAN_HASH = 3          /* no index: Crystal-style hash joins (mb_hash_join_grpby) over the
+                               dimensions, probed in one pass over the fact rows; waits once
+                               per query for its table sizes */
 } mb_plan_kind;
 
 /* Per-query plan knobs.  The arithmetic never depends on them. */

@@ -113,7 +113,7 @@ class mb_query(C.Structure):
     _fields_ = [("tmpl", C.c_uint32), ("p", C.c_uint32 * 8)]
 
 
-PLAN_FUSED, PLAN_SCAN, PLAN_MATERIALISED = range(3)
+PLAN_FUSED, PLAN_SCAN, PLAN_MATERIALISED, PLAN_HASH = range(4)
 MB_INDEX_PROBE_DIMS = 1
 MB_INDEX_LEVELS = 10
 MB_LEVELS_ALL = 0x3FF
@@ -205,6 +205,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_vprg_grpby": (I32, [C.POINTER(mb_vprg), C.POINTER(mb_op), U32, VOIDP, VOIDP,
                             C.POINTER(mb_launch), VOIDP]),
     "mb_join_grpby": (I32, [U64, C.POINTER(mb_op), U32, VOIDP, VOIDP, VOIDP]),
+    "mb_hash_join_grpby": (I32, [U64, C.POINTER(mb_op), U32, VOIDP, VOIDP, VOIDP]),
     "mb_col_from_bin": (I32, [U32, C.POINTER(C.c_void_p), C.POINTER(U64), U64, U64, C.POINTER(mb_col),
                                C.POINTER(C.c_void_p)]),
     "mb_col_from_bin2": (I32, [U32, C.POINTER(C.c_void_p), C.POINTER(U64), U32, C.POINTER(C.c_void_p),

@@ -46,6 +46,27 @@ const DevInfo &dev_info() {
   return d;
 }
 
+cudaMemPool_t scratch_pool() {
+  static std::mutex mu;
+  static std::vector<cudaMemPool_t> pools;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)pools.size() <= dev) pools.resize(dev + 1, nullptr);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+
 uint32_t *device_error_word() {
   static std::mutex mu;
   static std::vector<uint32_t *> words;

@@ -55,6 +55,36 @@ const DevInfo &dev_info();
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// A stream-ordered memory pool per device for short-lived scratch, which
+// keeps what it was given (release threshold: unlimited) so that repeated
+// calls reuse it instead of mapping fresh memory each time.
+cudaMemPool_t scratch_pool();
+
+// Device scratch from that pool, freed on scope exit (stream-ordered: after
+// the work enqueued on `st` before the exit).
+struct Scratch {
+  cudaStream_t st;
+  void *ptrs[16];
+  int n = 0;
+  explicit Scratch(cudaStream_t s) : st(s) {}
+  ~Scratch() {
+    for (int i = 0; i < n; ++i) cudaFreeAsync(ptrs[i], st);
+  }
+  Scratch(const Scratch &) = delete;
+  Scratch &operator=(const Scratch &) = delete;
+  template <typename T>
+  mb_status get(T **p, uint64_t count) {
+    cudaMemPool_t pool = scratch_pool();
+    if (!pool || n == 16) return fail(MB_ERR_CUDA, "scratch: no memory pool or too many buffers");
+    void *q = nullptr;
+    const cudaError_t e = cudaMallocFromPoolAsync(&q, count ? count * sizeof(T) : sizeof(T), pool, st);
+    if (e != cudaSuccess) return cuda_fail(e, "scratch allocation");
+    ptrs[n++] = q;
+    *p = static_cast<T *>(q);
+    return MB_OK;
+  }
+};
+
 inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
 inline uint64_t round_up(uint64_t a, uint64_t b) { return ceil_div(a, b) * b; }
 

@@ -532,7 +532,10 @@ void ssb_build_op(const SsbSrc &S, const mb_query &q, mb_op &out) {
   out = b.o;
 }
 
-static void build_op(const Engine &E, const mb_query &q, mb_op &out) {
+// joins: dimension attributes through their foreign keys even where the
+// engine keeps denormalised copies (the hash-join plan builds its tables
+// from the dimensions).
+static void build_op(const Engine &E, const mb_query &q, mb_op &out, bool joins = false) {
   SsbSrc S;
   S.date = fact_src(E.orderdate, E.fact_width("orderdate"));
   S.disc = fact_src(E.discount, E.fact_width("discount"));
@@ -541,8 +544,8 @@ static void build_op(const Engine &E, const mb_query &q, mb_op &out) {
   S.rev = fact_src(E.revenue, 4);
   S.scost = fact_src(E.supplycost, 4);
   S.scity = fact_src(E.suppcity, E.fact_width("suppcity"));
-  S.ccity = E.ccity_src();
-  S.mfgr = E.mfgr_src();
+  S.ccity = joins ? join_src(E.custcity, E.custkey, E.ncust + 1, 1) : E.ccity_src();
+  S.mfgr = joins ? join_src(E.partmfgr, E.partkey, E.npart + 1, 2) : E.mfgr_src();
   ssb_build_op(S, q, out);
 }
 
@@ -559,9 +562,10 @@ static void query_preds(const mb_query &q, std::vector<Pred> &preds) {
 mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered &L) {
   if (q.tmpl < 1 || q.tmpl > 4) return fail(MB_ERR_INVALID, "query: template %u not in 1..4", q.tmpl);
   if (!E.indexed) return fail(MB_ERR_INVALID, "query: the engine has no index (mb_engine_build_index)");
+  if (plan.kind > MB_PLAN_HASH) return fail(MB_ERR_INVALID, "query: plan kind %u", plan.kind);
   L = Lowered();
   L.ngroups = query_ngroups(q);
-  build_op(E, q, L.op);
+  build_op(E, q, L.op, plan.kind == MB_PLAN_HASH);
   query_preds(q, L.preds);
   const int nchk = (int)L.op.nclause;
   L.covers.resize(L.preds.size());
@@ -845,6 +849,7 @@ mb_status run_lowered(Engine &E, Lowered &L, const mb_plan &plan, int64_t *d_out
     return MB_OK;
   }
   if (plan.kind == MB_PLAN_SCAN) return mb_join_grpby(E.nrows, &L.op, L.ngroups, d_out, d_nq, st);
+  if (plan.kind == MB_PLAN_HASH) return mb_hash_join_grpby(E.nrows, &L.op, L.ngroups, d_out, d_nq, st);
   // materialise predicates whose bit is set: their operand becomes one
   // (certain, uncertain) bitmap pair evaluated up front
   const uint64_t W = E.stride;

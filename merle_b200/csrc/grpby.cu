@@ -732,3 +732,339 @@ extern "C" mb_status mb_bitmap_to_rows_noalloc(const uint32_t *possible, const u
   MB_LAUNCH_CHECK("rows_write_kernel");
   return MB_OK;
 }
+
+// ------------------------------------------------------- hash-join plan
+// Crystal-style join plan (the reference's comparison system, crystal/src/ssb/q21.cu and
+// its siblings: build a hash table per filtered dimension, then one pass over the fact rows
+// probes them).  For every foreign key whose dimension attributes carry a predicate of their
+// own (a clause all of whose terms read that dimension), the dimension rows passing those
+// clauses go into an open-addressing table keyed by dimension key and carrying the
+// attributes the op reads; the probe pass evaluates the fact-column clauses first, then looks
+// each key up (a miss eliminates the row), then the remaining clauses, group key and value.
+// Tables up to HJ_SMEM_MAX bytes are copied into every CTA's shared memory.  Results equal
+// mb_join_grpby's on the same op.
+namespace mb {
+
+constexpr uint32_t HJ_MAXT = 4;                 // tables (distinct foreign keys) per op
+constexpr uint32_t HJ_PAY = 3;                  // attributes one entry carries
+constexpr uint32_t HJ_SMEM_MAX = 48 * 1024;     // per staged table
+constexpr uint32_t HJ_SMEM_TOTAL = 128 * 1024;  // all staged tables
+
+struct HjTable {
+  const uint32_t *fk;
+  uint64_t dimsz;
+  uint4 *slots;       // {key, a0, a1, a2}; key HASH_EMPTY = free
+  uint32_t mask;      // capacity - 1
+  uint32_t npay;
+  uint32_t pushed;    // clauses evaluated at the build
+  uint32_t smem_off;  // byte offset of the staged copy, or ~0u
+  uint32_t pay_src[HJ_PAY];
+};
+
+struct HjPlan {
+  uint32_t ntab;
+  HjTable tab[HJ_MAXT];
+  int32_t src_tab[MB_MAXSRC];   // table carrying source s, -1: read directly
+  uint32_t src_pay[MB_MAXSRC];  // its slot in the entry
+  uint32_t fact_clauses;        // probe clauses that read fact columns only
+  uint32_t late_clauses;        // the other probe clauses
+  uint32_t term0[MB_MAXCLAUSE]; // first term of each clause
+};
+
+// Clauses `mask` on dimension row d of table t (sources read at index d).
+__device__ __forceinline__ bool hj_dim_pass(const mb_op &O, const HjPlan &H, uint32_t mask, uint64_t d) {
+  for (uint32_t c = 0; c < O.nclause; ++c) {
+    if (!(mask >> c & 1u)) continue;
+    bool any = false;
+    for (uint32_t k = 0, t = H.term0[c]; k < O.clause_len[c] && !any; ++k, ++t) {
+      const mb_term &tm = O.terms[t];
+      const uint64_t v = load_width(O.src[tm.src].col, d, O.src[tm.src].width);
+      any = v >= tm.lo && v < tm.hi;
+    }
+    if (!any) return false;
+  }
+  return true;
+}
+
+__global__ void hj_count_kernel(const __grid_constant__ mb_op O, const __grid_constant__ HjPlan H, uint32_t t,
+                                unsigned long long *count) {
+  const HjTable &T = H.tab[t];
+  uint32_t c = 0;
+  for (uint64_t d = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; d < T.dimsz; d += (uint64_t)gridDim.x * blockDim.x)
+    c += hj_dim_pass(O, H, T.pushed, d) ? 1u : 0u;
+  for (int o = 16; o; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count + t, (unsigned long long)c);
+}
+
+__global__ void hj_insert_kernel(const __grid_constant__ mb_op O, const __grid_constant__ HjPlan H, uint32_t t,
+                                 uint32_t *overflow) {
+  const HjTable &T = H.tab[t];
+  for (uint64_t d = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; d < T.dimsz;
+       d += (uint64_t)gridDim.x * blockDim.x) {
+    if (!hj_dim_pass(O, H, T.pushed, d)) continue;
+    uint32_t a[HJ_PAY] = {0, 0, 0};
+    for (uint32_t j = 0; j < T.npay; ++j) {
+      const mb_src &s = O.src[T.pay_src[j]];
+      a[j] = (uint32_t)load_width(s.col, d, s.width);
+    }
+    uint32_t h = hash32((uint32_t)d) & T.mask;
+    bool placed = false;
+    for (uint32_t p = 0; p <= T.mask && !placed; ++p, h = (h + 1) & T.mask) {
+      if (atomicCAS(&T.slots[h].x, HASH_EMPTY, (uint32_t)d) == HASH_EMPTY) {
+        T.slots[h].y = a[0], T.slots[h].z = a[1], T.slots[h].w = a[2];
+        placed = true;
+      }
+    }
+    if (!placed) atomicExch(overflow, 1u);  // cannot happen at capacity >= 2 x entries
+  }
+}
+
+// Value of source s at `row`: a table's attribute, or a direct read (as
+// src_value: false when a foreign key is out of its dimension).
+__device__ __forceinline__ bool hj_value(const mb_op &O, const HjPlan &H, uint32_t s, uint32_t row,
+                                         const uint32_t *got, uint64_t &v) {
+  const int32_t t = H.src_tab[s];
+  if (t >= 0) {
+    v = got[t * HJ_PAY + H.src_pay[s]];
+    return true;
+  }
+  return src_value(O.src[s], row, v);
+}
+
+__device__ __forceinline__ bool hj_clauses(const mb_op &O, const HjPlan &H, uint32_t mask, uint32_t row,
+                                           const uint32_t *got) {
+  for (uint32_t c = 0; c < O.nclause; ++c) {
+    if (!(mask >> c & 1u)) continue;
+    bool any = false;
+    for (uint32_t k = 0, t = H.term0[c]; k < O.clause_len[c] && !any; ++k, ++t) {
+      const mb_term &tm = O.terms[t];
+      uint64_t v;
+      any = hj_value(O, H, tm.src, row, got, v) && v >= tm.lo && v < tm.hi;
+    }
+    if (!any) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool hj_row(const mb_op &O, const HjPlan &H, const uint4 *const *tabs, uint32_t row,
+                                       uint32_t nr_grp, int64_t &value, uint32_t &group) {
+  uint32_t got[HJ_MAXT * HJ_PAY];
+  if (!hj_clauses(O, H, H.fact_clauses, row, got)) return false;
+  for (uint32_t t = 0; t < H.ntab; ++t) {
+    const HjTable &T = H.tab[t];
+    const uint32_t key = __ldg(T.fk + row);
+    uint32_t h = hash32(key) & T.mask;
+    const uint4 *tab = tabs[t];
+    for (;;) {  // at least half the slots are free: the walk ends
+      const uint4 e = tab[h];
+      if (e.x == key) {
+        got[t * HJ_PAY + 0] = e.y, got[t * HJ_PAY + 1] = e.z, got[t * HJ_PAY + 2] = e.w;
+        break;
+      }
+      if (e.x == HASH_EMPTY) return false;
+      h = (h + 1) & T.mask;
+    }
+  }
+  if (!hj_clauses(O, H, H.late_clauses, row, got)) return false;
+  uint32_t g = 0;
+  for (uint32_t k = 0; k < O.nkey; ++k) {
+    const mb_key &kk = O.keys[k];
+    uint64_t v;
+    if (!hj_value(O, H, kk.src, row, got, v)) return false;
+    uint32_t x = (uint32_t)v;
+    if (kk.xform == MB_X_DIV) x = (uint32_t)(v / kk.div);
+    else if (kk.xform == MB_X_YEAR) x = date_to_year((uint32_t)v);
+    g += kk.mul * (x - kk.base);
+  }
+  if (g >= nr_grp) return false;
+  uint64_t a = 0, b = 0;
+  switch (O.vkind) {
+  case MB_V_ONE: value = 1; break;
+  case MB_V_COL:
+    if (!hj_value(O, H, O.va, row, got, a)) return false;
+    value = (int64_t)a;
+    break;
+  case MB_V_MUL:
+    if (!hj_value(O, H, O.va, row, got, a) || !hj_value(O, H, O.vb, row, got, b)) return false;
+    value = (int64_t)(a * b);
+    break;
+  default:
+    if (!hj_value(O, H, O.va, row, got, a) || !hj_value(O, H, O.vb, row, got, b)) return false;
+    value = (int64_t)a - (int64_t)b;
+    break;
+  }
+  group = g;
+  return true;
+}
+
+template <int GS>
+__global__ void __launch_bounds__(512)
+hj_probe_kernel(uint64_t nrows, const __grid_constant__ mb_op O, const __grid_constant__ HjPlan H, uint32_t nr_grp,
+                uint32_t hcap, uint32_t grp_bytes, unsigned long long *__restrict__ out,
+                unsigned long long *__restrict__ nqual) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  __shared__ uint64_t red[64];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  GrpCtx G = grp_init<GS>(smem, nr_grp, hcap, out);
+  const uint4 *tabs[HJ_MAXT];
+  for (uint32_t t = 0; t < HJ_MAXT; ++t) {
+    tabs[t] = nullptr;
+    if (t >= H.ntab) continue;
+    const HjTable &T = H.tab[t];
+    if (T.smem_off == ~0u) {
+      tabs[t] = T.slots;
+      continue;
+    }
+    uint4 *dst = reinterpret_cast<uint4 *>(smem + grp_bytes + T.smem_off);
+    for (uint32_t i = threadIdx.x; i <= T.mask; i += blockDim.x) dst[i] = T.slots[i];
+    tabs[t] = dst;
+  }
+  __syncthreads();
+  int64_t acc = 0;
+  uint64_t cnt = 0;
+  const uint64_t nchunks = (nrows + 31) / 32;
+  for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nchunks; ch += (uint64_t)gridDim.x * nw) {
+    const uint64_t row = ch * 32 + lane;
+    bool kept = false;
+    int64_t val = 0;
+    uint32_t grp = 0;
+    if (row < nrows) kept = hj_row(O, H, tabs, (uint32_t)row, nr_grp, val, grp);
+    cnt += kept ? 1u : 0u;
+    aggregate<GS>(G, kept, grp, val, acc);
+  }
+  __syncthreads();
+  grp_flush<GS>(G, nr_grp, acc, cnt, nqual, red);
+}
+
+template <int GS>
+static mb_status launch_hj(uint64_t n, const mb_op &O, const HjPlan &H, uint32_t smem_tables, uint32_t nr_grp,
+                           int64_t *out, uint64_t *nqual, cudaStream_t st) {
+  auto kern = hj_probe_kernel<GS>;
+  const uint32_t warps = 8;
+  const size_t grp_bytes = (grp_smem_bytes(GS, nr_grp, DEFAULT_HCAP) + 15) & ~(size_t)15;
+  LaunchShape ls;
+  MB_CHECK(shape_for(kern, warps, grp_bytes + smem_tables, (n + 31) / 32, &ls, 0));
+  kern<<<ls.grid, ls.block, ls.smem, st>>>(n, O, H, nr_grp, DEFAULT_HCAP, (uint32_t)grp_bytes,
+                                           reinterpret_cast<unsigned long long *>(out),
+                                           reinterpret_cast<unsigned long long *>(nqual));
+  MB_LAUNCH_CHECK("hj_probe_kernel");
+  return MB_OK;
+}
+
+}  // namespace mb
+
+extern "C" mb_status mb_hash_join_grpby(uint64_t nrows, const mb_op *op, uint32_t nr_grp, int64_t *out,
+                                        uint64_t *nqual, void *stream) {
+  using namespace mb;
+  if (!out || !nqual) return fail(MB_ERR_INVALID, "mb_hash_join_grpby: NULL output");
+  if (nr_grp == 0) return fail(MB_ERR_INVALID, "mb_hash_join_grpby: nr_grp == 0");
+  MB_CHECK(validate_op(op));
+  if (nrows >= (1ull << 32)) return fail(MB_ERR_INVALID, "mb_hash_join_grpby: rows >= 2^32");
+  const mb_op &O = *op;
+  HjPlan H;
+  memset(&H, 0, sizeof(H));
+  for (uint32_t s = 0; s < MB_MAXSRC; ++s) H.src_tab[s] = -1;
+  uint32_t t0 = 0;
+  for (uint32_t c = 0; c < O.nclause; ++c) H.term0[c] = t0, t0 += O.clause_len[c];
+  // clauses whose terms all read one foreign key's dimension go into that key's table
+  uint32_t pushed_any = 0;
+  for (uint32_t c = 0; c < O.nclause; ++c) {
+    const uint32_t *fk = nullptr;
+    bool one = O.clause_len[c] > 0;
+    for (uint32_t k = 0; k < O.clause_len[c]; ++k) {
+      const mb_src &s = O.src[O.terms[H.term0[c] + k].src];
+      if (!s.fk || s.dimsz == 0 || s.width > 4 || (fk && s.fk != fk)) one = false;
+      fk = s.fk;
+    }
+    if (!one) continue;
+    uint32_t t = 0;
+    while (t < H.ntab && H.tab[t].fk != fk) ++t;
+    if (t == H.ntab) {
+      if (H.ntab == HJ_MAXT) continue;  // more keys than tables: probe this clause directly
+      H.tab[t].fk = fk;
+      H.tab[t].dimsz = ~0ull;
+      ++H.ntab;
+    }
+    H.tab[t].pushed |= 1u << c;
+    pushed_any |= 1u << c;
+  }
+  // each table carries every source on its key (the op may read them later)
+  for (uint32_t t = 0; t < H.ntab; ++t) {
+    HjTable &T = H.tab[t];
+    for (uint32_t s = 0; s < O.nsrc; ++s) {
+      if (O.src[s].fk != T.fk) continue;
+      if (O.src[s].width > 4 || T.npay == HJ_PAY)
+        return fail(MB_ERR_UNSUPPORTED, "mb_hash_join_grpby: more than %u attributes (or one over 4 bytes) on one key",
+                    HJ_PAY);
+      T.dimsz = std::min<uint64_t>(T.dimsz, O.src[s].dimsz ? O.src[s].dimsz : ~0ull);
+      H.src_tab[s] = (int32_t)t;
+      H.src_pay[s] = T.npay;
+      T.pay_src[T.npay++] = s;
+    }
+  }
+  for (uint32_t c = 0; c < O.nclause; ++c) {
+    if (pushed_any >> c & 1u) continue;
+    bool fact = true;
+    for (uint32_t k = 0; k < O.clause_len[c]; ++k)
+      if (O.src[O.terms[H.term0[c] + k].src].fk) fact = false;
+    (fact ? H.fact_clauses : H.late_clauses) |= 1u << c;
+  }
+  cudaStream_t st = as_stream(stream);
+  MB_CUDA(cudaMemsetAsync(out, 0, (size_t)nr_grp * sizeof(int64_t), st));
+  MB_CUDA(cudaMemsetAsync(nqual, 0, sizeof(uint64_t), st));
+  if (nrows == 0) return MB_OK;
+  // build: count the passing dimension rows of every table (one wait), size
+  // each table to a power of two >= 2 x its rows, insert
+  uint64_t cnt[HJ_MAXT] = {0, 0, 0, 0};
+  if (H.ntab) {
+    Scratch sc(st);  // freed after the probe, in stream order
+    unsigned long long *dcnt;
+    MB_CHECK(sc.get(&dcnt, HJ_MAXT + 1));
+    MB_CUDA(cudaMemsetAsync(dcnt, 0, 8 * (HJ_MAXT + 1), st));
+    for (uint32_t t = 0; t < H.ntab; ++t) {
+      const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(H.tab[t].dimsz, 256), (uint64_t)dev_info().sms * 8);
+      hj_count_kernel<<<grid, 256, 0, st>>>(O, H, t, dcnt);
+      MB_LAUNCH_CHECK("hj_count_kernel");
+    }
+    MB_CUDA(cudaMemcpyAsync(cnt, dcnt, 8 * HJ_MAXT, cudaMemcpyDeviceToHost, st));
+    MB_CUDA(cudaStreamSynchronize(st));
+    for (uint32_t t = 0; t < H.ntab; ++t)
+      if (cnt[t] == 0) return MB_OK;  // a dimension with no passing row: nothing qualifies
+    uint64_t off = 0, smem_tables = 0;
+    uint64_t offs[HJ_MAXT];
+    for (uint32_t t = 0; t < H.ntab; ++t) {
+      uint64_t capt = 64;
+      while (capt < 2 * cnt[t]) capt <<= 1;
+      H.tab[t].mask = (uint32_t)(capt - 1);
+      offs[t] = off;
+      off += capt * 16;
+      H.tab[t].smem_off = ~0u;
+      if (capt * 16 <= HJ_SMEM_MAX && smem_tables + capt * 16 <= HJ_SMEM_TOTAL) {
+        H.tab[t].smem_off = (uint32_t)smem_tables;
+        smem_tables += capt * 16;
+      }
+    }
+    uint8_t *base;
+    MB_CHECK(sc.get(&base, off));
+    uint32_t *overflow = reinterpret_cast<uint32_t *>(dcnt + HJ_MAXT);
+    for (uint32_t t = 0; t < H.ntab; ++t) {
+      H.tab[t].slots = reinterpret_cast<uint4 *>(base + offs[t]);
+      MB_CUDA(cudaMemsetAsync(H.tab[t].slots, 0xff, (size_t)(H.tab[t].mask + 1) * 16, st));
+    }
+    for (uint32_t t = 0; t < H.ntab; ++t) {
+      const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(H.tab[t].dimsz, 256), (uint64_t)dev_info().sms * 8);
+      hj_insert_kernel<<<grid, 256, 0, st>>>(O, H, t, overflow);
+      MB_LAUNCH_CHECK("hj_insert_kernel");
+    }
+    const int gs = pick_gs(nr_grp, MB_GRP_AUTO);
+    mb_status r;
+    switch (gs) {
+    case GS_SCALAR: r = launch_hj<GS_SCALAR>(nrows, O, H, (uint32_t)smem_tables, nr_grp, out, nqual, st); break;
+    case GS_SHARED: r = launch_hj<GS_SHARED>(nrows, O, H, (uint32_t)smem_tables, nr_grp, out, nqual, st); break;
+    default: r = launch_hj<GS_GLOBAL>(nrows, O, H, (uint32_t)smem_tables, nr_grp, out, nqual, st); break;
+    }
+    return r;
+  }
+  // no table to build: the plain scan
+  return mb_join_grpby(nrows, op, nr_grp, out, nqual, stream);
+}

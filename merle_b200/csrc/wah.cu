@@ -27,7 +27,6 @@
 // All passes are HBM-bound integer work: no tensor cores.
 #include <string.h>
 #include <stdio.h>
-#include <mutex>
 #include <vector>
 #include "common.cuh"
 
@@ -435,50 +434,6 @@ __global__ void __launch_bounds__(DT) wah_dec_emit(const uint32_t *wah, const ui
     bm[w] = o;
   }
 }
-
-// A stream-ordered memory pool per device for the passes' scratch, which
-// keeps what it was given (release threshold: unlimited) so that repeated
-// calls reuse it instead of mapping fresh memory each time.
-cudaMemPool_t scratch_pool() {
-  static std::mutex mu;
-  static cudaMemPool_t pools[64] = {};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-  std::lock_guard<std::mutex> lk(mu);
-  if (!pools[dev]) {
-    cudaMemPoolProps props{};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = dev;
-    cudaMemPool_t p = nullptr;
-    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
-    uint64_t keep = ~0ull;
-    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
-    pools[dev] = p;
-  }
-  return pools[dev];
-}
-
-// Device scratch from that pool, freed on scope exit (stream-ordered).
-struct Scratch {
-  cudaStream_t st;
-  std::vector<void *> ptrs;
-  explicit Scratch(cudaStream_t s) : st(s) {}
-  ~Scratch() {
-    for (void *p : ptrs) cudaFreeAsync(p, st);
-  }
-  template <typename T>
-  mb_status get(T **p, uint64_t count) {
-    cudaMemPool_t pool = scratch_pool();
-    if (!pool) return fail(MB_ERR_CUDA, "wah: no scratch memory pool");
-    void *q = nullptr;
-    const cudaError_t e = cudaMallocFromPoolAsync(&q, count ? count * sizeof(T) : sizeof(T), pool, st);
-    if (e != cudaSuccess) return cuda_fail(e, "wah: scratch allocation");
-    ptrs.push_back(q);
-    *p = static_cast<T *>(q);
-    return MB_OK;
-  }
-};
 
 // Encodes the groups of S into out (capacity words); *nwords = words of the
 // stream, also when it does not fit (nothing is written then).
