@@ -796,8 +796,9 @@ __global__ void hj_count_kernel(const __grid_constant__ mb_op O, const __grid_co
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(count + t, (unsigned long long)c);
 }
 
-__global__ void hj_insert_kernel(const __grid_constant__ mb_op O, const __grid_constant__ HjPlan H, uint32_t t,
-                                 uint32_t *overflow) {
+// Inserts the passing dimension rows of table t.  The walk from a key's hash
+// slot ends within the table: it holds at most half as many rows as slots.
+__global__ void hj_insert_kernel(const __grid_constant__ mb_op O, const __grid_constant__ HjPlan H, uint32_t t) {
   const HjTable &T = H.tab[t];
   for (uint64_t d = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; d < T.dimsz;
        d += (uint64_t)gridDim.x * blockDim.x) {
@@ -808,14 +809,11 @@ __global__ void hj_insert_kernel(const __grid_constant__ mb_op O, const __grid_c
       a[j] = (uint32_t)load_width(s.col, d, s.width);
     }
     uint32_t h = hash32((uint32_t)d) & T.mask;
-    bool placed = false;
-    for (uint32_t p = 0; p <= T.mask && !placed; ++p, h = (h + 1) & T.mask) {
+    for (uint32_t p = 0; p <= T.mask; ++p, h = (h + 1) & T.mask)
       if (atomicCAS(&T.slots[h].x, HASH_EMPTY, (uint32_t)d) == HASH_EMPTY) {
         T.slots[h].y = a[0], T.slots[h].z = a[1], T.slots[h].w = a[2];
-        placed = true;
+        break;
       }
-    }
-    if (!placed) atomicExch(overflow, 1u);  // cannot happen at capacity >= 2 x entries
   }
 }
 
@@ -1019,8 +1017,8 @@ extern "C" mb_status mb_hash_join_grpby(uint64_t nrows, const mb_op *op, uint32_
   if (H.ntab) {
     Scratch sc(st);  // freed after the probe, in stream order
     unsigned long long *dcnt;
-    MB_CHECK(sc.get(&dcnt, HJ_MAXT + 1));
-    MB_CUDA(cudaMemsetAsync(dcnt, 0, 8 * (HJ_MAXT + 1), st));
+    MB_CHECK(sc.get(&dcnt, HJ_MAXT));
+    MB_CUDA(cudaMemsetAsync(dcnt, 0, 8 * HJ_MAXT, st));
     for (uint32_t t = 0; t < H.ntab; ++t) {
       const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(H.tab[t].dimsz, 256), (uint64_t)dev_info().sms * 8);
       hj_count_kernel<<<grid, 256, 0, st>>>(O, H, t, dcnt);
@@ -1046,14 +1044,13 @@ extern "C" mb_status mb_hash_join_grpby(uint64_t nrows, const mb_op *op, uint32_
     }
     uint8_t *base;
     MB_CHECK(sc.get(&base, off));
-    uint32_t *overflow = reinterpret_cast<uint32_t *>(dcnt + HJ_MAXT);
     for (uint32_t t = 0; t < H.ntab; ++t) {
       H.tab[t].slots = reinterpret_cast<uint4 *>(base + offs[t]);
       MB_CUDA(cudaMemsetAsync(H.tab[t].slots, 0xff, (size_t)(H.tab[t].mask + 1) * 16, st));
     }
     for (uint32_t t = 0; t < H.ntab; ++t) {
       const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(H.tab[t].dimsz, 256), (uint64_t)dev_info().sms * 8);
-      hj_insert_kernel<<<grid, 256, 0, st>>>(O, H, t, overflow);
+      hj_insert_kernel<<<grid, 256, 0, st>>>(O, H, t);
       MB_LAUNCH_CHECK("hj_insert_kernel");
     }
     const int gs = pick_gs(nr_grp, MB_GRP_AUTO);
