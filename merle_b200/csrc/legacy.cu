@@ -679,8 +679,95 @@ extern "C" uint32_t *ssb_bmp_control_abl_nofuse(const ssb_schema *dat, size_t n)
   return ssb_control(dat, n, 1, 0x10u, 0, "ssb_bmp_control_abl_nofuse");
 }
 
-extern "C" void ssb_wah(const ssb_schema *, const ssb_schema *, size_t) {
-  printf("\nWAH\tthe compressed-bitmap baseline is not part of this library\n");
+// ------------------------------------------------------- WAH baseline
+// The reference's compressed-bitmap baseline (ssb/wah-demo.cu:22-240,
+// synth/wah_roast.cu:5-36) on this library's WAH kernels: one bitmap per
+// predicate, compressed with row 31g + j at bit 30 - j (dbjoinFlatWah's
+// order); timed: WAH_REPS repetitions of the streams' AND chain and the
+// decompression of the result (the synthetic query: OR, then AND), with
+// events around them, in milliseconds per repetition.
+namespace {
+constexpr int WAH_REPS = 100;
+
+struct WahPred {
+  mb_src src;
+  uint64_t lo, hi;
+};
+
+bool wah_streams(const std::vector<WahPred> &preds, uint64_t n, DevBufs &B, std::vector<uint32_t *> &w,
+                 std::vector<uint64_t> &wn, uint32_t **bm) {
+  const uint64_t G = mb_wah_groups(n), stride = mb_bitmap_stride(n);
+  *bm = static_cast<uint32_t *>(B.get(stride * 4));
+  if (!*bm) return false;
+  for (const WahPred &p : preds) {
+    uint32_t *s = static_cast<uint32_t *>(B.get(G * 4));
+    uint64_t k = 0;
+    if (!s || mb_bitmap_create(&p.src, n, &p.lo, &p.hi, 1, *bm, stride, nullptr, nullptr) != MB_OK ||
+        mb_wah_encode(*bm, n, MB_WAH_MSB, s, G, &k, nullptr) != MB_OK)
+      return false;
+    w.push_back(s);
+    wn.push_back(k);
+  }
+  return true;
+}
+
+// ops[i] combines the running result with stream i + 1; decode: expand the
+// result each repetition.
+bool wah_time(const std::vector<uint32_t *> &w, const std::vector<uint64_t> &wn, const std::vector<uint32_t> &ops,
+              bool decode, uint64_t n, uint32_t *bm, DevBufs &B, float *ms) {
+  const uint64_t G = mb_wah_groups(n);
+  uint32_t *t[2] = {static_cast<uint32_t *>(B.get(G * 4)), static_cast<uint32_t *>(B.get(G * 4))};
+  if (!t[0] || !t[1]) return false;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return false;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return false;
+  }
+  bool ok = cudaEventRecord(e0) == cudaSuccess;
+  for (int rep = 0; ok && rep < WAH_REPS; ++rep) {
+    const uint32_t *r = w[0];
+    uint64_t rn = wn[0];
+    for (size_t k = 1; ok && k < w.size(); ++k) {
+      uint32_t *o = t[k & 1];
+      uint64_t on = 0;
+      ok = mb_wah_op(ops[k - 1], r, rn, w[k], wn[k], G, o, G, &on, nullptr) == MB_OK;
+      r = o, rn = on;
+    }
+    if (ok && decode) ok = mb_wah_decode(r, rn, MB_WAH_MSB, n, bm, nullptr) == MB_OK;
+  }
+  ok = ok && cudaEventRecord(e1) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+       cudaEventElapsedTime(ms, e0, e1) == cudaSuccess;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms /= WAH_REPS;
+  return ok;
+}
+}  // namespace
+
+extern "C" void ssb_wah(const ssb_schema *, const ssb_schema *dat, size_t factSz) {
+  const SsbSrc S = ssb_srcs(dat);
+  puts("\nCase\tWAH\tRTScan");
+  for (const SsbQ &sq : SSB13) {
+    const uint32_t *p = sq.q.p;
+    std::vector<WahPred> preds;
+    switch (sq.q.tmpl) {
+    case 1: preds = {{S.date, p[0], p[1]}, {S.disc, p[2], p[3]}, {S.qty, p[4], p[5]}}; break;
+    case 2: preds = {{S.mfgr, p[0], p[1]}, {S.scity, p[2], p[3]}}; break;
+    case 3: preds = {{S.ccity, p[0], p[1]}, {S.scity, p[2], p[3]}, {S.date, p[4], p[5]}}; break;
+    default: preds = {{S.ccity, p[0], p[1]}, {S.scity, p[2], p[3]}, {S.mfgr, p[4], p[5]}, {S.date, p[6], p[7]}};
+    }
+    DevBufs B;
+    std::vector<uint32_t *> w;
+    std::vector<uint64_t> wn;
+    uint32_t *bm = nullptr;
+    float ms = 0;
+    const std::vector<uint32_t> ands(preds.size() - 1, MB_WAH_AND);
+    if (!wah_streams(preds, factSz, B, w, wn, &bm) || !wah_time(w, wn, ands, true, factSz, bm, B, &ms))
+      printf("%s\tfailed: %s\n", sq.name, mb_last_error());
+    else  // RTScan (an OptiX ray-tracing scan) is not run here
+      printf("%s\t%.4f\tunavailable\n", sq.name, ms);
+  }
 }
 
 extern "C" bool ssb_demoall(const char *dir) {
@@ -879,9 +966,24 @@ extern "C" float2 synth_method(const synth_schema *dat, uint32_t n, uint32_t fa1
   return r;
 }
 
-extern "C" void synth_wah(const synth_schema *, uint32_t, uint32_t, uint32_t, uint32_t, uint32_t, uint32_t,
-                          uint32_t) {
-  puts("\t0.0");
+extern "C" void synth_wah(const synth_schema *dat, uint32_t factsz, uint32_t fa1lo, uint32_t fa1hi, uint32_t fa2lo,
+                          uint32_t fa2hi, uint32_t da1lo, uint32_t da1hi) {
+  // (a1 in R1 OR a2 in R2) AND key in R3: the dimension attribute is the key
+  // itself (synth/cpuref.c:80), so its predicate is a range on the key column
+  const uint32_t w = dat->bitwidth / 8;
+  const std::vector<WahPred> preds = {{src_of(dat->factattr1, w), fa1lo, fa1hi},
+                                      {src_of(dat->factattr2, w), fa2lo, fa2hi},
+                                      {src_of(dat->fkey, 4), da1lo, da1hi}};
+  DevBufs B;
+  std::vector<uint32_t *> ws;
+  std::vector<uint64_t> wn;
+  uint32_t *bm = nullptr;
+  float ms = 0;
+  if (!wah_streams(preds, factsz, B, ws, wn, &bm) ||
+      !wah_time(ws, wn, {MB_WAH_OR, MB_WAH_AND}, false, factsz, bm, B, &ms))
+    printf("\tfailed: %s\n", mb_last_error());
+  else
+    printf("\t%.4f\n", ms);
 }
 
 extern "C" double *window_zipf(double s, size_t n, size_t win) {

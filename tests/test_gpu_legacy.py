@@ -88,11 +88,17 @@ def test_ssb_cpujoin_matches_reference_golden(cuda, mb, ssb_dir):
         L.ssb_free(C.byref(h), None)
 
 
-def test_ssb_demoall(cuda, mb, ssb_dir):
+def test_ssb_demoall(cuda, mb, ssb_dir, capfd):
     """Load, fixed index, every fixed-layout and controlled-layout path: all
-    equal ssb_cpujoin (the reference's own driver flow, ssb/cpuref.c:318-349)."""
+    equal ssb_cpujoin (the reference's own driver flow, ssb/cpuref.c:318-349).
+    The WAH baseline runs first and times all 13 queries (ssb/wah-demo.cu)."""
     L = _lib(mb)
     assert L.ssb_demoall(str(ssb_dir).encode())
+    out = capfd.readouterr().out.splitlines()
+    i = out.index("Case\tWAH\tRTScan")
+    rows = [ln.split("\t") for ln in out[i + 1:i + 14]]
+    assert [r[0] for r in rows] == [f"SSB{a}{b}" for a, n in ((1, 3), (2, 3), (3, 4), (4, 3)) for b in range(1, n + 1)]
+    assert all(len(r) == 3 and float(r[1]) > 0 and r[2] == "unavailable" for r in rows)
 
 
 def test_ssb_load_missing_dir(cuda, mb, tmp_path):
