@@ -86,7 +86,7 @@ struct CostModel {
   // mean gap between arrivals: decayed sums of gaps and of weights, so that
   // the first few gaps give their plain mean rather than the first alone
   double g_sum = 0, g_w = 0, last_us = -1;
-  static constexpr double DECAY = 0.97, GAP_DECAY = 1 - 1.0 / 128, OVERLOAD = 0.95;
+  static constexpr double DECAY = 0.97, GAP_DECAY = 1 - 1.0 / 128, OVERLOAD = 1.0;
   void add_arrival(double t_us) {
     if (last_us >= 0) {
       g_sum = GAP_DECAY * g_sum + (t_us - last_us) * 1e-3;
