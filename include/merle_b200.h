@@ -821,6 +821,17 @@ MB_API mb_status mb_wah_ngroups(const uint32_t *wah, uint64_t nwords, uint64_t *
  * forms (wahGpu.cuh:11-30; wahAndCPU, wahCpu.c:27-79). */
 MB_API mb_status mb_wah_op(uint32_t op, const uint32_t *a, uint64_t na, const uint32_t *b, uint64_t nb,
                            uint64_t ngroups, uint32_t *out, uint64_t capacity, uint64_t *nwords, void *stream);
+/* The same with the method chosen: MB_WAH_EXPLICIT expands both streams,
+ * combines the bitmaps and compresses the result (the reference's explicit
+ * forms, wahAndExpl ...); MB_WAH_DIRECT cuts the runs of both streams at the
+ * union of their word boundaries and combines each piece whole, never
+ * expanding (wahAnd / wahOr / wahXor, merle/wahGpuDirect.cu); MB_WAH_AUTO
+ * (mb_wah_op) takes the direct form when na + nb < ngroups / 8.  Both give
+ * the same canonical stream. */
+typedef enum mb_wah_method { MB_WAH_AUTO = 0, MB_WAH_EXPLICIT = 1, MB_WAH_DIRECT = 2 } mb_wah_method;
+MB_API mb_status mb_wah_op_ex(uint32_t op, const uint32_t *a, uint64_t na, const uint32_t *b, uint64_t nb,
+                              uint64_t ngroups, uint32_t method, uint32_t *out, uint64_t capacity,
+                              uint64_t *nwords, void *stream);
 /* The reference's WAH file (struct wahHost_s, wahCpu.h:10-15; read by
  * loadWahFile, wahConv.c:93-109): 24-byte header (has1Fill, magic 0x44f8a1ef,
  * cmprsNrWord, decmprsNrWord) then the words.  HOST buffers.  Load with

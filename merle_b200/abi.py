@@ -276,12 +276,14 @@ SIGNATURES: dict[str, tuple] = {
     "mb_wah_decode": (I32, [VOIDP, U64, U32, U64, VOIDP, VOIDP]),
     "mb_wah_ngroups": (I32, [VOIDP, U64, C.POINTER(U64), VOIDP]),
     "mb_wah_op": (I32, [U32, VOIDP, U64, VOIDP, U64, U64, VOIDP, U64, C.POINTER(U64), VOIDP]),
+    "mb_wah_op_ex": (I32, [U32, VOIDP, U64, VOIDP, U64, U64, U32, VOIDP, U64, C.POINTER(U64), VOIDP]),
     "mb_wah_save": (I32, [C.c_char_p, VOIDP, U64, U64]),
     "mb_wah_load": (I32, [C.c_char_p, VOIDP, U64, C.POINTER(U64), C.POINTER(U64)]),
 }
 
 WAH_LSB, WAH_MSB = 0, 1
 WAH_AND, WAH_OR, WAH_XOR = 0, 1, 2
+WAH_AUTO, WAH_EXPLICIT, WAH_DIRECT = 0, 1, 2
 
 
 def bind(lib: C.CDLL, sigs: dict[str, tuple]) -> None:

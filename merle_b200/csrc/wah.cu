@@ -508,6 +508,150 @@ mb_status decode(const uint32_t *wah, uint64_t n, uint32_t order, uint64_t nrows
 
 bool aligned4(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 3) == 0; }
 
+// ----------------------------------------------- direct (compressed) ops
+// The reference's direct operations (wahAnd / wahOr / wahXor,
+// merle/wahGpuDirect.cu) never expand the streams: the runs of both are cut
+// at the union of their word boundaries and each piece is combined whole.
+// Here: (1) the group scans SA, SB of both streams (saturated, clamped to G);
+// (2) a merge of the two boundary lists by rank (an A boundary's rank is its
+// index plus the B boundaries below it, a B boundary's its index plus the A
+// boundaries at or below it); (3) piece r is [m[r], m[r+1]) (the last one
+// ends at G), its value op(A's word, B's word) at its first group; a piece
+// starts an output word when its value is a literal or its kind differs from
+// the kind at the group before it; (4) fill runs as in the encoder.
+struct DirectSrc {
+  const uint32_t *a, *b, *SA, *SB;  // streams and their exclusive group scans
+  uint64_t na, nb, G;
+  uint32_t op;
+};
+
+// Value (31 bits) of op(A, B) at group g (< G), with its kind.
+__device__ __forceinline__ uint32_t direct_value(const DirectSrc &D, uint64_t g) {
+  uint32_t va = 0, vb = 0;
+  if (D.na && g < D.SA[D.na]) va = group_value(__ldg(D.a + last_le(D.SA, 0, D.na - 1, g)), 0);
+  if (D.nb && g < D.SB[D.nb]) vb = group_value(__ldg(D.b + last_le(D.SB, 0, D.nb - 1, g)), 0);
+  return D.op == 0 ? va & vb : D.op == 1 ? va | vb : va ^ vb;
+}
+
+__device__ __forceinline__ uint32_t clamp_g(uint32_t x, uint64_t G) { return x < G ? x : (uint32_t)G; }
+
+// (2) the merged boundary list m[0 .. na + nb + 1].
+__global__ void wah_direct_merge(const DirectSrc D, uint32_t *m) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i <= D.na) {
+    const uint32_t v = clamp_g(D.SA[i], D.G);
+    uint64_t lo = 0, hi = D.nb + 1;  // B boundaries < v
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) / 2;
+      if (clamp_g(D.SB[mid], D.G) < v) lo = mid + 1;
+      else hi = mid;
+    }
+    m[i + lo] = v;
+  } else if (i <= D.na + 1 + D.nb) {
+    const uint64_t j = i - D.na - 1;
+    const uint32_t v = clamp_g(D.SB[j], D.G);
+    uint64_t lo = 0, hi = D.na + 1;  // A boundaries <= v
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) / 2;
+      if (clamp_g(D.SA[mid], D.G) <= v) lo = mid + 1;
+      else hi = mid;
+    }
+    m[j + lo] = v;
+  }
+}
+
+// Piece r starts an output word: *v = its value, *x = its first group.
+__device__ __forceinline__ bool direct_flag(const DirectSrc &D, const uint32_t *m, uint64_t M, uint64_t r,
+                                            uint32_t *v, uint64_t *x) {
+  if (r >= M) return false;
+  const uint64_t x0 = m[r], y0 = r + 1 < M ? m[r + 1] : D.G;
+  *x = x0;
+  if (x0 >= y0 || x0 >= D.G) return false;
+  *v = direct_value(D, x0);
+  const uint32_t k = kind_of(*v);
+  if (k == 2u || x0 == 0) return true;
+  return k != kind_of(direct_value(D, x0 - 1));
+}
+
+// (3a) output words per block of WB pieces.
+__global__ void __launch_bounds__(WT) wah_direct_count(const DirectSrc D, const uint32_t *m, uint64_t M,
+                                                       uint64_t *bcnt) {
+  uint32_t c = 0, v;
+  uint64_t x;
+#pragma unroll
+  for (uint32_t i = 0; i < WI; ++i)
+    c += direct_flag(D, m, M, (uint64_t)blockIdx.x * WB + i * WT + threadIdx.x, &v, &x) ? 1u : 0u;
+  uint64_t total;
+  block_excl_scan<uint64_t>(c, &total);
+  if (threadIdx.x == 0) bcnt[blockIdx.x] = total;
+}
+
+// (3b) the words, in piece order; each word's first group into pos.
+__global__ void __launch_bounds__(WT) wah_direct_write(const DirectSrc D, const uint32_t *m, uint64_t M,
+                                                       const uint64_t *boff, uint32_t *out, uint32_t *pos) {
+  uint64_t at = boff[blockIdx.x];
+#pragma unroll 1
+  for (uint32_t i = 0; i < WI; ++i) {
+    uint32_t v = 0, total;
+    uint64_t x = 0;
+    const bool f = direct_flag(D, m, M, (uint64_t)blockIdx.x * WB + i * WT + threadIdx.x, &v, &x);
+    const uint32_t ex = block_flag_scan(f ? 1u : 0u, &total);
+    if (f) {
+      const uint32_t k = kind_of(v);
+      out[at + ex] = k == 2u ? v : (k == 1u ? FILL | ONES : FILL);
+      pos[at + ex] = (uint32_t)x;
+    }
+    at += total;
+  }
+}
+
+mb_status direct_op(uint32_t op, const uint32_t *a, uint64_t na, const uint32_t *b, uint64_t nb, uint64_t G,
+                    uint32_t *out, uint64_t capacity, uint64_t *nwords, cudaStream_t st) {
+  Scratch sc(st);
+  DirectSrc D{a, b, nullptr, nullptr, na, nb, G, op};
+  uint32_t *SA, *SB, *m;
+  const uint32_t zero = 0;
+  if (na) {
+    MB_CHECK(group_scan(a, na, sc, &SA, st));
+  } else {
+    MB_CHECK(sc.get(&SA, 1));
+    MB_CUDA(cudaMemcpyAsync(SA, &zero, 4, cudaMemcpyHostToDevice, st));
+  }
+  if (nb) {
+    MB_CHECK(group_scan(b, nb, sc, &SB, st));
+  } else {
+    MB_CHECK(sc.get(&SB, 1));
+    MB_CUDA(cudaMemcpyAsync(SB, &zero, 4, cudaMemcpyHostToDevice, st));
+  }
+  D.SA = SA, D.SB = SB;
+  const uint64_t M = na + nb + 2;
+  MB_CHECK(sc.get(&m, M));
+  wah_direct_merge<<<(unsigned)ceil_div(M, 256), 256, 0, st>>>(D, m);
+  MB_LAUNCH_CHECK("wah_direct_merge");
+  const uint64_t nblk = ceil_div(M, WB);
+  uint64_t *boff;
+  MB_CHECK(sc.get(&boff, nblk + 1));
+  wah_direct_count<<<(unsigned)nblk, WT, 0, st>>>(D, m, M, boff);
+  MB_LAUNCH_CHECK("wah_direct_count");
+  wah_scan_blocks<<<1, 1024, 0, st>>>(boff, nblk);
+  MB_LAUNCH_CHECK("wah_scan_blocks");
+  uint64_t K = 0;
+  MB_CUDA(cudaMemcpyAsync(&K, boff + nblk, 8, cudaMemcpyDeviceToHost, st));
+  MB_CUDA(cudaStreamSynchronize(st));
+  *nwords = K;
+  if (!out) return MB_OK;
+  if (K > capacity) return fail(MB_ERR_INVALID, "mb_wah_op: the stream has %llu words, the output holds %llu",
+                                (unsigned long long)K, (unsigned long long)capacity);
+  uint32_t *pos;
+  MB_CHECK(sc.get(&pos, K));
+  wah_direct_write<<<(unsigned)nblk, WT, 0, st>>>(D, m, M, boff, out, pos);
+  MB_LAUNCH_CHECK("wah_direct_write");
+  const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(K, 256), (uint64_t)dev_info().sms * 8);
+  wah_enc_fills<<<grid, 256, 0, st>>>(out, pos, K, G);
+  MB_LAUNCH_CHECK("wah_enc_fills");
+  return MB_OK;
+}
+
 }  // namespace
 }  // namespace mb
 
@@ -559,15 +703,26 @@ extern "C" mb_status mb_wah_ngroups(const uint32_t *wah, uint64_t nwords, uint64
 
 extern "C" mb_status mb_wah_op(uint32_t op, const uint32_t *a, uint64_t na, const uint32_t *b, uint64_t nb,
                                uint64_t ngroups, uint32_t *out, uint64_t capacity, uint64_t *nwords, void *stream) {
+  return mb_wah_op_ex(op, a, na, b, nb, ngroups, MB_WAH_AUTO, out, capacity, nwords, stream);
+}
+
+extern "C" mb_status mb_wah_op_ex(uint32_t op, const uint32_t *a, uint64_t na, const uint32_t *b, uint64_t nb,
+                                  uint64_t ngroups, uint32_t method, uint32_t *out, uint64_t capacity,
+                                  uint64_t *nwords, void *stream) {
   NvtxRange nvtx_("mb_wah_op");
   if (!nwords) return fail(MB_ERR_INVALID, "mb_wah_op: NULL word count");
   *nwords = 0;
   if (op > MB_WAH_XOR) return fail(MB_ERR_INVALID, "mb_wah_op: op %u", op);
+  if (method > MB_WAH_DIRECT) return fail(MB_ERR_INVALID, "mb_wah_op: method %u", method);
   if ((na && !a) || (nb && !b)) return fail(MB_ERR_INVALID, "mb_wah_op: NULL stream");
   if (ngroups > MAX_GROUPS) return fail(MB_ERR_INVALID, "mb_wah_op: %llu groups exceed the 30-bit run count",
                                         (unsigned long long)ngroups);
   if (ngroups == 0) return MB_OK;
   cudaStream_t st = as_stream(stream);
+  // direct when the streams are short next to the groups: its work follows
+  // the words (with a binary search per piece), the explicit form's the rows
+  if (method == MB_WAH_DIRECT || (method == MB_WAH_AUTO && 8 * (na + nb) < ngroups))
+    return direct_op(op, a, na, b, nb, ngroups, out, capacity, nwords, st);
   // decode both (the order is immaterial: both sides and the result keep
   // the streams' own), then encode op(x, y)
   const uint64_t nrows = 31 * ngroups, stride = mb_bitmap_stride(nrows);

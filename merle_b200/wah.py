@@ -9,7 +9,9 @@ Names follow the reference's:
   WAH streams (``order``: ``abi.WAH_LSB`` puts row 31g + j of group g at bit j,
   ``abi.WAH_MSB`` at bit 30 - j);
 - ``wah_and`` / ``wah_or`` / ``wah_xor``: ``wahAnd`` / ``wahOr`` / ``wahXor``
-  (merle/wahGpu.cuh:11-30): canonical streams in, a canonical stream out;
+  (merle/wahGpu.cuh:11-30): a canonical stream out, computed directly on the
+  runs when the streams are short next to the rows, else by expanding them
+  (``method`` picks one: ``abi.WAH_DIRECT`` / ``abi.WAH_EXPLICIT``);
 - ``load_wah_file`` / ``save_wah_file``: ``loadWahFile``
   (merle/host/wahConv.c:93-109) and the matching writer.
 
@@ -76,28 +78,28 @@ def wah_ngroups(wah, stream=None) -> int:
     return n.value
 
 
-def _op(op: int, a, b, ngroups: int | None, stream=None):
+def _op(op: int, a, b, ngroups: int | None, stream=None, method: int = abi.WAH_AUTO):
     torch = _torch()
     if ngroups is None:
         ngroups = max(wah_ngroups(a, stream), wah_ngroups(b, stream))
     cap = max(1, ngroups)
     out = torch.empty(cap, dtype=torch.int32, device=a.device)
     n = C.c_uint64()
-    check(lib().mb_wah_op(op, _ptr(a), a.numel(), _ptr(b), b.numel(), ngroups, _ptr(out), cap, C.byref(n),
-                          _stream(stream)))
+    check(lib().mb_wah_op_ex(op, _ptr(a), a.numel(), _ptr(b), b.numel(), ngroups, method, _ptr(out), cap,
+                             C.byref(n), _stream(stream)))
     return out[:n.value]
 
 
-def wah_and(a, b, ngroups: int | None = None, stream=None):
-    return _op(abi.WAH_AND, a, b, ngroups, stream)
+def wah_and(a, b, ngroups: int | None = None, stream=None, method: int = abi.WAH_AUTO):
+    return _op(abi.WAH_AND, a, b, ngroups, stream, method)
 
 
-def wah_or(a, b, ngroups: int | None = None, stream=None):
-    return _op(abi.WAH_OR, a, b, ngroups, stream)
+def wah_or(a, b, ngroups: int | None = None, stream=None, method: int = abi.WAH_AUTO):
+    return _op(abi.WAH_OR, a, b, ngroups, stream, method)
 
 
-def wah_xor(a, b, ngroups: int | None = None, stream=None):
-    return _op(abi.WAH_XOR, a, b, ngroups, stream)
+def wah_xor(a, b, ngroups: int | None = None, stream=None, method: int = abi.WAH_AUTO):
+    return _op(abi.WAH_XOR, a, b, ngroups, stream, method)
 
 
 def save_wah_file(path: str | Path, words: np.ndarray, ngroups: int) -> None:
@@ -223,9 +225,15 @@ def main(argv=None) -> None:
         enc_ms = timed(lambda: wah_compress(bm, n), a.reps)
         dec_ms = timed(lambda: wah_decompress(w, n), a.reps)
         bm_bytes, st_bytes = 4 * words, 4 * int(w.numel())
+        # AND with the same bitmap shifted by 1,000 words (another stream of its kind)
+        w2 = wah_compress(torch.roll(bm, 1000), n)
+        Gn = wah_groups(n)
+        ops_ms = {m: timed(lambda: wah_and(w, w2, Gn, method=k), a.reps)
+                  for m, k in (("explicit", abi.WAH_EXPLICIT), ("direct", abi.WAH_DIRECT))}
         emit({"what": "wah_codec", "bitmap": name, "rows": n, "stream_words": int(w.numel()),
               "encode_ms": enc_ms, "decode_ms": dec_ms,
-              "encode_gbs": (bm_bytes + st_bytes) / enc_ms / 1e6, "decode_gbs": (bm_bytes + st_bytes) / dec_ms / 1e6})
+              "encode_gbs": (bm_bytes + st_bytes) / enc_ms / 1e6, "decode_gbs": (bm_bytes + st_bytes) / dec_ms / 1e6,
+              "and_explicit_ms": ops_ms["explicit"], "and_direct_ms": ops_ms["direct"]})
     if a.out:
         Path(a.out).write_text("".join(json.dumps(d) + "\n" for d in lines))
 

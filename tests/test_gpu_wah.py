@@ -217,3 +217,47 @@ def test_round_trip_600M_rows(cuda):
         back = W.wah_decompress(w, n, order)
         assert T.equal(back[:words], bm) and not back[words:].any()
         assert T.equal(W.wah_and(w, w, W.wah_groups(n)), w)
+
+
+def _noncanonical(rng, G: int) -> np.ndarray:
+    """A stream over about G groups with what canonical streams never hold:
+    zero-count fills, literals equal to 0 or 0x7fffffff, neighbouring fills
+    of one kind."""
+    out, g = [], 0
+    while g < G:
+        k = int(rng.integers(0, 6))
+        if k == 0:
+            out.append(FILL | int(rng.integers(0, 50)))
+            g += out[-1] & 0x3FFFFFFF
+        elif k == 1:
+            out.append(FILL | ONES | int(rng.integers(0, 50)))
+            g += out[-1] & 0x3FFFFFFF
+        elif k == 2:
+            out.append(int(rng.choice([0, 0x7FFFFFFF])))
+            g += 1
+        else:
+            out.append(int(rng.integers(1, 0x7FFFFFFF)))
+            g += 1
+    return np.array(out, np.uint32)
+
+
+@pytest.mark.parametrize("op", [abi.WAH_AND, abi.WAH_OR, abi.WAH_XOR])
+def test_direct_ops_equal_explicit_and_oracle(orc, cuda, op):
+    """The direct form (runs cut at both streams' boundaries) gives the
+    explicit form's canonical stream: random, sparse, run-heavy and
+    non-canonical inputs, streams shorter and longer than the groups asked."""
+    rng = np.random.default_rng(40 + op)
+    cases = []
+    for nrows in (31, 62, 31 * 700 + 9, 1_000_003):
+        for ka, kb in (("runs", "sparse"), ("dense", "runs"), ("zero", "one"), ("sparse", "sparse")):
+            x, y = random_bitmap(rng, nrows, ka), random_bitmap(rng, nrows, kb)
+            cases.append((orc.wah_encode(x, nrows, 0), orc.wah_encode(y, nrows, 0), (nrows + 30) // 31))
+    for G in (1, 40, 1000, 5000):
+        cases.append((_noncanonical(rng, G), _noncanonical(rng, G // 2 + 1), G))
+        cases.append((_noncanonical(rng, G), np.zeros(0, np.uint32), G + 17))
+    for wa, wb, G in cases:
+        want = orc.wah_op(op, wa, wb, G)
+        da, db = dev32(wa) if len(wa) else D.empty(0, 4)[:0], dev32(wb) if len(wb) else D.empty(0, 4)[:0]
+        for method in (abi.WAH_EXPLICIT, abi.WAH_DIRECT, abi.WAH_AUTO):
+            got = host32(W._op(op, da, db, G, method=method))
+            np.testing.assert_array_equal(got, want, err_msg=f"op {op} method {method} G {G}")
