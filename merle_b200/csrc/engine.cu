@@ -559,7 +559,7 @@ static void query_preds(const mb_query &q, std::vector<Pred> &preds) {
   }
 }
 
-mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered &L) {
+mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered &L, bool stats) {
   if (q.tmpl < 1 || q.tmpl > 4) return fail(MB_ERR_INVALID, "query: template %u not in 1..4", q.tmpl);
   if (!E.indexed) return fail(MB_ERR_INVALID, "query: the engine has no index (mb_engine_build_index)");
   if (plan.kind > MB_PLAN_HASH) return fail(MB_ERR_INVALID, "query: plan kind %u", plan.kind);
@@ -573,9 +573,11 @@ mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered
     const Pred &pr = L.preds[i];
     L.covers[i] = plan_cover(E.idx[pr.col], pr.lo, pr.hi, E.stride, nchk);
     if (L.covers[i].empty) L.empty = true;
-    // plan-independent canonical count: the fewer of direct and complement exact covers
-    Cover d = plan_cover(E.idx[pr.col], pr.lo, pr.hi, E.stride, 1 << 20);  // edges priced out
-    L.canonical_bitmaps += d.full || d.empty ? 0 : d.nb();
+    if (stats) {
+      // plan-independent canonical count: the fewer of direct and complement exact covers
+      Cover d = plan_cover(E.idx[pr.col], pr.lo, pr.hi, E.stride, 1 << 20);  // edges priced out
+      L.canonical_bitmaps += d.full || d.empty ? 0 : d.nb();
+    }
   }
   // predicate order: most selective first (ANDM skips loads under zero words)
   std::vector<int> order;
@@ -899,7 +901,7 @@ extern "C" mb_status mb_engine_query(mb_engine *e, const mb_query *q, const mb_p
   if (plan) pl = *plan;
   else MB_CHECK(mb_engine_plan_rule(e, q, &pl));
   Lowered L;
-  MB_CHECK(lower_query(E, *q, pl, L));
+  MB_CHECK(lower_query(E, *q, pl, L, stats != nullptr));
   MB_CHECK(E.ensure_out(L.ngroups));
   MB_CUDA(cudaEventRecord(E.ev0, E.stream));
   MB_CHECK(run_lowered(E, L, pl, E.d_out, E.d_nqual, true));

@@ -158,7 +158,8 @@ bool mlp_shape(const mb_mlp *m, uint32_t *in, uint32_t *out);
 // The cheapest cover of [lo, hi) with c's levels; *cost_out (if given) = its
 // cost in bytes (bitmap bytes + candidate-check sectors of its edge rows).
 Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t W, int nchk_sources, uint64_t *cost_out = nullptr);
-mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered &L);
+// stats: also count the plan-independent canonical bitmaps (query stats only)
+mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered &L, bool stats = false);
 uint32_t query_ngroups(const mb_query &q);
 mb_status run_lowered(Engine &E, Lowered &L, const mb_plan &plan, int64_t *d_out, uint64_t *d_nq, bool zero);
 
