@@ -563,7 +563,7 @@ mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered
   if (q.tmpl < 1 || q.tmpl > 4) return fail(MB_ERR_INVALID, "query: template %u not in 1..4", q.tmpl);
   if (!E.indexed) return fail(MB_ERR_INVALID, "query: the engine has no index (mb_engine_build_index)");
   if (plan.kind > MB_PLAN_HASH) return fail(MB_ERR_INVALID, "query: plan kind %u", plan.kind);
-  L = Lowered();
+  L.reset();
   L.ngroups = query_ngroups(q);
   build_op(E, q, L.op, plan.kind == MB_PLAN_HASH);
   query_preds(q, L.preds);

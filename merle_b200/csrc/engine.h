@@ -59,6 +59,19 @@ struct Lowered {
   std::vector<Cover> covers;
   int col_pred[MB_MAXCOLS] = {};   // predicate (template order) of each program operand
   uint64_t canonical_bitmaps = 0;  // plan-independent: min(direct, complement) exact cover
+  // Back to the state of a fresh Lowered for the fields lowering reads before
+  // writing (prg, op and mids are rewritten in full, the vectors keep their
+  // storage).
+  void reset() {
+    ngroups = 1;
+    empty = false;
+    nbitmaps = 0;
+    chk = false;
+    preds.clear();
+    covers.clear();
+    for (int &c : col_pred) c = 0;
+    canonical_bitmaps = 0;
+  }
 };
 
 struct Engine {
