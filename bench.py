@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default launch shape instead of the autotuner's")
     ap.add_argument("--no-graph", action="store_true", help="enqueue each step instead of replaying a CUDA graph")
+    ap.add_argument("--wah", action="store_true",
+                    help="instead of the headline: the WAH baseline (compress two predicate bitmaps, AND the "
+                         "streams) on the GPU beside the reference's CPU WAH code")
     return ap.parse_args()
 
 
@@ -245,10 +248,75 @@ def batch_algo_bytes(star, scale: float, nrows: int, qs, ngroups) -> dict:
             "total": int(bm + sec * scale + out), "rows": int(rows * scale)}
 
 
+def wah_arm(args):
+    """One JSON line: SSB Q1.1's date and discount predicate bitmaps over the
+    table (the reference's WAH baseline, ssb/wah-demo.cu:22-76) compressed and
+    ANDed as WAH streams, per step; the reference's own CPU code for the same
+    steps (wahCmprsCPU in place, wahAndCPU; merle/host/) timed on a bounded
+    sample of the rows beside it.  Rows/s of both."""
+    import torch
+    from merle_b200 import abi, device as D, wah as W
+    from oracle import oracle as O
+    n = args.rows or 6_000_000 * args.k
+    star = D.DevStar(SEED_DATA, args.k, n)
+    bms = [D.bitmap_create(D.src_of(star[c]), n, [lo], [hi])[0][0]
+           for c, lo, hi in (("orderdate", 366, 731), ("discount", 1, 4))]
+    G = W.wah_groups(n)
+
+    def step():
+        a, b = (W.wah_compress(x, n, abi.WAH_MSB) for x in bms)
+        return W.wah_and(a, b, G)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        r = step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    # the reference on the host: the groups of the first sample rows (MSB
+    # order, as dbjoinFlatWah builds them), compressed in place and ANDed
+    cpu = None
+    wref = O.wah_ref()
+    if wref is not None:
+        sample = min(n, 310_000_000) // 31 * 31
+        words = (sample + 31) // 32
+        groups = []
+        for bm in bms:
+            bits = np.unpackbits(D.to_host(bm[:words], np.uint32).view(np.uint8), bitorder="little")[:sample]
+            g = np.packbits(bits.reshape(-1, 31), axis=1, bitorder="big")
+            g = (g.astype(np.uint32) @ np.array([1 << 24, 1 << 16, 1 << 8, 1], np.uint32)) >> 1
+            groups.append(np.ascontiguousarray(g.astype(np.uint32)))
+        t0 = time.perf_counter()
+        bufs, ns = [], []
+        for g in groups:
+            buf = g.copy()
+            ns.append(wref.wahCmprsCPU(O.ptr(buf), len(buf), O.ptr(buf)))
+            bufs.append(np.concatenate([buf[:ns[-1]], np.zeros(2, np.uint32)]))
+        out = np.zeros(ns[0] + ns[1] + 4, np.uint32)
+        wref.wahAndCPU(O.ptr(bufs[0]), O.ptr(bufs[0]) + 4 * ns[0], O.ptr(bufs[1]), O.ptr(bufs[1]) + 4 * ns[1],
+                       O.ptr(out), O.ptr(out) + 4 * len(out))
+        sec = time.perf_counter() - t0
+        cpu = {"value": sample / sec, "unit": "rows/s", "cores": 1, "kind": "reference",
+               "sample": f"the first {sample:,} rows: wahCmprsCPU of both predicates' 31-bit groups, wahAndCPU"}
+    print(json.dumps({"metric": "WAH baseline: compress two predicate bitmaps and AND the streams", "value": n / ms * 1e3,
+                      "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup),
+                      "ms_per_step": ms, "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+                      "config": {"workload": f"star schema k={args.k}, {n:,} rows; SSB Q1.1 date and discount "
+                                             "predicates", "stream_words": int(r.numel())},
+                      "cpu_baseline": cpu}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.wah:
+        wah_arm(args)
         return
     import torch
     import torch.distributed as dist
