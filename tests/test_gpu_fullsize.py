@@ -1,7 +1,8 @@
 """Parity at the benchmark configurations' full sizes, through properties
 that hold at any size (the CPU oracle is too slow there): at 600M rows the
 batched scan answers every query of the 64-query mix exactly as the plain
-path does; at 1.8B rows (row ids above 2^30, 132 GB resident) the answers of
+path does, and the no-index scan and the hash-join plan answer the SSB
+queries as the index plan does; at 1.8B rows (row ids above 2^30, 132 GB resident) the answers of
 the whole table equal the sums of the answers of its two halves, each half
 generated and indexed on its own (group sums and row counts are additive over
 row ranges)."""
@@ -26,6 +27,9 @@ def _plain(e, qs):
 
 
 def test_600M_batch_equals_plain(cuda, mb):
+    """The batched scan, the plain path, the no-index scan and the hash-join
+    plan agree on every query (the last two on the SSB queries)."""
+    from merle_b200 import abi
     e = Engine(0)
     try:
         e.gen_star(2, 100, 600_000_000, width4=True)
@@ -35,6 +39,14 @@ def test_600M_batch_equals_plain(cuda, mb):
         want, wn = _plain(e, qs)
         np.testing.assert_array_equal(out, want)
         np.testing.assert_array_equal(nq, wn)
+        for kind in (abi.PLAN_SCAN, abi.PLAN_HASH):
+            plan = abi.mb_plan()
+            plan.kind = kind
+            for q in WL.ssb13():
+                o1, n1, _ = e.query(q)
+                o2, n2, _ = e.query(q, plan)
+                np.testing.assert_array_equal(o2, o1, err_msg=f"kind {kind} {WL.as_tuple(q)}")
+                assert n2 == n1
     finally:
         e.close()
 
