@@ -241,26 +241,71 @@ vbp_grpby_kernel(const __grid_constant__ DevPrg P, const __grid_constant__ mb_op
 }
 
 // -------------------------------------------------------- no-index scan
+// Clause c alone on one row, as op_eval evaluates it.
+__device__ __forceinline__ bool clause_pass(const mb_op &O, uint32_t c, uint32_t t0, uint32_t row) {
+  bool any = false;
+  for (uint32_t k = 0; k < O.clause_len[c] && !any; ++k) {
+    const mb_term &tm = O.terms[t0 + k];
+    uint64_t v;
+    any = src_value(O.src[tm.src], row, v) && v >= tm.lo && v < tm.hi;
+  }
+  return any;
+}
+
+constexpr uint32_t JQ = 64;  // rows a warp queues between the screen and the op
+
+// Every row through the op.  A row first meets one clause (`screen`, first
+// term `t0`; none if screen >= nclause), one row per lane; the rows that pass
+// queue per warp, and each full warp of them runs the rest of the op, so the
+// lanes of its loads and branches are all live rows.  The result equals
+// op_eval on every row (the screen is one of the op's own clauses).
 template <int GS>
 __global__ void __launch_bounds__(512)
 join_grpby_kernel(uint64_t nrows, const __grid_constant__ mb_op O, uint32_t nr_grp, uint32_t hcap,
-                  unsigned long long *__restrict__ out, unsigned long long *__restrict__ nqual) {
+                  uint32_t grp_bytes, uint32_t screen, uint32_t t0, unsigned long long *__restrict__ out,
+                  unsigned long long *__restrict__ nqual) {
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ uint64_t red[64];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   GrpCtx G = grp_init<GS>(smem, nr_grp, hcap, out);
+  uint32_t *queue = reinterpret_cast<uint32_t *>(smem + grp_bytes) + (size_t)warp * JQ;
   __syncthreads();
   int64_t acc = 0;
   uint64_t cnt = 0;
-  const uint64_t nchunks = (nrows + 31) / 32;
-  for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nchunks; ch += (uint64_t)gridDim.x * nw) {
-    const uint64_t row = ch * 32 + lane;
+  uint32_t qn = 0;
+  const uint32_t lt = (1u << lane) - 1u;
+  auto drain = [&](uint32_t m) {  // the last m (<= 32) queued rows through the op
     bool kept = false;
     int64_t val = 0;
     uint32_t grp = 0;
-    if (row < nrows) kept = op_eval(O, (uint32_t)row, true, nr_grp, val, grp);
+    if (lane < m) kept = op_eval(O, queue[qn - m + lane], true, nr_grp, val, grp, screen);
     cnt += kept ? 1u : 0u;
     aggregate<GS>(G, kept, grp, val, acc);
+    qn -= m;
+    __syncwarp();
+  };
+  const uint64_t nchunks = (nrows + 31) / 32;
+  if (screen >= O.nclause) {  // no screen (or no room for the queues): every row through the op
+    for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nchunks; ch += (uint64_t)gridDim.x * nw) {
+      const uint64_t row = ch * 32 + lane;
+      bool kept = false;
+      int64_t val = 0;
+      uint32_t grp = 0;
+      if (row < nrows) kept = op_eval(O, (uint32_t)row, true, nr_grp, val, grp);
+      cnt += kept ? 1u : 0u;
+      aggregate<GS>(G, kept, grp, val, acc);
+    }
+  } else {
+    for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nchunks; ch += (uint64_t)gridDim.x * nw) {
+      const uint64_t row = ch * 32 + lane;
+      const bool pass = row < nrows && clause_pass(O, screen, t0, (uint32_t)row);
+      const uint32_t bal = __ballot_sync(0xffffffffu, pass);
+      if (pass) queue[qn + __popc(bal & lt)] = (uint32_t)row;
+      qn += __popc(bal);  // at most 31 + 32 < JQ
+      __syncwarp();
+      if (qn >= 32) drain(32);
+    }
+    if (qn) drain(qn);
   }
   __syncthreads();
   grp_flush<GS>(G, nr_grp, acc, cnt, nqual, red);
@@ -546,15 +591,49 @@ extern "C" mb_status mb_vprg_grpby(const mb_vprg *p, const mb_op *op, uint32_t n
   return fused_grpby(p, op, nr_grp, out, nqual, launch, as_stream(stream), true);
 }
 
+// The clause that screens rows in the no-index scan: the first whose terms
+// read fact columns only (one load a row), else the first; nclause if none.
+static uint32_t screen_clause(const mb_op &O, uint32_t *t0) {
+  uint32_t t = 0, first_t = 0;
+  for (uint32_t c = 0; c < O.nclause; ++c) {
+    bool fact = true;
+    for (uint32_t k = 0; k < O.clause_len[c]; ++k)
+      if (O.src[O.terms[t + k].src].fk) fact = false;
+    if (fact) {
+      *t0 = t;
+      return c;
+    }
+    t += O.clause_len[c];
+  }
+  *t0 = first_t;
+  return 0;
+}
+
 template <int GS>
 static mb_status launch_join(uint64_t n, const mb_op &O, uint32_t nr_grp, uint32_t hcap, int64_t *out,
                              uint64_t *nqual, cudaStream_t st) {
   auto kern = join_grpby_kernel<GS>;
   const uint32_t warps = 8;
-  const size_t smem = (grp_smem_bytes(GS, nr_grp, hcap) + 15) & ~(size_t)15;
+  const size_t gb = (grp_smem_bytes(GS, nr_grp, hcap) + 15) & ~(size_t)15;
+  uint32_t t0 = 0;
+  uint32_t screen = screen_clause(O, &t0);
+  // the row queues only where they cost no resident CTA (a large group
+  // table in shared memory can leave no room for them)
+  const size_t qbytes = (size_t)warps * JQ * 4;
+  if (screen < O.nclause) {
+    const size_t cap = (size_t)dev_info().max_smem_optin - 1024;  // room for the kernel's static shared memory
+    int with = 0, without = 0;
+    MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::min(cap, gb + qbytes)));
+    if (gb + qbytes <= cap)
+      MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&with, kern, (int)(warps * 32), gb + qbytes));
+    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&without, kern, (int)(warps * 32), gb));
+    if (with < without) screen = O.nclause;
+  }
+  const size_t smem = gb + (screen < O.nclause ? qbytes : 0);
   LaunchShape ls;
   MB_CHECK(shape_for(kern, warps, smem, (n + 31) / 32, &ls, 0));
-  kern<<<ls.grid, ls.block, ls.smem, st>>>(n, O, nr_grp, hcap, reinterpret_cast<unsigned long long *>(out),
+  kern<<<ls.grid, ls.block, ls.smem, st>>>(n, O, nr_grp, hcap, (uint32_t)gb, screen, t0,
+                                           reinterpret_cast<unsigned long long *>(out),
                                            reinterpret_cast<unsigned long long *>(nqual));
   MB_LAUNCH_CHECK("join_grpby_kernel");
   return MB_OK;
@@ -769,6 +848,7 @@ struct HjPlan {
   uint32_t fact_clauses;        // probe clauses that read fact columns only
   uint32_t late_clauses;        // the other probe clauses
   uint32_t term0[MB_MAXCLAUSE]; // first term of each clause
+  uint32_t smem_tables;         // bytes of the staged tables (the row queues follow)
 };
 
 // Clauses `mask` on dimension row d of table t (sources read at index d).
@@ -844,10 +924,10 @@ __device__ __forceinline__ bool hj_clauses(const mb_op &O, const HjPlan &H, uint
   return true;
 }
 
+// The op on a row whose fact-column clauses already passed.
 __device__ __forceinline__ bool hj_row(const mb_op &O, const HjPlan &H, const uint4 *const *tabs, uint32_t row,
                                        uint32_t nr_grp, int64_t &value, uint32_t &group) {
   uint32_t got[HJ_MAXT * HJ_PAY];
-  if (!hj_clauses(O, H, H.fact_clauses, row, got)) return false;
   for (uint32_t t = 0; t < H.ntab; ++t) {
     const HjTable &T = H.tab[t];
     const uint32_t key = __ldg(T.fk + row);
@@ -920,16 +1000,32 @@ hj_probe_kernel(uint64_t nrows, const __grid_constant__ mb_op O, const __grid_co
   __syncthreads();
   int64_t acc = 0;
   uint64_t cnt = 0;
-  const uint64_t nchunks = (nrows + 31) / 32;
-  for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nchunks; ch += (uint64_t)gridDim.x * nw) {
-    const uint64_t row = ch * 32 + lane;
+  // as the no-index scan: the fact-column clauses screen the rows one per
+  // lane, the rows that pass queue per warp and full warps of them probe
+  uint32_t *queue = reinterpret_cast<uint32_t *>(smem + grp_bytes + H.smem_tables) + (size_t)warp * JQ;
+  uint32_t qn = 0;
+  const uint32_t lt = (1u << lane) - 1u;
+  auto drain = [&](uint32_t m) {
     bool kept = false;
     int64_t val = 0;
     uint32_t grp = 0;
-    if (row < nrows) kept = hj_row(O, H, tabs, (uint32_t)row, nr_grp, val, grp);
+    if (lane < m) kept = hj_row(O, H, tabs, queue[qn - m + lane], nr_grp, val, grp);
     cnt += kept ? 1u : 0u;
     aggregate<GS>(G, kept, grp, val, acc);
+    qn -= m;
+    __syncwarp();
+  };
+  const uint64_t nchunks = (nrows + 31) / 32;
+  for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nchunks; ch += (uint64_t)gridDim.x * nw) {
+    const uint64_t row = ch * 32 + lane;
+    const bool pass = row < nrows && hj_clauses(O, H, H.fact_clauses, (uint32_t)row, nullptr);
+    const uint32_t bal = __ballot_sync(0xffffffffu, pass);
+    if (pass) queue[qn + __popc(bal & lt)] = (uint32_t)row;
+    qn += __popc(bal);
+    __syncwarp();
+    if (qn >= 32) drain(32);
   }
+  if (qn) drain(qn);
   __syncthreads();
   grp_flush<GS>(G, nr_grp, acc, cnt, nqual, red);
 }
@@ -941,7 +1037,7 @@ static mb_status launch_hj(uint64_t n, const mb_op &O, const HjPlan &H, uint32_t
   const uint32_t warps = 8;
   const size_t grp_bytes = (grp_smem_bytes(GS, nr_grp, DEFAULT_HCAP) + 15) & ~(size_t)15;
   LaunchShape ls;
-  MB_CHECK(shape_for(kern, warps, grp_bytes + smem_tables, (n + 31) / 32, &ls, 0));
+  MB_CHECK(shape_for(kern, warps, grp_bytes + smem_tables + (size_t)warps * JQ * 4, (n + 31) / 32, &ls, 0));
   kern<<<ls.grid, ls.block, ls.smem, st>>>(n, O, H, nr_grp, DEFAULT_HCAP, (uint32_t)grp_bytes,
                                            reinterpret_cast<unsigned long long *>(out),
                                            reinterpret_cast<unsigned long long *>(nqual));
@@ -1053,6 +1149,7 @@ extern "C" mb_status mb_hash_join_grpby(uint64_t nrows, const mb_op *op, uint32_
       hj_insert_kernel<<<grid, 256, 0, st>>>(O, H, t);
       MB_LAUNCH_CHECK("hj_insert_kernel");
     }
+    H.smem_tables = (uint32_t)smem_tables;
     const int gs = pick_gs(nr_grp, MB_GRP_AUTO);
     mb_status r;
     switch (gs) {

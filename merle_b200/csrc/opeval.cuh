@@ -27,12 +27,13 @@ __device__ __forceinline__ bool src_value(const mb_src &s, uint32_t row, uint64_
 }
 
 // The op on one row; returns true if the row is kept (value, group set).
+// Clause `passed` (if < nclause) is known to hold and is not re-evaluated.
 __device__ __forceinline__ bool op_eval(const mb_op &O, uint32_t row, bool chk, uint32_t nr_grp,
-                                        int64_t &value, uint32_t &group) {
+                                        int64_t &value, uint32_t &group, uint32_t passed = ~0u) {
   if (chk) {
     uint32_t t = 0;
     for (uint32_t c = 0; c < O.nclause; ++c) {
-      bool any = false;
+      bool any = c == passed;
       const uint32_t len = O.clause_len[c];
       for (uint32_t k = 0; k < len; ++k, ++t) {
         if (any) continue;
