@@ -252,15 +252,37 @@ __device__ __forceinline__ bool clause_pass(const mb_op &O, uint32_t c, uint32_t
   return any;
 }
 
-constexpr uint32_t JQ = 64;  // rows a warp queues between the screen and the op
+constexpr uint32_t JQ = 160;  // rows a warp queues between the screen and the op (31 + a 128-row chunk)
 
 // Every row through the op.  A row first meets one clause (`screen`, first
 // term `t0`; none if screen >= nclause), one row per lane; the rows that pass
 // queue per warp, and each full warp of them runs the rest of the op, so the
 // lanes of its loads and branches are all live rows.  The result equals
 // op_eval on every row (the screen is one of the op's own clauses).
-template <int GS>
-__global__ void __launch_bounds__(512)
+// Four consecutive values of a fact column of SW-byte elements from one
+// vector load (the column 16-byte aligned, rows r .. r+3 inside it, r a
+// multiple of 4).
+template <int SW>
+__device__ __forceinline__ void load4(const void *col, uint64_t r, uint64_t (&v)[4]) {
+  if (SW == 1) {
+    const uint32_t w = __ldg(reinterpret_cast<const uint32_t *>(col) + r / 4);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v[j] = (w >> (8 * j)) & 0xffu;
+  } else if (SW == 2) {
+    const uint2 w = __ldg(reinterpret_cast<const uint2 *>(col) + r / 4);
+    v[0] = w.x & 0xffffu, v[1] = w.x >> 16, v[2] = w.y & 0xffffu, v[3] = w.y >> 16;
+  } else if (SW == 4) {
+    const uint4 w = __ldg(reinterpret_cast<const uint4 *>(col) + r / 4);
+    v[0] = w.x, v[1] = w.y, v[2] = w.z, v[3] = w.w;
+  } else {
+    const ulonglong2 a = __ldg(reinterpret_cast<const ulonglong2 *>(col) + r / 2),
+                     b = __ldg(reinterpret_cast<const ulonglong2 *>(col) + r / 2 + 1);
+    v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+  }
+}
+
+template <int GS, int SW>
+__global__ void __launch_bounds__(256, 8)
 join_grpby_kernel(uint64_t nrows, const __grid_constant__ mb_op O, uint32_t nr_grp, uint32_t hcap,
                   uint32_t grp_bytes, uint32_t screen, uint32_t t0, unsigned long long *__restrict__ out,
                   unsigned long long *__restrict__ nqual) {
@@ -295,7 +317,7 @@ join_grpby_kernel(uint64_t nrows, const __grid_constant__ mb_op O, uint32_t nr_g
       cnt += kept ? 1u : 0u;
       aggregate<GS>(G, kept, grp, val, acc);
     }
-  } else {
+  } else if (SW == 0) {
     for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nchunks; ch += (uint64_t)gridDim.x * nw) {
       const uint64_t row = ch * 32 + lane;
       const bool pass = row < nrows && clause_pass(O, screen, t0, (uint32_t)row);
@@ -304,6 +326,34 @@ join_grpby_kernel(uint64_t nrows, const __grid_constant__ mb_op O, uint32_t nr_g
       qn += __popc(bal);  // at most 31 + 32 < JQ
       __syncwarp();
       if (qn >= 32) drain(32);
+    }
+    if (qn) drain(qn);
+  } else {
+    // the screen is one range on a fact column of SW-byte elements: four rows
+    // a lane from one vector load; 128-row chunks, the last one partly by
+    // scalar loads
+    const mb_term &tm = O.terms[t0];
+    const void *col = O.src[tm.src].col;
+    const uint64_t lo = tm.lo, hi = tm.hi, nch4 = (nrows + 127) / 128;
+    for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nch4; ch += (uint64_t)gridDim.x * nw) {
+      const uint64_t r = ch * 128 + 4 * lane;
+      uint64_t v[4] = {0, 0, 0, 0};
+      if (ch * 128 + 128 <= nrows) {
+        load4<SW>(col, r, v);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (r + j < nrows) v[j] = load_width(col, r + j, SW);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const bool pass = r + j < nrows && v[j] >= lo && v[j] < hi;
+        const uint32_t bal = __ballot_sync(0xffffffffu, pass);
+        if (pass) queue[qn + __popc(bal & lt)] = (uint32_t)(r + j);
+        qn += __popc(bal);  // at most 31 + 128 < JQ
+      }
+      __syncwarp();
+      while (qn >= 32) drain(32);
     }
     if (qn) drain(qn);
   }
@@ -609,14 +659,12 @@ static uint32_t screen_clause(const mb_op &O, uint32_t *t0) {
   return 0;
 }
 
-template <int GS>
-static mb_status launch_join(uint64_t n, const mb_op &O, uint32_t nr_grp, uint32_t hcap, int64_t *out,
-                             uint64_t *nqual, cudaStream_t st) {
-  auto kern = join_grpby_kernel<GS>;
+template <int GS, int SW>
+static mb_status launch_join_sw(uint64_t n, const mb_op &O, uint32_t nr_grp, uint32_t hcap, int64_t *out,
+                                uint64_t *nqual, cudaStream_t st, uint32_t screen, uint32_t t0) {
+  auto kern = join_grpby_kernel<GS, SW>;
   const uint32_t warps = 8;
   const size_t gb = (grp_smem_bytes(GS, nr_grp, hcap) + 15) & ~(size_t)15;
-  uint32_t t0 = 0;
-  uint32_t screen = screen_clause(O, &t0);
   // the row queues only where they cost no resident CTA (a large group
   // table in shared memory can leave no room for them)
   const size_t qbytes = (size_t)warps * JQ * 4;
@@ -637,6 +685,27 @@ static mb_status launch_join(uint64_t n, const mb_op &O, uint32_t nr_grp, uint32
                                            reinterpret_cast<unsigned long long *>(nqual));
   MB_LAUNCH_CHECK("join_grpby_kernel");
   return MB_OK;
+}
+
+// The screen's shape picks the kernel: one range on a 16-byte-aligned fact
+// column screens four rows a lane (its width a template argument).
+template <int GS>
+static mb_status launch_join(uint64_t n, const mb_op &O, uint32_t nr_grp, uint32_t hcap, int64_t *out,
+                             uint64_t *nqual, cudaStream_t st) {
+  uint32_t t0 = 0;
+  const uint32_t screen = screen_clause(O, &t0);
+  uint32_t sw = 0;
+  if (screen < O.nclause && O.clause_len[screen] == 1) {
+    const mb_src &s = O.src[O.terms[t0].src];
+    if (!s.fk && (reinterpret_cast<uintptr_t>(s.col) & 15) == 0) sw = s.width;
+  }
+  switch (sw) {
+  case 1: return launch_join_sw<GS, 1>(n, O, nr_grp, hcap, out, nqual, st, screen, t0);
+  case 2: return launch_join_sw<GS, 2>(n, O, nr_grp, hcap, out, nqual, st, screen, t0);
+  case 4: return launch_join_sw<GS, 4>(n, O, nr_grp, hcap, out, nqual, st, screen, t0);
+  case 8: return launch_join_sw<GS, 8>(n, O, nr_grp, hcap, out, nqual, st, screen, t0);
+  default: return launch_join_sw<GS, 0>(n, O, nr_grp, hcap, out, nqual, st, screen, t0);
+  }
 }
 
 extern "C" mb_status mb_join_grpby(uint64_t nrows, const mb_op *op, uint32_t nr_grp, int64_t *out,
