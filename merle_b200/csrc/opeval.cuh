@@ -97,11 +97,17 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x) {
   return x ^ (x >> 16);
 }
 
+// Group counts from which a lane adds its row straight into the table: the
+// 32 rows of a warp then rarely share a group, and finding peers first
+// (match + three reductions) costs more than the atomics it saves.
+constexpr uint32_t GRP_DIRECT_MIN = 256;
+
 // Per-CTA group-by state in shared memory.
 struct GrpCtx {
   unsigned long long *table;  // GS_SHARED: nr_grp sums; GS_HASH: hash sums
   uint32_t *keys;             // GS_HASH: keys (HASH_EMPTY = free)
   uint32_t hcap;              // GS_HASH: capacity (power of two)
+  bool direct;                // GS_SHARED / GS_GLOBAL: one atomic per row (nr_grp >= GRP_DIRECT_MIN)
   unsigned long long *gout;   // global output
 };
 
@@ -126,6 +132,10 @@ __device__ __forceinline__ void aggregate(const GrpCtx &G, bool kept, uint32_t g
                                           int64_t &acc) {
   if (GS == GS_SCALAR) {
     if (kept) acc += val;
+    return;
+  }
+  if ((GS == GS_SHARED || GS == GS_GLOBAL) && G.direct) {  // uniform over the warp
+    if (kept) atomicAdd(GS == GS_SHARED ? &G.table[grp] : &G.gout[grp], (unsigned long long)val);
     return;
   }
   const uint32_t key = kept ? grp : 0xffffffffu;
@@ -153,6 +163,7 @@ __device__ __forceinline__ GrpCtx grp_init(uint8_t *smem, uint32_t nr_grp, uint3
   GrpCtx G;
   G.gout = gout;
   G.hcap = hcap;
+  G.direct = nr_grp >= GRP_DIRECT_MIN;
   G.table = reinterpret_cast<unsigned long long *>(smem);
   G.keys = reinterpret_cast<uint32_t *>(smem + (size_t)hcap * 8);
   if (GS == GS_SHARED)
