@@ -179,6 +179,29 @@ def test_join_ssb13(stars, orc, cuda):
         assert int(host(nq, np.uint64)[0]) == nqw
 
 
+@pytest.mark.parametrize("width,n,offset", [(8, 100_003, 0), (4, 128 * 300 + 77, 0), (2, 4097, 0),
+                                            (1, 131, 0), (4, 50_001, 1)])
+def test_join_screen_widths_tails_alignment(orc, cuda, width, n, offset):
+    """The no-index scan's screen: one range on a fact column of each width
+    (four rows a lane from one vector load), row counts that end inside a
+    128-row chunk, and a column that is not 16-byte aligned (the per-row
+    screen); SUM(b * c) and the row count equal the oracle's."""
+    rng = np.random.default_rng(width * 1000 + n)
+    dt = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[width]
+    a_full = rng.integers(0, 200, n + offset).astype(dt)
+    b = rng.integers(0, 1000, n).astype(np.uint32)
+    c = rng.integers(0, 50, n).astype(np.uint32)
+    a = a_full[offset:]
+    def op(cols):
+        return ops.Op(srcs=[ops.Src(cols[0]), ops.Src(cols[1]), ops.Src(cols[2])],
+                      clauses=[[(0, 40, 90)], [(2, 5, 45)]], keys=[], vkind=abi.V_MUL, va=1, vb=2).to_c()
+    want, nqw = orc.join_grpby(n, op((np.ascontiguousarray(a), b, c)), 1)
+    da_full = D.from_host(a_full)
+    da = da_full[offset:] if offset else da_full
+    out, nq = D.join_grpby(n, op((da, D.from_host(b), D.from_host(c))), 1)
+    assert int(host(out, np.int64)[0]) == int(want[0]) and int(host(nq, np.uint64)[0]) == nqw
+
+
 def test_materialised_stages(stars, orc, mb, cuda):
     dev, ref = stars
     n = ref.n
