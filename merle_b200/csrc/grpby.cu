@@ -1196,6 +1196,9 @@ extern "C" mb_status mb_hash_join_grpby(uint64_t nrows, const mb_op *op, uint32_
     uint64_t off = 0, smem_tables = 0;
     uint64_t offs[HJ_MAXT];
     for (uint32_t t = 0; t < H.ntab; ++t) {
+      if (cnt[t] > (1ull << 30))
+        return fail(MB_ERR_UNSUPPORTED, "mb_hash_join_grpby: %llu dimension rows in one table (at most 2^30)",
+                    (unsigned long long)cnt[t]);
       uint64_t capt = 64;
       while (capt < 2 * cnt[t]) capt <<= 1;
       H.tab[t].mask = (uint32_t)(capt - 1);

@@ -777,7 +777,7 @@ extern "C" mb_status mb_wah_load(const char *path, uint32_t *words, uint64_t cap
   long size = -1;
   if (fread(&h, sizeof(h), 1, f) != 1) st = fail(MB_ERR_IO, "mb_wah_load: %s: short header", path);
   else if (h.magic != WAH_MAGIC) st = fail(MB_ERR_IO, "mb_wah_load: %s: bad magic 0x%08x", path, h.magic);
-  else if (fseek(f, 0, SEEK_END) != 0 || (size = ftell(f)) < 0 ||
+  else if (fseek(f, 0, SEEK_END) != 0 || (size = ftell(f)) < 0 || h.cmprs > ((uint64_t)size) / 4 ||
            (uint64_t)size != sizeof(h) + 4 * h.cmprs)
     st = fail(MB_ERR_IO, "mb_wah_load: %s: %ld bytes for %llu words", path, size, (unsigned long long)h.cmprs);
   if (st == MB_OK) {
