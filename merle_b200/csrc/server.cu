@@ -167,6 +167,7 @@ struct mb_server {
   void complete(Launch *L);
   void finish(Request *r, int32_t status);
   uint64_t footprint(const mb_query &q, uint32_t *plan_idx, mb_plan *plan);
+  uint64_t inter_bytes(const mb_query &q, const mb_plan &plan);
 };
 
 // Bytes a request reserves: its group table and row count in the arena, and
@@ -186,19 +187,26 @@ uint64_t mb_server::footprint(const mb_query &q, uint32_t *plan_idx, mb_plan *pl
       *plan_idx = 0;
     }
   }
+  return table + inter_bytes(q, *plan);
+}
+
+// Intermediate bitmap bytes a plan writes: a (certain, uncertain) pair per
+// materialised predicate; the materialised plan's result pair and row list.
+uint64_t mb_server::inter_bytes(const mb_query &q, const mb_plan &plan) {
+  Engine &E = eng->E;
   const uint64_t W = E.stride * 4;
   uint64_t inter = 0;
-  if (plan->kind == MB_PLAN_MATERIALISED) inter = 2 * W + (E.nrows + 1) * 4;
-  if (plan->materialise && plan->kind == MB_PLAN_FUSED) {
+  if (plan.kind == MB_PLAN_MATERIALISED) inter = 2 * W + (E.nrows + 1) * 4;
+  if (plan.materialise && plan.kind == MB_PLAN_FUSED) {
     Lowered L;
-    if (lower_query(E, q, *plan, L) == MB_OK) {
+    if (lower_query(E, q, plan, L) == MB_OK) {
       uint32_t nmat = 0;
       for (uint32_t c = 0; c < L.prg.ncols; ++c)
-        if (plan->materialise & (1u << L.col_pred[c])) ++nmat;
+        if (plan.materialise & (1u << L.col_pred[c])) ++nmat;
       inter = 2ull * nmat * W;
     }
   }
-  return table + inter;
+  return inter;
 }
 
 void mb_server::finish(Request *r, int32_t status) {
@@ -366,6 +374,11 @@ bool mb_server::launch_some(std::unique_lock<std::mutex> &lk) {
   }
   const bool learned = learn && (take[0]->planned || ahead_ok);
   const mb_plan *lplan = take[0]->planned ? &take[0]->plan : ahead_ok ? &ahead_plans[0] : nullptr;
+  // intermediate bytes of the plans just made (take[0]'s, if planned here, is
+  // extra[0]; one planned ahead earlier already carries its own in its foot)
+  std::vector<uint64_t> extra(std::max<size_t>(1, ahead.size()), 0);
+  if (ahead_ok)
+    for (size_t i = 0; i < ahead.size(); ++i) extra[i] = inter_bytes(ahead[i]->q, ahead_plans[i]);
   if (learn) take[0]->info.plan = take[0]->planned ? take[0]->info.plan : ahead_ok ? ahead_pick[0] : 0;
   mb_status s = MB_OK;
   if (f_a) s = fail(MB_ERR_OOM, "serving: injected arena allocation failure");
@@ -382,10 +395,21 @@ bool mb_server::launch_some(std::unique_lock<std::mutex> &lk) {
     s = fail(MB_ERR_CUDA, "serving: error word copy");
   cudaEventRecord(L->ev1, st);
   lk.lock();
+  // a learned plan may write intermediate bitmaps: the queued requests
+  // planned ahead reserve them when they are admitted; the launched one adds
+  // them to its launch's reservation now
   for (size_t i = 0; i < ahead.size(); ++i) {
     Request *r = ahead[i];
     r->planning = false;
-    if (ahead_ok) r->plan = ahead_plans[i], r->info.plan = ahead_pick[i], r->planned = true;
+    if (ahead_ok) {
+      r->plan = ahead_plans[i], r->info.plan = ahead_pick[i], r->planned = true;
+      if (i > 0) r->foot += extra[i];
+    }
+  }
+  if (learned && extra[0]) {
+    L->reserved += extra[0];
+    reserved += extra[0];
+    if (reserved > stats.peak_reserved) stats.peak_reserved = reserved;
   }
   L->st = s;
   return true;
