@@ -1044,10 +1044,10 @@ __device__ __forceinline__ bool hj_row(const mb_op &O, const HjPlan &H, const ui
   return true;
 }
 
-template <int GS>
-__global__ void __launch_bounds__(512)
+template <int GS, int SW>
+__global__ void __launch_bounds__(SW ? 256 : 512, SW ? 4 : 1)
 hj_probe_kernel(uint64_t nrows, const __grid_constant__ mb_op O, const __grid_constant__ HjPlan H, uint32_t nr_grp,
-                uint32_t hcap, uint32_t grp_bytes, unsigned long long *__restrict__ out,
+                uint32_t hcap, uint32_t grp_bytes, uint32_t t0, unsigned long long *__restrict__ out,
                 unsigned long long *__restrict__ nqual) {
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ uint64_t red[64];
@@ -1084,30 +1084,86 @@ hj_probe_kernel(uint64_t nrows, const __grid_constant__ mb_op O, const __grid_co
     qn -= m;
     __syncwarp();
   };
-  const uint64_t nchunks = (nrows + 31) / 32;
-  for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nchunks; ch += (uint64_t)gridDim.x * nw) {
-    const uint64_t row = ch * 32 + lane;
-    const bool pass = row < nrows && hj_clauses(O, H, H.fact_clauses, (uint32_t)row, nullptr);
-    const uint32_t bal = __ballot_sync(0xffffffffu, pass);
-    if (pass) queue[qn + __popc(bal & lt)] = (uint32_t)row;
-    qn += __popc(bal);
-    __syncwarp();
-    if (qn >= 32) drain(32);
+  if (SW == 0) {
+    const uint64_t nchunks = (nrows + 31) / 32;
+    for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nchunks; ch += (uint64_t)gridDim.x * nw) {
+      const uint64_t row = ch * 32 + lane;
+      const bool pass = row < nrows && hj_clauses(O, H, H.fact_clauses, (uint32_t)row, nullptr);
+      const uint32_t bal = __ballot_sync(0xffffffffu, pass);
+      if (pass) queue[qn + __popc(bal & lt)] = (uint32_t)row;
+      qn += __popc(bal);
+      __syncwarp();
+      if (qn >= 32) drain(32);
+    }
+  } else {
+    // the fact clauses are one range on an aligned column: four rows a lane
+    // from one vector load, as the no-index scan screens
+    const mb_term &tm = O.terms[t0];
+    const void *col = O.src[tm.src].col;
+    const uint64_t lo = tm.lo, hi = tm.hi, nch4 = (nrows + 127) / 128;
+    for (uint64_t ch = (uint64_t)blockIdx.x * nw + warp; ch < nch4; ch += (uint64_t)gridDim.x * nw) {
+      const uint64_t r = ch * 128 + 4 * lane;
+      uint64_t v[4] = {0, 0, 0, 0};
+      if (ch * 128 + 128 <= nrows) {
+        load4<SW>(col, r, v);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (r + j < nrows) v[j] = load_width(col, r + j, SW);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const bool pass = r + j < nrows && v[j] >= lo && v[j] < hi;
+        const uint32_t bal = __ballot_sync(0xffffffffu, pass);
+        if (pass) queue[qn + __popc(bal & lt)] = (uint32_t)(r + j);
+        qn += __popc(bal);  // at most 31 + 128 < JQ
+      }
+      __syncwarp();
+      while (qn >= 32) drain(32);
+    }
   }
   if (qn) drain(qn);
   __syncthreads();
   grp_flush<GS>(G, nr_grp, acc, cnt, nqual, red);
 }
 
+template <int GS, int SW>
+static mb_status launch_hj_sw(uint64_t n, const mb_op &O, const HjPlan &H, uint32_t smem_tables, uint32_t nr_grp,
+                              int64_t *out, uint64_t *nqual, cudaStream_t st, uint32_t t0);
+
+// The probe's screen shape picks the kernel: the fact clauses one range on a
+// 16-byte-aligned fact column screen four rows a lane.
 template <int GS>
 static mb_status launch_hj(uint64_t n, const mb_op &O, const HjPlan &H, uint32_t smem_tables, uint32_t nr_grp,
                            int64_t *out, uint64_t *nqual, cudaStream_t st) {
-  auto kern = hj_probe_kernel<GS>;
+  uint32_t sw = 0, t0 = 0;
+  const uint32_t fc = H.fact_clauses;
+  if (fc && !(fc & (fc - 1))) {
+    const uint32_t c = (uint32_t)__builtin_ctz(fc);
+    if (O.clause_len[c] == 1) {
+      t0 = H.term0[c];
+      const mb_src &s = O.src[O.terms[t0].src];
+      if (!s.fk && (reinterpret_cast<uintptr_t>(s.col) & 15) == 0) sw = s.width;
+    }
+  }
+  switch (sw) {
+  case 1: return launch_hj_sw<GS, 1>(n, O, H, smem_tables, nr_grp, out, nqual, st, t0);
+  case 2: return launch_hj_sw<GS, 2>(n, O, H, smem_tables, nr_grp, out, nqual, st, t0);
+  case 4: return launch_hj_sw<GS, 4>(n, O, H, smem_tables, nr_grp, out, nqual, st, t0);
+  case 8: return launch_hj_sw<GS, 8>(n, O, H, smem_tables, nr_grp, out, nqual, st, t0);
+  default: return launch_hj_sw<GS, 0>(n, O, H, smem_tables, nr_grp, out, nqual, st, t0);
+  }
+}
+
+template <int GS, int SW>
+static mb_status launch_hj_sw(uint64_t n, const mb_op &O, const HjPlan &H, uint32_t smem_tables, uint32_t nr_grp,
+                              int64_t *out, uint64_t *nqual, cudaStream_t st, uint32_t t0) {
+  auto kern = hj_probe_kernel<GS, SW>;
   const uint32_t warps = 8;
   const size_t grp_bytes = (grp_smem_bytes(GS, nr_grp, DEFAULT_HCAP) + 15) & ~(size_t)15;
   LaunchShape ls;
   MB_CHECK(shape_for(kern, warps, grp_bytes + smem_tables + (size_t)warps * JQ * 4, (n + 31) / 32, &ls, 0));
-  kern<<<ls.grid, ls.block, ls.smem, st>>>(n, O, H, nr_grp, DEFAULT_HCAP, (uint32_t)grp_bytes,
+  kern<<<ls.grid, ls.block, ls.smem, st>>>(n, O, H, nr_grp, DEFAULT_HCAP, (uint32_t)grp_bytes, t0,
                                            reinterpret_cast<unsigned long long *>(out),
                                            reinterpret_cast<unsigned long long *>(nqual));
   MB_LAUNCH_CHECK("hj_probe_kernel");
