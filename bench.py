@@ -1,18 +1,19 @@
 #!/usr/bin/env python
 """bench.py - fact rows/s of the fused bitmap-index query path on B200.
 
-Workload (one GPU): the synthetic star schema at k=20 (120,000,000 fact rows,
-every fact column 4 bytes), its canonical 242-bitmap index resident in HBM,
-and a seeded 64-query mix of the four templates (s1op..s4op of the
-reference).  One step runs the 64 queries; fact rows/s = rows x queries /
-device time.  With N GPUs every rank holds its own 120M-row shard of an
-N x 120M-row table (weak scaling) and each step ends with one NCCL all-reduce
+Workload (one GPU): the synthetic star schema at k=100 (600,000,000 fact
+rows, every fact column 4 bytes), its canonical 242-bitmap index resident in
+HBM, and a seeded 64-query mix of the four templates (s1op..s4op of the
+reference) whose selectivities are spread log-uniformly over [1e-6, 0.5]
+(workload.span_mix).  One step answers the 64 queries; fact rows/s = rows x
+queries / device time.  With N GPUs every rank holds its own row shard of an
+N x 600M-row table (weak scaling) and each step ends with one NCCL all-reduce
 of the int64 group tables (the only exchange step of a sharded query).
 
   value     device-resident: one step = the 64 queries in one batched
-            launch (mb_engine_enqueue_batch), results in HBM, CUDA events on
-            the engine stream around the timed steps; "plain" beside it times
-            the same queries one fused launch each
+            launch, results in HBM, CUDA events on the engine stream around
+            the timed steps; "plain" beside it times the same queries one
+            fused launch each
   e2e       through the public C ABI (mb_engine_query_batch): query
             descriptors from host memory, int64 results read back to host
             every step, host wall clock
@@ -20,11 +21,19 @@ of the int64 group tables (the only exchange step of a sharded query).
             bitmap once + the union of the 32-byte payload sectors holding a
             selected row + outputs, computed by the oracle on a host row
             sample) / the event-timed step
-  cpu_baseline  the reference's own CPU oracle (ssb/cpuref.c s1ref..s4ref,
-            built from its sources into oracle/_ref) on a 24M-row sample, one
-            query per thread over all host cores (the ssb_cpujoin shape)
+  parity    every query's answer against the reference's own s1ref..s4ref
+            (ssb/cpuref.c, built from its sources into oracle/_ref) over the
+            whole table on the host: uint32 group arrays equal (uint32) of the
+            int64 sums, s1ref's uint64 sum equal; row counts give the realised
+            selectivities
+  cpu_baseline  that same pass of s1ref..s4ref, timed: one query per thread
+            over all host cores (the ssb_cpujoin shape)
+  latency_ms  the serving loop (mb_server_*) under seeded Poisson arrivals at
+            two rates, below and above the plain server's capacity, batched
+            and plain servers: q/s, p50, p99 over every request
 
-`--impl reference` times that reference CPU path alone (rank 0 only).
+`--impl reference` times the reference CPU path alone (rank 0 only) on a
+bounded row sample.
 """
 from __future__ import annotations
 
@@ -49,6 +58,7 @@ METRIC = "fact rows/s + %HBM roofline, learned+batched vs plain plan; p50/p99 la
 UNIT = "fact rows/s"
 SEED_DATA, SEED_QUERIES = 2, 3
 CPU_SAMPLE_ROWS = 24_000_000
+PEAK_FALLBACK_GBS = 6650.0
 
 
 def parse():
@@ -57,13 +67,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--k", type=int, default=20)
+    ap.add_argument("--k", type=int, default=100)
     ap.add_argument("--rows", type=int, default=0, help="rows per GPU (default 6M x k)")
     ap.add_argument("--queries", type=int, default=64)
-    ap.add_argument("--narrow", type=float, default=0.3)
+    ap.add_argument("--mix", default="span", choices=["span", "random"],
+                    help="span: selectivities log-uniform over [1e-6, 0.5]; random: the older level-based mix")
+    ap.add_argument("--narrow", type=float, default=0.3, help="(random mix) share of city/brand/week constants")
     ap.add_argument("--width4", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the host parity pass and the CPU baseline")
+    ap.add_argument("--serve-requests", type=int, default=1024, help="requests per serving run (0: no serving leg)")
     ap.add_argument("--no-tune", action="store_true", help="default launch shape instead of the autotuner's")
     ap.add_argument("--no-graph", action="store_true", help="enqueue each step instead of replaying a CUDA graph")
     ap.add_argument("--wah", action="store_true",
@@ -121,74 +134,78 @@ class Clocks:
 
 
 # ------------------------------------------------------- reference (CPU)
-def cpu_sample(k: int, nrows: int):
+def mix_of(args):
+    from merle_b200 import workload as WL
+    if args.mix == "span":
+        return WL.span_mix(SEED_QUERIES, args.queries)
+    return WL.random_mix(SEED_QUERIES, args.queries, args.narrow)
+
+
+def host_table(k: int, nrows: int):
+    """The star table generated on the host by the oracle's generator (the
+    same seeded counter-based columns the engine generates on the device), in
+    the reference's ssb_schema widths, or None if host memory is short."""
     from oracle import oracle as O
+    need = nrows * 29 + (1 << 30)  # narrow fact columns + dimensions + slack
+    try:
+        import psutil
+        if psutil.virtual_memory().available < need * 1.2:
+            return None
+    except ImportError:
+        pass
     return O.StarHost(SEED_DATA, k, nrows)
 
 
-def run_cpuref(ref, schema, n, qs, threads) -> float:
-    """One pass of the query mix through the reference's s1ref..s4ref, one
-    query per thread (ssb_cpujoin's shape, ssb/cpuref.c:244-302).  Seconds."""
-    import merle_b200
-    from merle_b200 import workload as WL
-
-    def one(q):
-        t, p = WL.as_tuple(q)
-        ng = int(max(1, merle_b200.lib().mb_query_ngroups(C.byref(q))))
-        out = np.zeros(ng + 1, np.uint32)
-        if t == 1:
-            ref.s1ref(C.byref(schema), n, *p)
-        elif t == 2:
-            ref.s2ref(C.byref(schema), n, *p, out.ctypes.data)
-        elif t == 3:
-            ref.s3ref(C.byref(schema), n, *p, out.ctypes.data)
-        else:
-            ref.s4ref(C.byref(schema), n, *p, out.ctypes.data)
-        return out
-    t0 = time.perf_counter()
-    with ThreadPoolExecutor(threads) as ex:
-        list(ex.map(one, qs))
-    return time.perf_counter() - t0
-
-
-def cpu_baseline(args, qs, steps: int = 1) -> dict:
+def reference_pass(star, nrows: int, qs, threads: int):
+    """The reference's s1ref..s4ref over the first nrows rows (one query per
+    thread): (answers, seconds)."""
     from oracle import oracle as O
-    ref = O.ref()
-    if ref is None:
-        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                "sample": "unavailable: oracle/_ref not built"}
-    n = min(CPU_SAMPLE_ROWS, args.rows or 6_000_000 * args.k)
-    star = cpu_sample(args.k, n)
     schema = star.ssb_schema()
-    threads = os.cpu_count() or 1
-    run_cpuref(ref, schema, n, qs[:4], threads)  # warm the pages
-    ts = [run_cpuref(ref, schema, n, qs, threads) for _ in range(steps)]
-    sec = float(np.median(ts))
-    return {"value": n * len(qs) / sec, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"the {len(qs)}-query mix over the first {n:,} rows of the k={args.k} table in ssb_schema "
-                      f"widths, reference s1ref..s4ref, one query per thread on {threads} threads",
-            "seconds_per_pass": sec}
+    return O.ref_answers(schema, nrows, qs, threads)
+
+
+def parity_check(qs, answers, out_host: np.ndarray, offs, nq: np.ndarray, nrows: int) -> dict:
+    """Our int64 group sums against the reference's answers: (uint32) of
+    every group sum equals its uint32 array, s1ref's uint64 sum equals ours
+    (as uint64).  Row counts give each query's realised selectivity."""
+    bad = []
+    for i, (q, ref_ans) in enumerate(zip(qs, answers)):
+        mine = out_host[offs[i]:offs[i] + len(ref_ans)]
+        if int(q.tmpl) == 1:
+            ok = int(mine[0]) % (1 << 64) == int(ref_ans[0])
+        else:
+            ok = np.array_equal(mine.astype(np.uint64).astype(np.uint32), ref_ans)
+        if not ok:
+            bad.append(i)
+    sel = nq.astype(np.float64) / nrows
+    return {"reference_equal": not bad, "queries": len(qs), "mismatched": bad,
+            "groups_compared": int(sum(len(a) for a in answers)),
+            "against": "reference ssb/cpuref.c s1ref..s4ref over every row of the timed table "
+                       "((uint32) of the int64 group sums; s1ref's uint64 sum)",
+            "selectivity": {"min": float(sel.min()), "median": float(np.median(sel)), "max": float(sel.max()),
+                            "per_query": [float(x) for x in sel]},
+            "selected_rows_per_step": int(nq.sum())}
 
 
 def reference_arm(args):
-    from merle_b200 import workload as WL
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    qs = WL.random_mix(SEED_QUERIES, args.queries, args.narrow)
+    qs = mix_of(args)
     from oracle import oracle as O
-    ref = O.ref()
-    if ref is None:
+    if O.ref() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's cpuref.c built from "
                           "its sources) is missing"}))
         return
     n = min(CPU_SAMPLE_ROWS, args.rows or 6_000_000 * args.k)
-    star = cpu_sample(args.k, n)
-    schema = star.ssb_schema()
+    star = host_table(args.k, n)
+    if star is None:
+        print(json.dumps({"impl": "reference", "unavailable": "host memory too small for the row sample"}))
+        return
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
-        run_cpuref(ref, schema, n, qs, threads)
-    ts = [run_cpuref(ref, schema, n, qs, threads) for _ in range(args.steps)]
+        reference_pass(star, n, qs, threads)
+    ts = [reference_pass(star, n, qs, threads)[1] for _ in range(args.steps)]
     tot = sum(ts)
     v = n * len(qs) * args.steps / tot
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
@@ -196,18 +213,20 @@ def reference_arm(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic", "config": config_of(args, args.rows or 6_000_000 * args.k),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                             "sample": f"{len(qs)}-query mix over the first {n:,} rows (ssb_schema widths), "
-                                       f"one query per thread"},
+                             "sample": f"each step: the {len(qs)}-query mix over the first {n:,} rows of the "
+                                       f"table (ssb_schema widths), one query per thread"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
 def config_of(args, nrows_per_gpu):
+    mix = ("selectivities log-uniform over [1e-6, 0.5] (workload.span_mix)" if args.mix == "span"
+           else f"level-based constants, {args.narrow:.0%} city/brand/week level")
     return {"workload": f"star schema k={args.k}, {nrows_per_gpu:,} fact rows per GPU "
                         f"({'4-byte' if args.width4 else 'ssb_schema-width'} fact columns), 242-bitmap index, "
-                        f"{args.queries}-query seeded mix of 4 templates",
-            "rows_per_gpu": nrows_per_gpu, "queries_per_step": args.queries, "k": args.k,
-            "l2": "inputs larger than L2 (each step reads several GB of bitmaps and payload)",
+                        f"{args.queries}-query seeded mix of 4 templates, {mix}",
+            "rows_per_gpu": nrows_per_gpu, "queries_per_step": args.queries, "k": args.k, "mix": args.mix,
+            "l2": "inputs larger than L2 (each step reads tens of GB of bitmaps and payload)",
             "parallelism": f"row shards x{args.gpus}"}
 
 
@@ -224,7 +243,7 @@ BATCH_GATHER = {1: [("extendedprice", 4), ("discount", 4)],
 BATCH_HDR_BYTES = 256 + 16 * 24 + 128 * 64 * 4 + 4096 * 2 + 128
 
 
-def batch_algo_bytes(star, scale: float, nrows: int, qs, ngroups) -> dict:
+def batch_algo_bytes(star, scale: float, nrows: int, qs, ngroups, sample_n: int) -> dict:
     """Algorithmic bytes of one batched pass: every DISTINCT canonical bitmap
     once, the union over the queries of the 32-byte payload sectors holding a
     selected row (counted on the host sample, scaled), the int64 outputs."""
@@ -237,7 +256,7 @@ def batch_algo_bytes(star, scale: float, nrows: int, qs, ngroups) -> dict:
     for q in qs:
         t, p = WL.as_tuple(q)
         bins |= O.canonical_bins(t, p)
-        r = np.flatnonzero(O.qualifying_mask(star, t, p))
+        r = np.flatnonzero(O.qualifying_mask(star, t, p, sample_n))
         rows += len(r)
         for col, w in BATCH_GATHER[t]:
             sectors.setdefault((col, w), []).append(r // (32 // w))
@@ -339,11 +358,13 @@ def main():
     eng.gen_star(SEED_DATA, args.k, n, width4=bool(args.width4), row0=row0)
     eng.build_index()
     info = eng.info()
-    qs = WL.random_mix(SEED_QUERIES, args.queries, args.narrow)
+    qs = mix_of(args)
     Q = len(qs)
     qarr = (abi.mb_query * Q)(*qs)
     ngroups = [Engine.ngroups(q) for q in qs]
-    total_g = int(L.mb_queries_layout(qarr, Q, None))
+    offs_c = (C.c_uint64 * Q)()
+    total_g = int(L.mb_queries_layout(qarr, Q, offs_c))
+    offs = [int(x) for x in offs_c]
     out = torch.zeros(total_g, dtype=torch.int64, device="cuda")
     nq = torch.zeros(Q, dtype=torch.int64, device="cuda")
     ext = torch.cuda.ExternalStream(int(L.mb_engine_stream(eng.handle) or 0))
@@ -363,6 +384,12 @@ def main():
         check(L.mb_engine_tune_batch(eng.handle, qarr, Q, 3, C.byref(bopts), C.byref(tms), C.byref(tried)))
         tune = {"tuned": True, "shapes_timed": tried.value, "best_ms": tms.value, "tune_s": time.perf_counter() - t0,
                 "opts": {f: getattr(bopts, f) for f, _ in bopts._fields_ if f != "pad_"}}
+    binfo = (abi.mb_batch_launch_info * 16)()
+    nlaunch, nalone = C.c_uint32(0), C.c_uint32(0)
+    check(L.mb_engine_batch_info(eng.handle, qarr, Q, C.byref(bopts), binfo, 16, C.byref(nlaunch), C.byref(nalone)))
+    tune["launches"] = [{f: getattr(binfo[i], f) for f, _ in binfo[i]._fields_ if f != "pad_"}
+                        for i in range(nlaunch.value)]
+    tune["queries_alone"] = nalone.value
     graph = C.c_void_p()
     if not args.no_graph:
         check(L.mb_batch_graph_create(eng.handle, qarr, Q, C.byref(bopts), out.data_ptr(), nq.data_ptr(),
@@ -399,6 +426,7 @@ def main():
         step_batch()
     check(L.mb_engine_sync(eng.handle, None, 0))
     batch_out = out.clone()
+    batch_nq = nq.clone()
     if world > 1:
         dist.barrier()
     with Clocks(local) as clk:
@@ -410,7 +438,7 @@ def main():
     for _ in range(args.warmup):
         step_plain()
     check(L.mb_engine_sync(eng.handle, None, 0))
-    same = bool(torch.equal(out, batch_out))
+    same = bool(torch.equal(out, batch_out)) and bool(torch.equal(nq, batch_nq))
     if world > 1:
         dist.barrier()
     plain_ms = timed(step_plain, args.steps, 2, 3)
@@ -425,17 +453,11 @@ def main():
     check(L.mb_engine_query_batch(eng.handle, qarr, Q, C.byref(bopts), res_host.ctypes.data, nq_host.ctypes.data))
     if world > 1:
         dist.barrier()
-    lat = []
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        t1 = time.perf_counter()
-        check(L.mb_engine_mark(eng.handle, 4))
         check(L.mb_engine_query_batch(eng.handle, qarr, Q, C.byref(bopts), res_host.ctypes.data,
                                       nq_host.ctypes.data))
-        check(L.mb_engine_mark(eng.handle, 5))
-        lat.append((time.perf_counter() - t1) * 1e3)
-    e2e_wall = time.perf_counter() - t0
-    e2e_ms = float(e2e_wall * 1e3)
+    e2e_ms = float((time.perf_counter() - t0) * 1e3)
     if world > 1:
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -446,6 +468,12 @@ def main():
            "api": "mb_engine_query_batch (host query descriptors in, host int64 group sums and row counts out, "
                   "returns when they are on the host)",
            "timing": "host wall clock around each call", "ms_per_step": e2e_ms / args.e2e_steps}
+    e2e_same = bool(np.array_equal(res_host, batch_out.cpu().numpy())) if world == 1 else None
+
+    # ---- serving: Poisson arrivals through the batched and the plain server
+    serving = None
+    if args.serve_requests and world == 1:
+        serving = serve_leg(eng, args, bopts, float(qtimes.mean()))
 
     line = None
     if rank == 0:
@@ -454,15 +482,33 @@ def main():
         pk = ROOT / "MEASURED_PEAKS.json"
         if pk.exists():
             peaks = json.loads(pk.read_text())
-        peak = float(peaks.get("hbm_gbs", 6650.0))
+        peak = float(peaks.get("hbm_gbs", PEAK_FALLBACK_GBS))
+        peak_src = ("MEASURED_PEAKS.json hbm_gbs (burst copy), of measured" if peaks
+                    else f"fallback {PEAK_FALLBACK_GBS / 1000:.2f} TB/s")
+        # parity and the CPU baseline: the reference's cpuref over the whole
+        # table, generated on the host by the oracle
+        parity, cpu, star = None, None, None
+        if not args.no_cpu and world == 1:
+            star = host_table(args.k, n)
+            if star is None:
+                parity = {"reference_equal": None, "skipped": "host memory too small for the full table"}
+            else:
+                threads = os.cpu_count() or 1
+                answers, sec = reference_pass(star, n, qs, threads)
+                parity = parity_check(qs, answers, batch_out.cpu().numpy(), offs,
+                                      batch_nq.cpu().numpy().astype(np.uint64), n)
+                cpu = {"value": n * Q / sec, "unit": UNIT, "cores": threads, "kind": "reference",
+                       "sample": f"one pass of the {Q}-query mix over all {n:,} rows of the table in ssb_schema "
+                                 f"widths (the reference's s1ref..s4ref, one query per thread on {threads} "
+                                 f"threads); the same pass is the parity check", "seconds_per_pass": sec}
         sample_n = min(CPU_SAMPLE_ROWS, n)
-        star = cpu_sample(args.k, sample_n)
-        ab = batch_algo_bytes(star, n / sample_n, n, qs, ngroups)
+        if star is None:
+            star = O.StarHost(SEED_DATA, args.k, sample_n)
+        ab = batch_algo_bytes(star, n / sample_n, n, qs, ngroups, sample_n)
         step_s = ms_total / args.steps / 1e3
         achieved = ab["total"] / step_s / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy), of measured" if peaks
-                               else "fallback 6.65 TB/s",
+                "peak_source": peak_src,
                 "kernel": "batch_scan_kernel (one launch per 64-query step)",
                 "algo_bytes_per_launch": ab["total"], "algo_bytes_detail": ab,
                 "launch_ms_avg": ms_total / args.steps,
@@ -470,16 +516,16 @@ def main():
         tj = ROOT / "profiles" / "traffic.json"
         if tj.exists():
             t = json.loads(tj.read_text()).get("batch_scan_kernel")
-            if t:
+            if t and t.get("mix") == args.mix:
                 roof["traffic"] = t["dram_bytes_per_row"] * n
-                roof["traffic_note"] = "ncu capture of a 24M-row launch scaled to this launch's rows: " + t["source"]
+                roof["traffic_note"] = ("ncu capture of a smaller launch of the same mix scaled to this launch's "
+                                        "rows: " + t["source"])
         widths = {c: (4 if args.width4 else {"orderdate": 2, "discount": 1, "quantity": 1, "suppcity": 1}.get(c, 4))
                   for c in ["extendedprice", "discount", "partkey", "orderdate", "revenue", "custkey", "suppcity",
                             "supplycost", "quantity"]}
-        plain_algo = sum(O.algo_bytes(star, n / sample_n, n, *WL.as_tuple(q), Engine.ngroups(q), widths)["total"]
-                         for q in qs)
-        cpu = None if args.no_cpu or world > 1 else cpu_baseline(args, qs)
-        lat_a = np.array(lat)
+        plain_algo = sum(O.algo_bytes(star, n / sample_n, n, *WL.as_tuple(q), Engine.ngroups(q), widths,
+                                      sample_n)["total"] for q in qs)
+        build_bytes = index_build_bytes(n, info, args.width4)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
@@ -487,20 +533,21 @@ def main():
                 "plan": "batched: the whole mix in one persistent launch per step (rule-planner covers)"
                         + ("; replayed as a CUDA graph" if graph else ""),
                 "batch_shape": tune,
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "parity": parity,
                 "plain": {"value": rows_total * Q * args.steps / (plain_ms / 1e3), "ms_per_step": plain_ms / args.steps,
                           "batched_speedup": plain_ms / ms_total, "results_identical": same,
+                          "e2e_results_identical": e2e_same,
                           "roofline_frac": plain_algo / (qtimes.sum() / 1e3) / 1e9 / peak,
                           "plan": "one fused launch per query (rule planner)"},
-                "latency_ms": {"batch_e2e_p50": float(np.percentile(lat_a, 50)),
-                               "batch_e2e_p99": float(np.percentile(lat_a, 99)),
-                               "plain_kernel_p50": float(np.percentile(qtimes, 50)),
-                               "plain_kernel_p99": float(np.percentile(qtimes, 99))},
-                "gpu_launches": args.steps,
+                "latency_ms": serving,
+                "gpu_launches": args.steps * (nlaunch.value + nalone.value),
                 "clocks": clk.summary(),
                 "index": {"bitmaps": info["nbitmaps"], "bytes": info["index_bytes"],
-                          "build_ms": info["index_build_ms"], "denorm_bytes": info["denorm_bytes"]},
-                "selected_rows_per_step": ab["rows"]}
+                          "build_ms": info["index_build_ms"], "denorm_bytes": info["denorm_bytes"],
+                          "algo_bytes": build_bytes,
+                          "achieved_gbs": build_bytes / (info["index_build_ms"] / 1e3) / 1e9,
+                          "frac": build_bytes / (info["index_build_ms"] / 1e3) / 1e9 / peak},
+                "selected_rows_per_step": int(batch_nq.sum().item())}
         print(json.dumps(line))
     if graph:
         check(L.mb_batch_graph_destroy(graph))
@@ -508,6 +555,38 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def index_build_bytes(n: int, info: dict, width4: int) -> int:
+    """Algorithmic bytes of the index build: each indexed column read once
+    (the date, discount, quantity and supplier city columns; the customer
+    and part foreign keys plus their dimension arrays for the customer city
+    and part mfgr levels) and every bitmap written once."""
+    w = 4 if width4 else None
+    k = max(1, info["k"])
+    from oracle import oracle as O
+    col = (w or 2) * n + (w or 1) * n + (w or 1) * n + (w or 1) * n  # date, discount, quantity, suppcity
+    fk = 4 * n * 2 + (30000 * k + 1) * 1 + (O.star_npart(k) + 1) * 2
+    bm = info["nbitmaps"] * ((n + 31) // 32) * 4
+    return int(col + fk + bm)
+
+
+def serve_leg(eng, args, bopts, plain_query_ms: float) -> dict:
+    """Seeded Poisson arrivals of a selectivity-spanning mix through the
+    batched and the plain server, at half and at twice the plain path's
+    capacity (1 / mean plain query time): q/s, p50 and p99 latency over every
+    request of each run."""
+    from merle_b200 import serving as S, workload as WL
+    base = WL.span_mix(SEED_QUERIES + 2, 256) if args.mix == "span" else WL.random_mix(SEED_QUERIES + 2, 256)
+    qs = (base * ((args.serve_requests + len(base) - 1) // len(base)))[:args.serve_requests]
+    cap = 1e3 / max(plain_query_ms, 1e-3)
+    rates = [0.5 * cap, 2.0 * cap]
+    recs = S.sweep(eng, qs, rates, ("batched", "plain"), batch=bopts)
+    keep = ("mode", "offered_qps", "requests", "ok", "qps", "p50_ms", "p99_ms", "mean_ms", "max_ms", "mean_batch",
+            "launches", "statuses", "wall_s")
+    return {"plain_capacity_qps": cap, "runs": [{k: r[k] for k in keep} for r in recs],
+            "note": "request latency submit -> result on the host, every request of each run "
+                    f"({args.serve_requests} per run), seeded Poisson arrivals"}
 
 
 if __name__ == "__main__":

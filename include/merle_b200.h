@@ -220,6 +220,28 @@ MB_API mb_status mb_bitmap_create(const mb_src *src, uint64_t nrows, const uint6
                            const uint64_t *hi, uint32_t nbins, uint32_t *out,
                            uint64_t stride_words, uint64_t *popcounts, void *stream);
 
+/* Several levels of bins from ONE pass over a column (a hierarchy such as the
+ * years and months of a date, or the regions and nations of a city).  The
+ * reference builds every level with its own create_bin pass
+ * (bmpidx_create.cu:14-56, driven per level by ssb/bmpidx-create.cu:56-116);
+ * here each row's bin in every level comes from one lookup, so the column is
+ * read once.  Level l writes levels[l].nbins bitmaps (bin j = [lo[j], hi[j]))
+ * to levels[l].out, `stride_words` apart, and accumulates their popcounts
+ * into levels[l].popcounts (device uint64[nbins], or NULL).  src, nrows and
+ * the stride as for mb_bitmap_create.  Levels with overlapping or unsorted
+ * bins, 255 bins or more, or a value domain too wide for the one-pass lookup
+ * run one mb_bitmap_create pass per level instead (same results). */
+#define MB_MAXLEVELS 4
+typedef struct mb_level {
+  const uint64_t *lo, *hi; /* host: nbins bounds each */
+  uint32_t nbins;
+  uint32_t pad_;
+  uint32_t *out;           /* device: nbins bitmaps, 16-byte aligned */
+  uint64_t *popcounts;     /* device: nbins (accumulated), or NULL */
+} mb_level;
+MB_API mb_status mb_bitmap_create_levels(const mb_src *src, uint64_t nrows, const mb_level *levels,
+                                         uint32_t nlevels, uint64_t stride_words, void *stream);
+
 /* Materialised stage 1 (abla::_stg1, primitive_abla.cuh:262-288): runs the
  * program and writes the possible bitmap (and, when chk, the uncertain one).
  * chk selects vprg::chk vs vprg::nochk semantics.  popcount: optional device
@@ -561,20 +583,20 @@ MB_API void *mb_engine_stream(mb_engine *e);
  * mb_queries_layout). */
 #define MB_BATCH_MAX 128
 typedef enum mb_prefetch {
-  MB_PREFETCH_AUTO = 0,     /* columns the batch's selected rows hit densely */
-  MB_PREFETCH_NONE = 1,
-  MB_PREFETCH_ALL = 2       /* every column an op reads for every selected row */
+  MB_PREFETCH_AUTO = 0,     /* the columns the batch's selected rows hit densely, into L2 */
+  MB_PREFETCH_NONE = 1,     /* gathers straight from HBM */
+  MB_PREFETCH_ALL = 2       /* every column an op reads for every selected row, into L2 */
 } mb_prefetch;
 typedef struct mb_batch_opts {
-  uint32_t words_per_lane;  /* 1, 2, 4 or 6 (0 = 4, narrower if a tile does not fit): a tile
-                               is 1024 * words_per_lane rows */
-  uint32_t warps;           /* warps per CTA, 2..16 (0 = 16) */
+  uint32_t words_per_lane;  /* 1, 2, 4 or 6 (0 = the widest of 4, 2, 1 that keeps two stages in
+                               flight): a tile is 1024 * words_per_lane rows */
+  uint32_t warps;           /* warps per CTA, 2..16: one fills the stages, the others work (0 = 16) */
   uint32_t stages;          /* at most this many staged tiles in flight per CTA, 1..4
                                (0 = 4); fewer if they do not fit in shared memory */
   uint32_t ctas_per_sm;     /* 0 = occupancy */
   uint32_t prefetch;        /* mb_prefetch */
-  uint32_t drain_warps;     /* of the warps, those that run the ops (0 = about a fifth);
-                               the others evaluate the bitmaps */
+  uint32_t table_kb;        /* shared memory for per-CTA group tables of the queries with
+                               many rows per group, at most this many KB (0 = up to 48) */
   uint32_t pad_[2];
 } mb_batch_opts;
 MB_API mb_status mb_engine_enqueue_batch(mb_engine *e, const mb_query *qs, uint32_t n,
@@ -587,13 +609,26 @@ MB_API mb_status mb_engine_query_batch(mb_engine *e, const mb_query *qs, uint32_
                                        const mb_batch_opts *opts, int64_t *out_host,
                                        uint64_t *nqual_host);
 
+/* For tests of the bounded device waits: the next `launches` batched-scan
+ * launches of this engine arm their first staged tile without copying into
+ * it, so the wait for that tile runs out after `tries` mbarrier tries
+ * (0: the default limit, about a second).  The kernel records the wait
+ * (code 1, MB_DEVERR_TMA_WAIT) and the block in the device error word, lets
+ * its other copies land and exits; the call or the server then reports
+ * MB_ERR_TIMEOUT (the results of that launch are not delivered) and the
+ * engine carries on.  Nothing faults and nothing spins unbounded.  The
+ * reference has no counterpart: it waits for its kernels without a limit
+ * and exits on a launch error (ssb/lambdas.cuh:233-234). */
+MB_API mb_status mb_engine_test_stall(mb_engine *e, uint32_t launches, uint32_t tries);
+
 /* The launches a batch takes, planned on the host without GPU work: per
  * batched launch its queries, the bitmap rows it stages per tile, its
  * staging copies and its launch shape; *nalone = queries outside the batch
  * kernel's form (they run alone on the plain path). */
 typedef struct mb_batch_launch_info {
   uint32_t queries, staged_rows, copies;
-  uint32_t words_per_lane, warps, drain_warps, stages;
+  uint32_t words_per_lane, warps, table_slots, stages;
+  uint32_t chain_entries;   /* bitmap reads per 32-row word, over all queries */
   uint32_t pad_;
 } mb_batch_launch_info;
 MB_API mb_status mb_engine_batch_info(mb_engine *e, const mb_query *qs, uint32_t n,

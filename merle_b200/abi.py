@@ -53,6 +53,11 @@ class mb_src(C.Structure):
                 ("width", C.c_uint32), ("pad_", C.c_uint32)]
 
 
+class mb_level(C.Structure):
+    _fields_ = [("lo", C.POINTER(C.c_uint64)), ("hi", C.POINTER(C.c_uint64)), ("nbins", C.c_uint32),
+                ("pad_", C.c_uint32), ("out", C.c_void_p), ("popcounts", C.c_void_p)]
+
+
 class mb_term(C.Structure):
     _fields_ = [("src", C.c_uint32), ("pad_", C.c_uint32), ("lo", C.c_uint64), ("hi", C.c_uint64)]
 
@@ -123,13 +128,13 @@ PREFETCH_AUTO, PREFETCH_NONE, PREFETCH_ALL = range(3)
 
 class mb_batch_opts(C.Structure):
     _fields_ = [("words_per_lane", C.c_uint32), ("warps", C.c_uint32), ("stages", C.c_uint32),
-                ("ctas_per_sm", C.c_uint32), ("prefetch", C.c_uint32), ("drain_warps", C.c_uint32),
+                ("ctas_per_sm", C.c_uint32), ("prefetch", C.c_uint32), ("table_kb", C.c_uint32),
                 ("pad_", C.c_uint32 * 2)]
 
 
 class mb_batch_launch_info(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("queries", "staged_rows", "copies", "words_per_lane", "warps",
-                                          "drain_warps", "stages", "pad_")]
+                                          "table_slots", "stages", "chain_entries", "pad_")]
 
 
 class mb_plan(C.Structure):
@@ -198,6 +203,8 @@ SIGNATURES: dict[str, tuple] = {
     "mb_vprg_is_nochk": (I32, [C.POINTER(mb_vprg)]),
     "mb_bitmap_create": (I32, [C.POINTER(mb_src), U64, C.POINTER(U64), C.POINTER(U64), U32, VOIDP, U64,
                                VOIDP, VOIDP]),
+    "mb_bitmap_create_levels": (I32, [C.POINTER(mb_src), U64, C.POINTER(mb_level), U32, U64, VOIDP]),
+    "mb_engine_test_stall": (I32, [VOIDP, U32, U32]),
     "mb_vprg_eval": (I32, [C.POINTER(mb_vprg), I32, VOIDP, VOIDP, VOIDP, VOIDP]),
     "mb_bitmap_to_rows": (I32, [VOIDP, VOIDP, U64, VOIDP, VOIDP, VOIDP]),
     "mb_bitmap_to_rows_noalloc": (I32, [VOIDP, VOIDP, U64, VOIDP, VOIDP, VOIDP]),

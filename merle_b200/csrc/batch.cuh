@@ -6,11 +6,10 @@
 // every DISTINCT bitmap the batch reads (the union: each word fetched from
 // HBM once per batch instead of once per query) with a few 2-D tensor copies
 // of runs of index-slab rows, and prefetches into L2 the tile's rows of the
-// payload columns the batch's ops read densely.  Producer warps take the
-// batch's queries off a counter, costliest first, evaluate each query's
-// conjunctive chain on the staged words and queue its selected rows; every
-// 64 queued rows of a query become a job that consumer warps run through the
-// query's op (batch.cu).
+// payload columns the batch's ops read densely.  Warps take the batch's
+// queries off a counter, costliest first, evaluate each query's conjunctive
+// chain on the staged words and run the query's op on its selected rows of
+// the tile at once (batch.cu).
 //
 // The op of a batch query is its mb_op restated per source slot: the
 // intersected bounds of the single-term clauses on the slot (re-checked for
@@ -23,11 +22,12 @@
 
 namespace mb {
 
-constexpr uint32_t BQ_MAX = 128;   // queries per launch (7-bit query field of a row entry)
+constexpr uint32_t BQ_MAX = 128;   // queries per launch
 constexpr uint32_t BU_MAX = 256;   // bitmap rows staged per tile
 constexpr uint32_t BCP_MAX = 48;   // tensor copies per tile
 constexpr uint32_t BS_MAX = 16;    // distinct op sources per launch
-constexpr uint32_t BC_MAX = 4096;  // chain entries per launch
+constexpr uint32_t BC_MAX = 4096;  // chain entries (bins) per launch
+constexpr uint32_t BJ_MAX = 1024;  // conjuncts per launch
 constexpr uint32_t BW_MAX = 16;    // warps per CTA
 constexpr uint32_t BSLOT = MB_MAXSRC;
 
@@ -42,7 +42,7 @@ struct BatchSrc {
 // Query descriptor: BQD_WORDS 32-bit words.
 //   [0] nslot | single group << 8 | vkind << 16 | va << 20 | vb << 24
 //   [1] groups   [2] first output slot   [3] row-count slot
-//   [4] first chain entry | entries << 16
+//   [4] first conjunct | conjuncts << 16
 //   [5] kv mask | filt mask << 8 | key mask << 16 | term mask << 24 (bit s: slot s)
 //   [6] compiled op shape (BSHAPES index + 1; 0: the generic drain)
 //   [7] slots read through a foreign key (bit s)
@@ -53,23 +53,19 @@ struct BatchSrc {
 enum : uint32_t { BQD_SLOT0 = 8, BQD_SLOTW = 7, BQD_WORDS = 8 + 7 * BSLOT };
 
 // Op shapes with a compiled drain: which slots every row loads (kv), which
-// only uncertain rows load (filt), which are group-key slots and their
-// transform (2 bits per slot: 0 identity, 1 division, 2 year), the value
-// kind and its slots.  The engine's four query templates lower to these
-// (tmpl 1; tmpl 2; tmpl 3 at city or nation level; tmpl 4 with either key
-// scaled); any other op runs the generic drain.
+// only uncertain rows load (filt), which are group-key slots and which of
+// those take the year of a date (the others divide by their divisor, 1 for
+// an identity key, by the magic number of the descriptor), the value kind and
+// its slots.  The engine's four query templates lower to these; any other op
+// runs the generic drain.
 struct BShape {
-  uint32_t ns, kv, filt, keym, xf, vk, va, vb;
+  uint32_t ns, kv, filt, keym, yearm, vk, va, vb;
 };
 constexpr BShape BSHAPES[] = {
     {4, 0x0a, 0x07, 0x00, 0x00, MB_V_MUL, 3, 1},  // tmpl 1
-    {4, 0x0e, 0x03, 0x06, 0x20, MB_V_COL, 3, 0},  // tmpl 2
-    {4, 0x0f, 0x07, 0x07, 0x08, MB_V_COL, 3, 0},  // tmpl 3, city keys
-    {4, 0x0f, 0x07, 0x07, 0x19, MB_V_COL, 3, 0},  // tmpl 3, nation keys
-    {6, 0x3b, 0x0f, 0x0b, 0x08, MB_V_SUB, 4, 5},  // tmpl 4
-    {6, 0x3b, 0x0f, 0x0b, 0x09, MB_V_SUB, 4, 5},
-    {6, 0x3b, 0x0f, 0x0b, 0x48, MB_V_SUB, 4, 5},
-    {6, 0x3b, 0x0f, 0x0b, 0x49, MB_V_SUB, 4, 5},
+    {4, 0x0e, 0x03, 0x06, 0x04, MB_V_COL, 3, 0},  // tmpl 2
+    {4, 0x0f, 0x07, 0x07, 0x02, MB_V_COL, 3, 0},  // tmpl 3
+    {6, 0x3b, 0x0f, 0x0b, 0x02, MB_V_SUB, 4, 5},  // tmpl 4
 };
 constexpr uint32_t BNSHAPE = sizeof(BSHAPES) / sizeof(BSHAPES[0]);
 
@@ -87,28 +83,34 @@ struct BatchHdr {
   uint32_t copy[BCP_MAX];
   BatchSrc src[BS_MAX];
   uint32_t Qd[BQ_MAX * BQD_WORDS];
-  uint16_t chain[BC_MAX];  // one entry per bin (BCH_*): stage row and flags
+  uint16_t chain[BC_MAX];  // one entry per bin: its stage row (slab row while the batch is built)
+  uint32_t conj[BJ_MAX];   // one entry per conjunct (BJ_*)
+  uint32_t nconj;
   uint8_t order[BQ_MAX];   // the order in which warps take the queries (costliest first)
+  // Group tables in shared memory: query q sums into slots [toff[q],
+  // toff[q] + groups) of each CTA's table (0xffffffff: into the output
+  // directly), nstab slots in all.
+  uint32_t toff[BQ_MAX];
+  uint32_t nstab;
 };
 
-// A chain entry: a bin of a query's conjunctive program.  Conjuncts are
-// consecutive runs of entries, the last one flagged; a conjunct is the OR of
-// its bins (edge bins also mark uncertain rows), the query the AND of its
-// conjuncts (of the complement of a negated one).  The host builds entries
-// with slab rows (BCH_SLAB_*) and rewrites them to stage rows when the batch
-// is complete.
+// A query's conjunctive program: conjuncts, each the OR of its bins (edge
+// bins also mark uncertain rows); the query is the AND of its conjuncts (of
+// the complement of a negated one).  A conjunct entry gives its first chain
+// entry, its middle bins and its edge bins (the middle ones first in the
+// chain), and whether it is negated.
 enum : uint32_t {
-  BCH_ROW = 0xffu, BCH_EDGE = 1u << 8, BCH_LAST = 1u << 9, BCH_NEG = 1u << 10,
-  BCH_SLAB_ROW = 0xfffu, BCH_SLAB_FLAGS = 12  // slab row | flags << 12 (flags as above, >> 8)
-};
+  BJ_FIRST = 0xfffu, BJ_NMID_SHIFT = 12, BJ_NEDGE_SHIFT = 20, BJ_NEG = 1u << 24
+};  // first | nmid << 12 (8 bits) | nedge << 20 (4 bits) | negated
 
 // Launch shape of the batched scan.
 struct BatchCfg {
   uint32_t V;       // words per lane: tile = 32 * V words
-  uint32_t warps;     // warps per CTA
-  uint32_t drainers;  // of them, warps that run the jobs (the others produce them)
-  uint32_t stages;    // staged tiles in flight per CTA
+  uint32_t warps;   // warps per CTA
+  uint32_t stages;  // staged tiles in flight per CTA
   uint32_t cps;     // CTAs per SM (0: as many as fit)
+  uint32_t wait_tries;   // try limit of a stage wait (0: 2^20, about a second)
+  uint32_t skip_stage0;  // tests only: the first stage is armed and never filled, so its wait runs out
 };
 
 // Tensor maps of a bitmap slab for one tile width T (words): map h - 1 has

@@ -20,6 +20,8 @@
 //    single-predicate kernel writes past the bitmap end, primitive.cuh:94-99,
 //    and its multi-bin kernel breaks out of a full-mask ballot,
 //    primitive.cuh:110-113; neither happens here).
+#include <string.h>
+#include <algorithm>
 #include "common.cuh"
 #include "tma.cuh"
 
@@ -212,6 +214,162 @@ bitmap_create_kernel(const __grid_constant__ BinSpec S, const void *__restrict__
   }
 }
 
+// ---------------------------------------------------------------- levels
+// One column pass for several levels of bins (years and months of a date,
+// regions and nations of a city): each row's bin in every level comes from
+// one lookup in a shared-memory table over the column's value domain, so
+// the column is read once however many levels it has.
+//  - Levels of up to BL_BALLOT_MAX bins: one __ballot_sync per bin and word;
+//    lane b stores bin b's word, so every word of the tile is written and
+//    the tile needs no clearing.
+//  - Wider levels: each row ORs its bit into its bin's word with one
+//    shared-memory atomic; the write-out clears the words it reads.
+// Words are written out as coalesced 16-byte stores, one warp per bin.
+constexpr int BL_THREADS = 512;
+constexpr int BL_MAXLEVELS = MB_MAXLEVELS;
+constexpr int BL_BALLOT_MAX = 16;
+constexpr uint32_t BL_LUT_BYTES = 24576;  // domain values x levels, one byte each
+constexpr uint8_t BL_NOBIN = 0xff;
+
+struct LevelSpec {
+  uint32_t nlevels, total_bins;
+  uint32_t nb[BL_MAXLEVELS];     // bins of each level (<= 255)
+  uint32_t first[BL_MAXLEVELS];  // first bin of each level in [0, total_bins)
+  uint32_t tile0[BL_MAXLEVELS];  // first word of each level's tile in shared memory
+  uint32_t ballot_mask;          // bit l: level l by ballots
+  uint32_t dom_n;                // values [dom_lo, dom_lo + dom_n) in the table
+  uint64_t dom_lo;
+  uint32_t *out[BL_MAXLEVELS];
+  unsigned long long *pop[BL_MAXLEVELS];
+  uint8_t lut[BL_LUT_BYTES];     // value v: lut[(v - dom_lo) * nlevels + l] = bin of level l (BL_NOBIN: none)
+};
+
+template <int W, bool JOIN, int DW>
+__global__ void __launch_bounds__(BL_THREADS)
+bitmap_levels_kernel(const __grid_constant__ LevelSpec S, const void *__restrict__ col,
+                     const void *__restrict__ dim, uint64_t dimsz, uint64_t n, uint64_t stride, uint32_t *errw) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  constexpr uint32_t STAGE_BYTES = BC_TILE_ROWS * W;
+  uint8_t *stage = smem;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + BC_STAGES * STAGE_BYTES);
+  unsigned long long *cnt = reinterpret_cast<unsigned long long *>(smem + BC_STAGES * STAGE_BYTES + 64);
+  uint32_t *tiles = reinterpret_cast<uint32_t *>(cnt + ((S.total_bins + 1) & ~1u));  // 16-byte aligned
+  uint8_t *lut = reinterpret_cast<uint8_t *>(tiles + S.total_bins * BC_TILE_WORDS);
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = BL_THREADS / 32;
+  const uint64_t nwords = (n + 31) / 32;
+  const uint64_t ntiles = (n + BC_TILE_ROWS - 1) / BC_TILE_ROWS;
+  const uint8_t *colb = reinterpret_cast<const uint8_t *>(col);
+  const uint32_t NL = S.nlevels;
+
+  for (uint32_t i = tid; i < S.dom_n * NL; i += BL_THREADS) lut[i] = S.lut[i];
+  for (uint32_t b = tid; b < S.total_bins; b += BL_THREADS) cnt[b] = 0;
+  for (uint32_t i = tid; i < S.total_bins * BC_TILE_WORDS; i += BL_THREADS) tiles[i] = 0;
+  if (tid == 0) {
+    for (int s = 0; s < BC_STAGES; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  auto tile_bulk_bytes = [&](uint64_t t) -> uint32_t {
+    uint64_t rows = n - t * BC_TILE_ROWS;
+    if (rows > BC_TILE_ROWS) rows = BC_TILE_ROWS;
+    return (uint32_t)((rows * W) & ~(uint64_t)15);
+  };
+  auto issue = [&](uint64_t t, int s) {
+    const uint32_t bytes = tile_bulk_bytes(t);
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&bars[s], bytes);
+    if (bytes) bulk_g2s(stage + s * STAGE_BYTES, colb + t * (uint64_t)STAGE_BYTES, bytes, &bars[s]);
+  };
+  if (tid == 0) {
+    uint64_t t = blockIdx.x;
+    for (int s = 0; s < BC_STAGES && t < ntiles; ++s, t += gridDim.x) issue(t, s);
+  }
+
+  uint32_t it = 0;
+  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+    const int s = it % BC_STAGES;
+    const uint32_t parity = (it / BC_STAGES) & 1u;
+    const bool arrived = mbar_wait_bounded(&bars[s], parity, errw, MB_DEVERR_TMA_WAIT);
+    if (!__syncthreads_and(arrived)) {
+      if (tid == 0) mbar_wait_bounded(&bars[s], parity, nullptr, 0, 1u << 16);
+      return;
+    }
+    const uint8_t *sp = stage + s * STAGE_BYTES;
+    const uint32_t bulk_rows = tile_bulk_bytes(t) / W;
+    const uint64_t row0 = t * BC_TILE_ROWS;
+
+    for (uint32_t wi = warp; wi < BC_TILE_WORDS; wi += nwarps) {
+      const uint32_t r = wi * 32 + lane;
+      const uint64_t row = row0 + r;
+      bool valid = row < n;
+      uint64_t v = 0;
+      if (valid) {
+        const uint64_t x = r < bulk_rows ? ld_smem_w<W>(sp, r) : load_width(col, row, W);
+        if (JOIN) {
+          if (dimsz != 0 && x >= dimsz) valid = false;
+          else v = load_width(dim, x, DW);
+        } else {
+          v = x;
+        }
+      }
+      const bool inlut = valid && v >= S.dom_lo && v - S.dom_lo < S.dom_n;
+      const uint32_t li = inlut ? (uint32_t)(v - S.dom_lo) * NL : 0u;
+      for (uint32_t l = 0; l < NL; ++l) {
+        const uint32_t b = inlut ? lut[li + l] : BL_NOBIN;
+        uint32_t *tl = tiles + S.tile0[l];
+        if ((S.ballot_mask >> l) & 1u) {
+          const uint32_t nb = S.nb[l];
+          uint32_t mine = 0;
+          for (uint32_t j = 0; j < nb; ++j) {
+            const uint32_t m = __ballot_sync(0xffffffffu, b == j);
+            if (lane == j) mine = m;
+          }
+          if (lane < nb) tl[tile_word(lane, wi)] = mine;
+        } else if (b != BL_NOBIN) {
+          atomicOr(&tl[tile_word(b, wi)], 1u << lane);
+        }
+      }
+    }
+    __syncthreads();  // stage s fully read, tiles complete
+
+    if (tid == 0 && t + (uint64_t)BC_STAGES * gridDim.x < ntiles) issue(t + (uint64_t)BC_STAGES * gridDim.x, s);
+
+    // write-out: warp g takes bin g (over all levels), its 128 words as 32
+    // lanes x uint4
+    const uint64_t w = t * BC_TILE_WORDS + lane * 4;
+    for (uint32_t g = warp; g < S.total_bins; g += nwarps) {
+      uint32_t l = 0;
+      while (l + 1 < NL && g >= S.first[l + 1]) ++l;
+      const uint32_t b = g - S.first[l];
+      uint4 *src = reinterpret_cast<uint4 *>(tiles + S.tile0[l] + tile_word(b, lane * 4));
+      const uint4 v4 = *src;
+      if (!((S.ballot_mask >> l) & 1u)) *src = make_uint4(0, 0, 0, 0);
+      uint32_t c = 0;
+      if (w < nwords) {
+        uint32_t *dst = S.out[l] + b * stride + w;
+        if (w + 4 <= nwords) {
+          *reinterpret_cast<uint4 *>(dst) = v4;
+        } else {
+          dst[0] = v4.x;
+          if (w + 1 < nwords) dst[1] = v4.y;
+          if (w + 2 < nwords) dst[2] = v4.z;
+        }
+        c = __popc(v4.x) + __popc(v4.y) + __popc(v4.z) + __popc(v4.w);
+      }
+      c = __reduce_add_sync(0xffffffffu, c);
+      if (lane == 0 && c) cnt[g] += c;  // this warp owns bin g in this tile
+    }
+    __syncthreads();  // tiles reused by the next tile
+  }
+  __syncthreads();
+  for (uint32_t g = tid; g < S.total_bins; g += BL_THREADS) {
+    uint32_t l = 0;
+    while (l + 1 < NL && g >= S.first[l + 1]) ++l;
+    if (S.pop[l] && cnt[g]) atomicAdd(&S.pop[l][g - S.first[l]], cnt[g]);
+  }
+}
+
 // ---------------------------------------------------------------- host
 template <int W, bool JOIN, int DW, int MODE>
 static mb_status launch_bc(const BinSpec &S, const mb_src *src, uint64_t n, uint32_t *out,
@@ -255,6 +413,71 @@ static mb_status dispatch_w(uint32_t w, int mode, const BinSpec &S, const mb_src
   case 4: return dispatch_mode<4, JOIN, DW>(mode, S, src, n, out, stride, pop, st);
   default: return dispatch_mode<8, JOIN, DW>(mode, S, src, n, out, stride, pop, st);
   }
+}
+
+
+// ---------------------------------------------------------------- levels host
+template <int W, bool JOIN, int DW>
+static mb_status launch_levels(const LevelSpec &S, const mb_src *src, uint64_t n, uint64_t stride, cudaStream_t st) {
+  auto kern = bitmap_levels_kernel<W, JOIN, DW>;
+  const size_t smem = (size_t)BC_STAGES * BC_TILE_ROWS * W + 64 + (size_t)((S.total_bins + 1) & ~1u) * 8 +
+                      (size_t)S.total_bins * BC_TILE_WORDS * 4 + round_up((uint64_t)S.dom_n * S.nlevels, 16);
+  MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, BL_THREADS, smem));
+  if (occ < 1) return fail(MB_ERR_INVALID, "bitmap_create_levels: %u bins do not fit in shared memory", S.total_bins);
+  uint64_t grid = (uint64_t)dev_info().sms * occ;
+  const uint64_t ntiles = ceil_div(n, BC_TILE_ROWS);
+  if (grid > ntiles) grid = ntiles;
+  uint32_t *errw = device_error_word();
+  if (!errw) return fail(MB_ERR_OOM, "bitmap_create_levels: device error word");
+  const void *colp = JOIN ? (const void *)src->fk : src->col;
+  const void *dimp = JOIN ? src->col : nullptr;
+  kern<<<(unsigned)grid, BL_THREADS, smem, st>>>(S, colp, dimp, src->dimsz, n, stride, errw);
+  MB_LAUNCH_CHECK("bitmap_levels_kernel");
+  return MB_OK;
+}
+
+// The levels as one LevelSpec, if the fast path takes them: each level
+// sorted and disjoint with at most 255 bins, the value domain small enough
+// for the lookup table, the tiles within shared memory.
+static bool levels_spec(const mb_level *lv, uint32_t nl, LevelSpec &S) {
+  if (nl == 0 || nl > (uint32_t)BL_MAXLEVELS) return false;
+  memset(&S, 0, sizeof(S));
+  S.nlevels = nl;
+  uint64_t dlo = ~0ull, dhi = 0;
+  uint32_t words = 0;
+  for (uint32_t l = 0; l < nl; ++l) {
+    const mb_level &L = lv[l];
+    if (L.nbins == 0 || L.nbins >= BL_NOBIN || !L.lo || !L.hi || !L.out) return false;
+    for (uint32_t j = 0; j < L.nbins; ++j) {
+      if (L.hi[j] <= L.lo[j]) return false;
+      if (j + 1 < L.nbins && L.lo[j + 1] < L.hi[j]) return false;
+    }
+    dlo = std::min<uint64_t>(dlo, L.lo[0]);
+    dhi = std::max<uint64_t>(dhi, L.hi[L.nbins - 1]);
+    S.nb[l] = L.nbins;
+    S.first[l] = S.total_bins;
+    S.total_bins += L.nbins;
+    S.tile0[l] = words;
+    words += L.nbins * BC_TILE_WORDS;
+    if (L.nbins <= (uint32_t)BL_BALLOT_MAX) S.ballot_mask |= 1u << l;
+    S.out[l] = L.out;
+    S.pop[l] = reinterpret_cast<unsigned long long *>(L.popcounts);
+  }
+  if (dhi - dlo > BL_LUT_BYTES / nl) return false;
+  S.dom_lo = dlo;
+  S.dom_n = (uint32_t)(dhi - dlo);
+  for (uint32_t l = 0; l < nl; ++l) {
+    const mb_level &L = lv[l];
+    uint32_t j = 0;
+    for (uint64_t v = dlo; v < dhi; ++v) {
+      while (j < L.nbins && L.hi[j] <= v) ++j;
+      const bool in = j < L.nbins && L.lo[j] <= v;
+      S.lut[(v - dlo) * nl + l] = in ? (uint8_t)j : BL_NOBIN;
+    }
+  }
+  return true;
 }
 
 static int classify_bins(const uint64_t *lo, const uint64_t *hi, uint32_t nb, uint64_t *lo0,
@@ -330,4 +553,46 @@ extern "C" mb_status mb_bitmap_create(const mb_src *src, uint64_t nrows, const u
     if (r != MB_OK) return r;
   }
   return MB_OK;
+}
+
+extern "C" mb_status mb_bitmap_create_levels(const mb_src *src, uint64_t nrows, const mb_level *levels,
+                                             uint32_t nlevels, uint64_t stride_words, void *stream) {
+  if (!src || (!levels && nlevels)) return fail(MB_ERR_INVALID, "mb_bitmap_create_levels: NULL argument");
+  if (nlevels == 0) return MB_OK;
+  const uint32_t w = src->width;
+  if (w != 1 && w != 2 && w != 4 && w != 8)
+    return fail(MB_ERR_INVALID, "mb_bitmap_create_levels: width %u not in {1,2,4,8}", w);
+  if (!src->col) return fail(MB_ERR_INVALID, "mb_bitmap_create_levels: column is NULL");
+  if (stride_words < mb_bitmap_words(nrows) || (stride_words & 3) != 0)
+    return fail(MB_ERR_INVALID, "mb_bitmap_create_levels: stride %llu < words or not a multiple of 4",
+                (unsigned long long)stride_words);
+  for (uint32_t l = 0; l < nlevels; ++l)
+    if (levels[l].nbins && (!levels[l].out || ((uintptr_t)levels[l].out & 15) != 0))
+      return fail(MB_ERR_INVALID, "mb_bitmap_create_levels: level %u output NULL or not 16-byte aligned", l);
+  const void *staged = src->fk ? (const void *)src->fk : src->col;
+  if (((uintptr_t)staged & 15) != 0)
+    return fail(MB_ERR_INVALID, "mb_bitmap_create_levels: staged column not 16-byte aligned");
+  if (nrows == 0) return MB_OK;
+  cudaStream_t st = as_stream(stream);
+  static thread_local LevelSpec S;  // 24 KB lookup table: not on the stack
+  const bool fast = levels_spec(levels, nlevels, S) && (w <= 4 || src->fk);
+  if (!fast) {  // one pass per level
+    for (uint32_t l = 0; l < nlevels; ++l)
+      MB_CHECK(mb_bitmap_create(src, nrows, levels[l].lo, levels[l].hi, levels[l].nbins, levels[l].out, stride_words,
+                                levels[l].popcounts, stream));
+    return MB_OK;
+  }
+  if (src->fk == nullptr) {
+    switch (w) {
+    case 1: return launch_levels<1, false, 1>(S, src, nrows, stride_words, st);
+    case 2: return launch_levels<2, false, 1>(S, src, nrows, stride_words, st);
+    default: return launch_levels<4, false, 1>(S, src, nrows, stride_words, st);
+    }
+  }
+  switch (w) {  // staged column is the 4-byte key; w is the dimension width
+  case 1: return launch_levels<4, true, 1>(S, src, nrows, stride_words, st);
+  case 2: return launch_levels<4, true, 2>(S, src, nrows, stride_words, st);
+  case 4: return launch_levels<4, true, 4>(S, src, nrows, stride_words, st);
+  default: return launch_levels<4, true, 8>(S, src, nrows, stride_words, st);
+  }
 }

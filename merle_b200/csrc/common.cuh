@@ -91,6 +91,10 @@ inline uint64_t round_up(uint64_t a, uint64_t b) { return ceil_div(a, b) * b; }
 // ---------------------------------------------------------------- device
 // Error word written by kernels whose bounded waits ran out.  Index 0 is a
 // flag, index 1 a code (which wait), index 2 the block that gave up.
+// MB_DEVERR_TMA_WAIT: copies into a shared-memory stage did not arrive;
+// MB_DEVERR_IDLE_WAIT: a stage was not released by the warps reading it.
+// A kernel that gave up has left its outputs partial: the host treats the
+// whole launch's results as lost (and zeroes what it hands back).
 enum { MB_DEVERR_NONE = 0, MB_DEVERR_TMA_WAIT = 1, MB_DEVERR_IDLE_WAIT = 2 };
 uint32_t *device_error_word();   // per-device, allocated on first use
 mb_status check_device_error(cudaStream_t s);

@@ -213,13 +213,11 @@ __global__ void denorm_kernel(const uint32_t *__restrict__ fk, const D *__restri
 // Builds custcity_row and partmfgr_row; a column whose foreign keys leave
 // their dimension is dropped again (its queries keep the probe, which
 // treats such rows as the op semantics say).
-mb_status Engine::build_denorm() {
-  free_denorm();
-  unsigned long long *d_bad = nullptr;
-  MB_CHECK(alloc((void **)&d_bad, 16));
+// The denormalised per-row columns (allocated by the caller), filled on the
+// engine stream; d_bad (device, 2 counters) counts foreign keys outside their
+// dimension.
+mb_status Engine::enqueue_denorm(unsigned long long *d_bad) {
   MB_CUDA(cudaMemsetAsync(d_bad, 0, 16, stream));
-  MB_CHECK(alloc((void **)&custcity_row, nrows));
-  MB_CHECK(alloc((void **)&partmfgr_row, nrows * 2));
   const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(nrows, 256), 148ull * 8));
   denorm_kernel<uint8_t><<<grid, 256, 0, stream>>>(reinterpret_cast<const uint32_t *>(custkey), custcity,
                                                     ncust + 1, custcity_row, nrows, d_bad);
@@ -227,18 +225,23 @@ mb_status Engine::build_denorm() {
   denorm_kernel<uint16_t><<<grid, 256, 0, stream>>>(reinterpret_cast<const uint32_t *>(partkey), partmfgr,
                                                      npart + 1, partmfgr_row, nrows, d_bad + 1);
   MB_LAUNCH_CHECK("denorm_kernel");
+  return MB_OK;
+}
+
+// The denormalised columns, built and checked before returning; a foreign key
+// outside its dimension leaves the probes in place instead.
+mb_status Engine::build_denorm() {
+  free_denorm();
+  unsigned long long *d_bad = nullptr;
+  MB_CHECK(alloc((void **)&d_bad, 16));
+  MB_CHECK(alloc((void **)&custcity_row, nrows));
+  MB_CHECK(alloc((void **)&partmfgr_row, nrows * 2));
+  MB_CHECK(enqueue_denorm(d_bad));
   unsigned long long bad[2] = {0, 0};
   MB_CUDA(cudaMemcpyAsync(bad, d_bad, 16, cudaMemcpyDeviceToHost, stream));
   MB_CUDA(cudaStreamSynchronize(stream));
   free_one(allocs, d_bad);
-  if (bad[0]) {
-    free_one(allocs, custcity_row);
-    custcity_row = nullptr;
-  }
-  if (bad[1]) {
-    free_one(allocs, partmfgr_row);
-    partmfgr_row = nullptr;
-  }
+  if (bad[0] || bad[1]) free_denorm();
   return MB_OK;
 }
 
@@ -737,34 +740,68 @@ extern "C" mb_status mb_engine_build_index_levels(mb_engine *e, uint32_t flags, 
   if (!E.custkey) return fail(MB_ERR_INVALID, "mb_engine_build_index: no table");
   MB_CUDA(cudaSetDevice(E.device));
   E.drop_index();
-  MB_CUDA(cudaEventRecord(E.ev0, E.stream));
-  if (flags & MB_INDEX_PROBE_DIMS) E.free_denorm();
-  else MB_CHECK(E.build_denorm());
-  MB_CHECK(E.setup_index_cols());
-  uint64_t *d_pop = nullptr;
-  MB_CHECK(E.alloc((void **)&d_pop, 1024 * 8));
+  const bool denorm = !(flags & MB_INDEX_PROBE_DIMS);
+  // every allocation first, so the timed build below is device work only
+  unsigned long long *d_bad = nullptr;
+  MB_CHECK(E.alloc((void **)&d_bad, 16));
+  E.free_denorm();
+  if (denorm) {
+    MB_CHECK(E.alloc((void **)&E.custcity_row, E.nrows));
+    MB_CHECK(E.alloc((void **)&E.partmfgr_row, E.nrows * 2));
+  }
+  MB_CHECK(E.setup_index_cols());  // sources: the denormalised columns filled below
   for (auto &c : E.idx)
     for (auto &l : c.levels) E.nbm += l.nbins();
+  uint64_t *d_pop = nullptr;
+  MB_CHECK(E.alloc((void **)&d_pop, (size_t)E.nbm * 8));
   MB_CHECK(E.alloc((void **)&E.islab, (size_t)E.nbm * E.stride * 4));
-  MB_CUDA(cudaMemsetAsync(E.islab, 0, (size_t)E.nbm * E.stride * 4, E.stream));
+  const uint64_t nwords = (E.nrows + 31) / 32;
+
+  MB_CUDA(cudaEventRecord(E.ev0, E.stream));
+  if (denorm) MB_CHECK(E.enqueue_denorm(d_bad));
+  // only the padding words past each bitmap's end need clearing: the passes
+  // write every word below it
+  if (E.stride > nwords)
+    MB_CUDA(cudaMemset2DAsync(E.islab + nwords, E.stride * 4, 0, (E.stride - nwords) * 4, E.nbm, E.stream));
+  MB_CUDA(cudaMemsetAsync(d_pop, 0, (size_t)E.nbm * 8, E.stream));
   uint64_t first = 0;
   for (auto &c : E.idx) {
-    for (auto &l : c.levels) {
+    std::vector<std::vector<uint64_t>> lo(c.levels.size()), hi(c.levels.size());
+    std::vector<mb_level> lv(c.levels.size());
+    for (size_t i = 0; i < c.levels.size(); ++i) {
+      Level &l = c.levels[i];
       const uint32_t nb = l.nbins();
       l.slab = E.islab + first * E.stride;
+      lo[i].assign(l.bounds.begin(), l.bounds.end() - 1);
+      hi[i].assign(l.bounds.begin() + 1, l.bounds.end());
+      memset(&lv[i], 0, sizeof(mb_level));
+      lv[i].lo = lo[i].data(), lv[i].hi = hi[i].data(), lv[i].nbins = nb;
+      lv[i].out = l.slab, lv[i].popcounts = d_pop + first;
       first += nb;
-      MB_CUDA(cudaMemsetAsync(d_pop, 0, nb * 8, E.stream));
-      std::vector<uint64_t> lo(l.bounds.begin(), l.bounds.end() - 1), hi(l.bounds.begin() + 1, l.bounds.end());
-      MB_CHECK(mb_bitmap_create(&c.src, E.nrows, lo.data(), hi.data(), nb, l.slab, E.stride, d_pop, E.stream));
-      l.pop.assign(nb, 0);
-      MB_CUDA(cudaMemcpyAsync(l.pop.data(), d_pop, nb * 8, cudaMemcpyDeviceToHost, E.stream));
     }
+    MB_CHECK(mb_bitmap_create_levels(&c.src, E.nrows, lv.data(), (uint32_t)lv.size(), E.stride, E.stream));
   }
   MB_CUDA(cudaEventRecord(E.ev1, E.stream));
+  std::vector<uint64_t> pops(E.nbm);
+  unsigned long long bad[2] = {0, 0};
+  MB_CUDA(cudaMemcpyAsync(pops.data(), d_pop, (size_t)E.nbm * 8, cudaMemcpyDeviceToHost, E.stream));
+  MB_CUDA(cudaMemcpyAsync(bad, d_bad, 16, cudaMemcpyDeviceToHost, E.stream));
   MB_CUDA(cudaStreamSynchronize(E.stream));
   MB_CHECK(check_device_error(E.stream));
   cudaEventElapsedTime(&E.index_build_ms, E.ev0, E.ev1);
   free_one(E.allocs, d_pop);
+  free_one(E.allocs, d_bad);
+  if (denorm && (bad[0] || bad[1])) {
+    // a foreign key outside its dimension: the denormalised columns cannot
+    // stand in for the probes; build over the probes instead
+    return mb_engine_build_index_levels(e, flags | MB_INDEX_PROBE_DIMS, level_mask);
+  }
+  first = 0;
+  for (auto &c : E.idx)
+    for (auto &l : c.levels) {
+      l.pop.assign(pops.begin() + first, pops.begin() + first + l.nbins());
+      first += l.nbins();
+    }
   E.indexed = true;
   return MB_OK;
 }
@@ -1018,6 +1055,7 @@ struct BatchBuild {
   std::vector<uint8_t> used;  // slab rows the batch reads
   uint32_t nused = 0;
   std::vector<double> cost;   // estimated cost of each query (per bitmap word)
+  std::vector<double> sel;    // estimated selected-row fraction of each query
   double src_weight[BS_MAX] = {};  // selected-row fraction reading each source
 
   void reset(BatchHdr *hh, const Engine &E) {
@@ -1028,23 +1066,24 @@ struct BatchBuild {
     h->stride = E.stride;
     h->slab = E.islab;
     h->nslab = E.nbm;
+    for (uint32_t q = 0; q < BQ_MAX; ++q) h->toff[q] = 0xffffffffu;
     used.assign(E.nbm, 0);
     nused = 0;
     cost.clear();
+    sel.clear();
     for (double &w : src_weight) w = 0;
   }
 };
 
-// The staging of a set of slab rows: runs of rows (gaps of up to two unused
-// rows merged in: reading them costs less than issuing another copy), one
-// tensor copy per run.  Fills copy[] (BatchHdr packing) and, if stage_of is
+// The staging of a set of slab rows: runs of rows, one tensor copy per run
+// (the smallest gaps merged while there would be more than BCP_MAX copies).  Fills copy[] (BatchHdr packing) and, if stage_of is
 // given, the stage row of every used slab row; returns the rows staged, or
 // 0 if the set needs more than BU_MAX rows or BCP_MAX copies.
 static uint32_t stage_plan(const std::vector<uint8_t> &used, uint32_t *copy, uint32_t *ncopy, uint16_t *stage_of) {
   std::vector<std::pair<uint32_t, uint32_t>> runs;  // [a, b)
   for (uint32_t r = 0; r < used.size(); ++r) {
     if (!used[r]) continue;
-    if (!runs.empty() && r - runs.back().second <= 2) runs.back().second = r + 1;
+    if (!runs.empty() && r == runs.back().second) runs.back().second = r + 1;
     else runs.push_back({r, r + 1});
   }
   if (runs.empty()) runs.push_back({0, 1});  // no bitmap read: stage one row anyway
@@ -1118,10 +1157,12 @@ static bool slot_plan(const mb_op &O, uint32_t *d) {
     keym |= 1u << kk.src;
     uint32_t *sl = d + BQD_SLOT0 + BQD_SLOTW * kk.src;
     uint32_t sh = 0;
-    if (kk.xform == MB_X_DIV) {
-      const DivMagic m = div_magic(kk.div);
-      for (uint32_t x : {0u, 1u, kk.div - 1, kk.div, kk.div + 1, 12345u, 0x7fffffffu, 0xfffffffeu, 0xffffffffu})
-        if (div_by_magic(x, m.m, m.sh1, m.sh2) != x / kk.div) return false;
+    if (kk.xform == MB_X_DIV || kk.xform == MB_X_ID) {  // an identity key divides by 1
+      const uint32_t dv = kk.xform == MB_X_DIV ? kk.div : 1u;
+      if (dv == 0) return false;
+      const DivMagic m = div_magic(dv);
+      for (uint32_t x : {0u, 1u, dv - 1, dv, dv + 1, 12345u, 0x7fffffffu, 0xfffffffeu, 0xffffffffu})
+        if (div_by_magic(x, m.m, m.sh1, m.sh2) != x / dv) return false;
       sl[3] = m.m;
       sh = m.sh1 | (m.sh2 << 4);
     }
@@ -1144,16 +1185,14 @@ static bool slot_plan(const mb_op &O, uint32_t *d) {
   for (uint32_t s2 = 0; s2 < O.nsrc; ++s2)
     if (O.src[s2].fk) d[7] |= 1u << s2;
   // a compiled drain for this shape, if there is one
-  uint32_t xf = 0;
-  for (uint32_t k = 0; k < O.nkey; ++k) {
-    const uint32_t x = O.keys[k].xform == MB_X_DIV ? 1u : O.keys[k].xform == MB_X_YEAR ? 2u : 0u;
-    xf |= x << (2 * O.keys[k].src);
-  }
   const uint32_t va = O.vkind == MB_V_ONE ? 0 : O.va, vb = (O.vkind == MB_V_MUL || O.vkind == MB_V_SUB) ? O.vb : 0;
+  uint32_t yearm = 0;
+  for (uint32_t k = 0; k < O.nkey; ++k)
+    if (O.keys[k].xform == MB_X_YEAR) yearm |= 1u << O.keys[k].src;
   for (uint32_t i = 0; i < BNSHAPE; ++i) {
     const BShape &b = BSHAPES[i];
     if (b.ns == O.nsrc && b.kv == (N.kv_mask & 0xffu) && b.filt == (N.filt_mask & 0xffu) && b.keym == keym &&
-        b.xf == xf && b.vk == O.vkind && b.va == va && b.vb == vb && termm == b.filt) {
+        b.yearm == yearm && b.vk == O.vkind && b.va == va && b.vb == vb && termm == b.filt) {
       d[6] = i + 1;
       break;
     }
@@ -1187,6 +1226,13 @@ static int batch_add(BatchBuild &B, const Lowered &L, const DevPrg &P, uint64_t 
     if (!seen) ++newsrc;
   }
   const uint32_t nch = P.ncnf;  // chain entries
+  uint32_t ncj = 0;             // conjuncts, each of at most 255 middle and 15 edge bins
+  for (uint32_t i = 0, nm = 0, ne = 0; i < P.ncnf; ++i) {
+    if (P.cnf_flag[i] & CNF_EDGE) ++ne;
+    else ++nm;
+    if (nm > 0xff || ne > 0xf) return BADD_ALONE;
+    if (P.cnf_flag[i] & CNF_END) ++ncj, nm = 0, ne = 0;
+  }
   bool stages_ok = true;
   if (!fresh.empty()) {
     for (uint32_t r : fresh) B.used[r] = 1;
@@ -1194,8 +1240,9 @@ static int batch_add(BatchBuild &B, const Lowered &L, const DevPrg &P, uint64_t 
     if (!stages_ok)
       for (uint32_t r : fresh) B.used[r] = 0;
   }
-  if (newsrc > BS_MAX || nch > BC_MAX || (!stages_ok && B.nused == 0)) return BADD_ALONE;
-  if (h.nq + 1 > BQ_MAX || !stages_ok || h.nsrc + newsrc > BS_MAX || h.nchain + nch > BC_MAX) {
+  if (newsrc > BS_MAX || nch > BC_MAX || ncj > BJ_MAX || (!stages_ok && B.nused == 0)) return BADD_ALONE;
+  if (h.nq + 1 > BQ_MAX || !stages_ok || h.nsrc + newsrc > BS_MAX || h.nchain + nch > BC_MAX ||
+      h.nconj + ncj > BJ_MAX) {
     if (stages_ok)
       for (uint32_t r : fresh) B.used[r] = 0;
     return BADD_FULL;
@@ -1221,24 +1268,29 @@ static int batch_add(BatchBuild &B, const Lowered &L, const DevPrg &P, uint64_t 
   d[1] = L.ngroups;
   d[2] = (uint32_t)out_off;
   d[3] = nq_slot;
-  // the chain: one entry per bin, slab row | flags (made stage rows by
-  // batch_finish)
-  const uint32_t c0 = h.nchain;
+  // the program: per conjunct its middle bins then its edge bins in the
+  // chain (slab rows, made stage rows by batch_finish) and one conjunct entry
+  const uint32_t j0 = h.nconj;
   for (uint32_t i = 0; i < P.ncnf;) {
     uint32_t j = i;
     while (!(P.cnf_flag[j] & CNF_END)) ++j;  // [i, j] is one conjunct
-    for (uint32_t k = i; k <= j; ++k) {
-      uint32_t f = (P.cnf_flag[k] & CNF_EDGE) ? BCH_EDGE : 0u;
-      if (k == j) f |= BCH_LAST | ((P.cnf_flag[j] & CNF_NEG) ? BCH_NEG : 0u);
-      h.chain[h.nchain++] = (uint16_t)((uint32_t)slab_row(h, P.cnf_ptr[k]) | ((f >> 8) << BCH_SLAB_FLAGS));
-    }
+    const uint32_t first = h.nchain;
+    uint32_t nmid = 0, nedge = 0;
+    for (uint32_t k = i; k <= j; ++k)
+      if (!(P.cnf_flag[k] & CNF_EDGE)) h.chain[h.nchain++] = (uint16_t)slab_row(h, P.cnf_ptr[k]), ++nmid;
+    for (uint32_t k = i; k <= j; ++k)
+      if (P.cnf_flag[k] & CNF_EDGE) h.chain[h.nchain++] = (uint16_t)slab_row(h, P.cnf_ptr[k]), ++nedge;
+    h.conj[h.nconj++] = first | (nmid << BJ_NMID_SHIFT) | (nedge << BJ_NEDGE_SHIFT) |
+                        ((P.cnf_flag[j] & CNF_NEG) ? BJ_NEG : 0u);
     i = j + 1;
   }
-  d[4] = c0 | ((h.nchain - c0) << 16);
+  d[4] = j0 | ((h.nconj - j0) << 16);
   memcpy(h.Qd + (size_t)q * BQD_WORDS, d, sizeof(d));
-  // cost per bitmap word of a tile: the chain entries, the compaction, and
-  // the ops of the selected rows (about 2 chain entries' worth per row)
-  B.cost.push_back((double)P.ncnf + 2.0 + 64.0 * sel);
+  // cost per bitmap word of a tile: the chain entries and the ops of the
+  // selected rows (a round of 32 rows costs about as much as 20 entries of a
+  // word per lane)
+  B.cost.push_back((double)P.ncnf + 2.0 + 600.0 * sel);
+  B.sel.push_back(sel);
   return BADD_OK;
 }
 
@@ -1252,29 +1304,75 @@ static double est_selectivity(const Engine &E, const Lowered &L) {
   return f;
 }
 
-// The launch shape: the options given, and for stages left at 0 the most
-// (up to 4) that fit in shared memory, narrowing the tile if not even two do.
-static BatchCfg batch_cfg(const BatchHdr &h, const mb_batch_opts &o) {
-  BatchCfg c;
-  c.V = o.words_per_lane ? o.words_per_lane : 4;
-  c.warps = o.warps ? std::min<uint32_t>(o.warps, BW_MAX) : 16;
-  c.drainers = o.drain_warps ? o.drain_warps : std::max<uint32_t>(1, (c.warps + 2) / 5);
-  c.cps = o.ctas_per_sm;
+// The most stages (up to smax) of shape c that fit in shared memory.
+static bool fit_stages(const BatchHdr &h, BatchCfg &c, uint32_t smax) {
   const size_t cap = (size_t)dev_info().max_smem_optin;
-  const uint32_t smax = o.stages ? o.stages : 4;
-  while (true) {
-    for (c.stages = smax; c.stages > 1; --c.stages)
-      if (batch_smem(h, c) && batch_smem(h, c) <= cap) break;
-    if (batch_smem(h, c) && batch_smem(h, c) <= cap) break;  // (one stage, if that is all that fits)
-    if (c.V == 1 || o.words_per_lane) break;
-    c.V = c.V == 6 ? 4 : c.V >> 1;  // not even one stage of this tile fits: narrower tiles
+  for (c.stages = smax; c.stages >= 1; --c.stages) {
+    const size_t b = batch_smem(h, c);
+    if (b && b <= cap) return true;
   }
+  c.stages = 1;
+  return false;
+}
+
+// The launch shape: the options given; for what they leave open, the widest
+// tile (4, 2, then 1 words per lane) that keeps two stages in flight, and as
+// many stages (up to 4) as fit.
+static BatchCfg batch_cfg(const BatchHdr &h, const mb_batch_opts &o) {
+  const uint32_t smax = o.stages ? o.stages : 4;
+  std::vector<uint32_t> Vs;
+  if (o.words_per_lane) Vs.push_back(o.words_per_lane);
+  else Vs = {4u, 2u, 1u};
+  BatchCfg one;  // the first shape with one stage, if none has two
+  bool have_one = false;
+  for (uint32_t V : Vs) {
+    BatchCfg c;
+    memset(&c, 0, sizeof(c));
+    c.V = V;
+    c.warps = o.warps ? std::min<uint32_t>(o.warps, BW_MAX) : 16;
+    c.cps = o.ctas_per_sm;
+    if (!fit_stages(h, c, smax)) continue;
+    if (c.stages >= 2 || smax == 1) return c;
+    if (!have_one) one = c, have_one = true;
+  }
+  if (have_one) return one;
+  BatchCfg c;  // nothing fits: batch_scan reports the shape
+  memset(&c, 0, sizeof(c));
+  c.V = Vs.back();
+  c.warps = o.warps ? std::min<uint32_t>(o.warps, BW_MAX) : 16;
+  c.stages = 1;
   return c;
 }
 
+// Shared group tables: the multi-group queries whose estimated rows per CTA
+// are many times their group count (so a flush of the table costs far less
+// than the global atomics it saves), most rows first, while they fit in the
+// shared memory the launch shape leaves (at most table_kb KB; 48 KB if 0).
+static void batch_tables(BatchBuild &B, const mb_batch_opts &o, const BatchCfg &c) {
+  BatchHdr &h = *B.h;
+  const size_t cap = (size_t)dev_info().max_smem_optin;
+  const size_t used = batch_smem(h, c);
+  h.nstab = 0;
+  if (!used || used >= cap) return;
+  uint64_t slots = std::min<uint64_t>((cap - used) / 8 - 2, (o.table_kb ? o.table_kb : 48u) * 128ull);
+  const double ctas = (double)dev_info().sms;
+  std::vector<uint32_t> cand;
+  for (uint32_t q = 0; q < h.nq; ++q) {
+    const uint32_t ng = h.Qd[(size_t)q * BQD_WORDS + 1];
+    if (ng > 1 && B.sel[q] * (double)h.nrows >= 8.0 * ctas * ng) cand.push_back(q);
+  }
+  std::stable_sort(cand.begin(), cand.end(), [&](uint32_t a, uint32_t b) { return B.sel[a] > B.sel[b]; });
+  for (uint32_t q : cand) {
+    const uint32_t ng = h.Qd[(size_t)q * BQD_WORDS + 1];
+    if (h.nstab + ng > slots) continue;
+    h.toff[q] = h.nstab;
+    h.nstab += ng;
+  }
+}
+
 // Completes a batch's header: the order of its queries, its staging copies
-// (the chain's slab rows become stage rows), its L2 prefetches, and its
-// launch shape.
+// (the chain's slab rows become stage rows), its L2 prefetches, its launch
+// shape and its shared group tables.
 static mb_status batch_finish(BatchBuild &B, const mb_batch_opts &o, BatchCfg *cfg) {
   BatchHdr &h = *B.h;
   std::vector<uint32_t> order(h.nq);
@@ -1284,14 +1382,11 @@ static mb_status batch_finish(BatchBuild &B, const mb_batch_opts &o, BatchCfg *c
   std::vector<uint16_t> stage_of(h.nslab ? h.nslab : 1, 0xffffu);
   h.nu = stage_plan(B.used, h.copy, &h.ncopy, stage_of.data());
   if (h.nu == 0) return fail(MB_ERR_INVALID, "batch: staging plan over its limits");
-  for (uint32_t q = 0; q < h.nq; ++q) {
-    const uint32_t c0 = h.Qd[(size_t)q * BQD_WORDS + 4] & 0xffffu, n = h.Qd[(size_t)q * BQD_WORDS + 4] >> 16;
-    for (uint32_t i = c0; i < c0 + n; ++i) {
-      const uint32_t e = h.chain[i], r = e & BCH_SLAB_ROW;
-      const uint16_t t = r < h.nslab ? stage_of[r] : 0xffffu;
-      if (t >= h.nu || t > BCH_ROW) return fail(MB_ERR_INVALID, "batch: chain row %u not staged", r);
-      h.chain[i] = (uint16_t)(t | ((e >> BCH_SLAB_FLAGS) << 8));
-    }
+  for (uint32_t i = 0; i < h.nchain; ++i) {
+    const uint32_t r = h.chain[i];
+    const uint16_t t = r < h.nslab ? stage_of[r] : 0xffffu;
+    if (t >= h.nu) return fail(MB_ERR_INVALID, "batch: chain row %u not staged", r);
+    h.chain[i] = t;
   }
   h.pf_mask = 0;
   for (uint32_t i = 0; i < h.nsrc; ++i) {
@@ -1300,7 +1395,9 @@ static mb_status batch_finish(BatchBuild &B, const mb_batch_opts &o, BatchCfg *c
     const bool dense = o.prefetch == MB_PREFETCH_ALL || (o.prefetch == MB_PREFETCH_AUTO && B.src_weight[i] >= 0.02);
     if (aligned && dense && B.src_weight[i] > 0) h.pf_mask |= 1u << i;
   }
+  h.nstab = 0;
   *cfg = batch_cfg(h, o);
+  batch_tables(B, o, *cfg);
   return MB_OK;
 }
 
@@ -1380,8 +1477,8 @@ static mb_status batch_staging(Engine &E, BatchHdr **out, uint32_t *slot);
 static mb_status batch_opts_check(const mb_batch_opts &o, const char *who) {
   if ((o.words_per_lane && o.words_per_lane != 1 && o.words_per_lane != 2 && o.words_per_lane != 4 &&
        o.words_per_lane != 6) ||
-      o.warps == 1 || o.warps > 16 || o.stages > 4 || o.prefetch > MB_PREFETCH_ALL ||
-      o.drain_warps >= (o.warps ? o.warps : 16u))
+      o.warps == 1 || o.warps > BW_MAX || o.stages > 4 || o.prefetch > MB_PREFETCH_ALL ||
+      o.table_kb > 227)
     return fail(MB_ERR_INVALID, "%s: options out of range", who);
   return MB_OK;
 }
@@ -1410,7 +1507,13 @@ static mb_status batch_launch(Engine &E, const mb_query *qs, const BatchPlanned 
       MB_CUDA(cudaEventRecord(E.bq_copied[slot], E.stream));
       dh = static_cast<const BatchHdr *>(E.bq_dev);
     }
-    MB_CHECK(batch_scan(h, dh, P.cfgs[i], maps, out, nq, E.stream));
+    BatchCfg c = P.cfgs[i];
+    if (E.test_stall) {
+      c.skip_stage0 = 1;
+      c.wait_tries = E.test_tries;
+      --E.test_stall;
+    }
+    MB_CHECK(batch_scan(h, dh, c, maps, out, nq, E.stream));
   }
   if (!P.alone.empty()) {
     mb_plan pl;
@@ -1482,7 +1585,8 @@ extern "C" mb_status mb_engine_batch_info(mb_engine *e, const mb_query *qs, uint
     l.copies = P.hdrs[i]->ncopy;
     l.words_per_lane = P.cfgs[i].V;
     l.warps = P.cfgs[i].warps;
-    l.drain_warps = P.cfgs[i].drainers;
+    l.table_slots = P.hdrs[i]->nstab;
+    l.chain_entries = P.hdrs[i]->nchain;
     l.stages = P.cfgs[i].stages;
   }
   if (nlaunches) *nlaunches = (uint32_t)P.hdrs.size();
@@ -1506,7 +1610,19 @@ extern "C" mb_status mb_engine_query_batch(mb_engine *e, const mb_query *qs, uin
   MB_CUDA(cudaMemcpyAsync(out_host, E.bout, total * 8, cudaMemcpyDeviceToHost, E.stream));
   if (nqual_host) MB_CUDA(cudaMemcpyAsync(nqual_host, E.bout + total, (size_t)n * 8, cudaMemcpyDeviceToHost, E.stream));
   MB_CUDA(cudaStreamSynchronize(E.stream));
-  return check_device_error(E.stream);
+  const mb_status st = check_device_error(E.stream);
+  if (st != MB_OK) {  // a launch gave up part way: its partial sums are not results
+    memset(out_host, 0, total * 8);
+    if (nqual_host) memset(nqual_host, 0, (size_t)n * 8);
+  }
+  return st;
+}
+
+extern "C" mb_status mb_engine_test_stall(mb_engine *e, uint32_t launches, uint32_t tries) {
+  if (!e) return fail(MB_ERR_INVALID, "mb_engine_test_stall: NULL engine");
+  e->E.test_stall = launches;
+  e->E.test_tries = tries;
+  return MB_OK;
 }
 
 // ------------------------------------------------------------ batch graphs
@@ -1627,7 +1743,7 @@ extern "C" mb_status mb_engine_tune_batch(mb_engine *e, const mb_query *qs, uint
     if (ms < bms) bms = ms, b = o;
     return MB_OK;
   };
-  // tile width x warps (default drain warps: about a fifth)
+  // tile width x warps
   for (uint32_t V : {6u, 4u, 2u, 1u})
     for (uint32_t w : {16u, 12u, 8u}) {
       mb_batch_opts o;
@@ -1636,11 +1752,11 @@ extern "C" mb_status mb_engine_tune_batch(mb_engine *e, const mb_query *qs, uint
       o.warps = w;
       MB_CHECK(consider(o));
     }
-  // drain warps
+  // shared group tables: as large as fits, 16 KB, 1 KB
   const mb_batch_opts b1 = b;
-  for (uint32_t d = 1; d <= 6 && d < b1.warps; ++d) {
+  for (uint32_t kb : {16u, 1u}) {
     mb_batch_opts o = b1;
-    o.drain_warps = d;
+    o.table_kb = kb;
     MB_CHECK(consider(o));
   }
   // L2 prefetch of the payload

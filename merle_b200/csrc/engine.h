@@ -132,6 +132,9 @@ struct Engine {
   // the autotuner's last launch shape, used by batches enqueued without options
   mb_batch_opts tuned{};
   bool have_tuned = false;
+  // tests of the bounded waits (mb_engine_test_stall): batched launches left
+  // to stall, and their try limit
+  uint32_t test_stall = 0, test_tries = 0;
   int64_t *bout = nullptr;  // device results of mb_engine_query_batch
   uint64_t bout_cap = 0;
   // timing: per-query event pairs of the last enqueue, and markers
@@ -155,6 +158,7 @@ struct Engine {
   mb_src ccity_src() const;
   mb_src mfgr_src() const;
   mb_status build_denorm();
+  mb_status enqueue_denorm(unsigned long long *d_bad);
 };
 
 // The op functors s1op..s4op (ssb/lambdas.cuh:19-152) of a template query as

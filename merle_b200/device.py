@@ -108,6 +108,31 @@ def bitmap_create(src: abi.mb_src, n: int, lo, hi, pop: bool = True):
     return slab.view(nb, stride), pc
 
 
+def bitmap_create_levels(src: abi.mb_src, n: int, levels, pop: bool = True):
+    """Several bin levels of one column in one pass (mb_bitmap_create_levels):
+    levels = [(lo, hi), ...]; returns [(slab [nbins x stride] words, popcounts)]
+    per level."""
+    L = lib()
+    stride = int(L.mb_bitmap_stride(n))
+    arr = (abi.mb_level * max(1, len(levels)))()
+    keep, outs = [], []
+    for i, (lo, hi) in enumerate(levels):
+        lo = np.ascontiguousarray(lo, np.uint64)
+        hi = np.ascontiguousarray(hi, np.uint64)
+        nb = len(lo)
+        slab = empty(nb * stride, 4, zero=True)
+        pc = empty(nb, 8, zero=True) if pop else None
+        keep += [lo, hi]
+        arr[i].lo = lo.ctypes.data_as(C.POINTER(C.c_uint64))
+        arr[i].hi = hi.ctypes.data_as(C.POINTER(C.c_uint64))
+        arr[i].nbins = nb
+        arr[i].out = slab.data_ptr()
+        arr[i].popcounts = pc.data_ptr() if pc is not None else None
+        outs.append((slab.view(nb, stride), pc))
+    check(L.mb_bitmap_create_levels(C.byref(src), n, arr, len(levels), stride, stream_ptr()))
+    return outs
+
+
 def vprg_grpby(prg: abi.mb_vprg, op: abi.mb_op, nr_grp: int, launch: abi.mb_launch | None = None,
                out=None, nq=None):
     L = lib()

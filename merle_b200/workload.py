@@ -120,3 +120,117 @@ def random_query(r: np.random.Generator, tmpl: int | None = None, narrow: float 
 def random_mix(seed: int, n: int, narrow: float = 0.3) -> list[abi.mb_query]:
     r = np.random.default_rng(seed)
     return [random_query(r, None, narrow) for _ in range(n)]
+
+
+# ------------------------------------------------ selectivity-spanning mix
+NDAYS, NCITY, NMFGR = 2556, 250, 1000
+
+
+def est_selectivity(q: abi.mb_query) -> float:
+    """Expected fraction of fact rows a query selects on the star schema's
+    distributions (order date uniform over 2,556 days, quantity U[1,50],
+    discount U[0,10], customer / supplier city U[0,249] and part mfgr code
+    U[0,999] per dimension row, foreign keys uniform): the product of the
+    predicates' fractions."""
+    t, p = as_tuple(q)
+
+    def frac(lo, hi, dom_lo, dom_hi):
+        return max(0, min(hi, dom_hi) - max(lo, dom_lo)) / (dom_hi - dom_lo)
+    if t == 1:
+        return frac(p[0], p[1], 0, NDAYS) * frac(p[2], p[3], 0, 11) * frac(p[4], p[5], 1, 51)
+    if t == 2:
+        return frac(p[0], p[1], 0, NMFGR) * frac(p[2], p[3], 0, NCITY)
+    if t == 3:
+        return frac(p[0], p[1], 0, NCITY) * frac(p[2], p[3], 0, NCITY) * frac(p[4], p[5], 0, NDAYS)
+    return (frac(p[0], p[1], 0, NCITY) * frac(p[2], p[3], 0, NCITY) * frac(p[4], p[5], 0, NMFGR)
+            * frac(p[6], p[7], 0, NDAYS))
+
+
+def _loguni_int(r: np.random.Generator, lo: int, hi: int) -> int:
+    """An integer in [lo, hi], log-uniformly distributed."""
+    return int(min(hi, max(lo, round(float(np.exp(r.uniform(np.log(lo), np.log(hi + 0.999))) - 0.499)))))
+
+
+def _span(r: np.random.Generator, width: int, dom: int, align: int = 1) -> tuple[int, int]:
+    """[x, x + width) inside [0, dom), x a multiple of align."""
+    x = int(r.integers(0, (dom - width) // align + 1)) * align
+    return x, x + width
+
+
+def broad_query(r: np.random.Generator, tmpl: int) -> abi.mb_query:
+    """A query of template tmpl whose range widths are drawn log-uniformly,
+    so that its selectivity can lie anywhere from the template's least to
+    the whole table.  The reference's group-index formulas stay inside their
+    group counts (its CPU code writes its output without a bound check,
+    ssb/cpuref.c:157-242): template 3 takes equally wide customer and supplier
+    ranges, aligned to nations (10 cities) when 50 or more wide (the /10
+    scaling); template 4 aligns a supplier range of 50 or more to nations and a
+    part range of 200 or more to categories (the /40 scaling), the part
+    range's scaled width at least the supplier range's."""
+    if tmpl == 1:
+        d = _span(r, _loguni_int(r, 1, NDAYS), NDAYS)
+        di = _span(r, _loguni_int(r, 1, 11), 11)
+        qw = _loguni_int(r, 1, 50)
+        q0 = int(r.integers(1, 51 - qw + 1))
+        return abi.query(1, d[0], d[1], di[0], di[1], q0, q0 + qw)
+    if tmpl == 2:
+        m = _span(r, _loguni_int(r, 1, NMFGR), NMFGR)
+        s = _span(r, _loguni_int(r, 1, NCITY), NCITY)
+        return abi.query(2, m[0], m[1], s[0], s[1])
+    if tmpl == 3:
+        w = _loguni_int(r, 1, NCITY)
+        if w >= 50:
+            w = w // 10 * 10
+            c, s = _span(r, w, NCITY, 10), _span(r, w, NCITY, 10)
+        else:
+            c, s = _span(r, w, NCITY), _span(r, w, NCITY)
+        d = _span(r, _loguni_int(r, 1, NDAYS), NDAYS)
+        return abi.query(3, c[0], c[1], s[0], s[1], d[0], d[1])
+    c = _span(r, _loguni_int(r, 1, NCITY), NCITY)
+    sw = _loguni_int(r, 1, NCITY)
+    if sw >= 50:
+        sw = sw // 10 * 10
+        s = _span(r, sw, NCITY, 10)
+        ssc = sw // 10
+    else:
+        s = _span(r, sw, NCITY)
+        ssc = sw
+    pw = max(_loguni_int(r, 1, NMFGR), ssc)
+    if pw >= 200 and max(pw // 40, ssc) * 40 > NMFGR:
+        pw = 199  # the scaled part range cannot reach the supplier range's width: stay unscaled
+    if pw >= 200:
+        pw = max(pw // 40, ssc) * 40
+        p = _span(r, pw, NMFGR, 40)
+    else:
+        p = _span(r, pw, NMFGR)
+    d = _span(r, _loguni_int(r, 1, NDAYS), NDAYS)
+    return abi.query(4, c[0], c[1], s[0], s[1], p[0], p[1], d[0], d[1])
+
+
+def span_mix(seed: int, n: int, lo: float = 1e-6, hi: float = 0.5, tries: int = 4000) -> list[abi.mb_query]:
+    """n queries of the four templates (in turn) whose expected
+    selectivities (est_selectivity) follow a log-uniform spread over
+    [lo, hi]: for each query a target drawn log-uniformly, then the closest of
+    up to `tries` broad_query draws (within 10 % ends the search).  The
+    first and last targets are lo and hi themselves, so the mix reaches both
+    ends."""
+    r = np.random.default_rng(seed)
+    targets = np.exp(r.uniform(np.log(lo), np.log(hi), n))
+    if n >= 2:
+        targets[0], targets[-1] = lo, hi
+    out = []
+    for i, tgt in enumerate(targets):
+        t = 2 if (i == n - 1 and n >= 2) else 1 + i % 4  # template 2 reaches the widest end most easily
+        best, best_err = None, np.inf
+        for _ in range(tries):
+            q = broad_query(r, t)
+            s = est_selectivity(q)
+            if s <= 0:
+                continue
+            err = abs(np.log(s / tgt))
+            if err < best_err:
+                best, best_err = q, err
+                if err < 0.1:
+                    break
+        out.append(best)
+    return out

@@ -162,7 +162,7 @@ class StarHost:
         o = object.__new__(StarHost)
         o.n, o.k, o.seed = self.n, self.k, self.seed
         nw = {"orderdate": np.uint16, "quantity": np.uint8, "discount": np.uint8, "suppcity": np.uint8}
-        o.cols = {f: a.astype(nw.get(f, np.uint32)) for f, a in self.cols.items()}
+        o.cols = {f: a.astype(nw.get(f, np.uint32), copy=False) for f, a in self.cols.items()}
         o.custcity, o.suppcity, o.partmfgr = self.custcity, self.suppcity, self.partmfgr
         return o
 
@@ -183,6 +183,64 @@ class StarHost:
                       loRevenue=ptr(s["revenue"]), loSupplyCost=ptr(s["supplycost"]),
                       loQuantity=ptr(s["quantity"]), loDiscount=ptr(s["discount"]),
                       loSuppCity=ptr(s["suppcity"]), custCity=ptr(s.custcity), partMfgr=ptr(s.partmfgr))
+
+
+def ngroups(tmpl: int, p) -> int:
+    """Group count of a template query: the size of the reference's output
+    array for it (s1ref one sum; s2ref 7 x mfgr width; s3ref a x b x years;
+    s4ref a x b x years with its /10 and /40 scalings; ssb/cpuref.c:141-242)."""
+    def years(dmin, dmax):
+        return 1 if dmax <= dmin else _year(dmax - 1) - _year(dmin) + 1
+    if tmpl == 1:
+        return 1
+    if tmpl == 2:
+        return 7 * (p[1] - p[0]) if p[1] > p[0] else 1
+    if tmpl == 3:
+        a, b = p[1] - p[0], p[3] - p[2]
+        if p[1] - p[0] >= 50:
+            a, b = p[1] // 10 - p[0] // 10, p[3] // 10 - p[2] // 10
+        return max(1, a * b * years(p[4], p[5]))
+    a, b = p[3] - p[2], p[5] - p[4]
+    if p[3] - p[2] >= 50:
+        a = p[3] // 10 - p[2] // 10
+    if p[5] - p[4] >= 200:
+        b = p[5] // 40 - p[4] // 40
+    return max(1, a * b * years(p[6], p[7]))
+
+
+def _year(d: int) -> int:
+    """ssbDateToYear (ssb/ssbdemo.h:28-39): day 0 = 1992-01-01 -> year index."""
+    return int(np.searchsorted(np.array(_YEARS[1:]), d, side="right"))
+
+
+def ref_answers(schema: "SsbSchema", n: int, qs, threads: int):
+    """Each template query through the reference's own s1ref..s4ref
+    (ssb/cpuref.c:141-242) over the first n rows of schema, one query per
+    thread on `threads` threads (ssb_cpujoin's shape, ssb/cpuref.c:244-302):
+    (answers, seconds).  An answer is the uint64 sum of s1ref, or the uint32
+    group array s2ref..s4ref fill (ngroups values)."""
+    import time
+    from concurrent.futures import ThreadPoolExecutor
+    r = ref()
+    if r is None:
+        raise RuntimeError("oracle/_ref/libcpuref.so is not built")
+
+    def one(q):
+        t = int(q.tmpl)
+        k = {1: 6, 2: 4, 3: 6, 4: 8}[t]
+        p = tuple(int(q.p[i]) for i in range(k))
+        if t == 1:
+            return np.array([r.s1ref(C.byref(schema), n, *p)], np.uint64)
+        out = np.zeros(ngroups(t, p) + 1, np.uint32)  # one spare word: nothing may land there
+        f = {2: r.s2ref, 3: r.s3ref, 4: r.s4ref}[t]
+        f(C.byref(schema), n, *p, out.ctypes.data)
+        if out[-1] != 0:
+            raise RuntimeError(f"reference wrote past its group array for {t} {p}")
+        return out[:-1]
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max(1, threads)) as ex:
+        res = list(ex.map(one, qs))
+    return res, time.perf_counter() - t0
 
 
 def star_npart(k: int) -> int:
@@ -355,30 +413,35 @@ def canonical_bins(tmpl: int, p) -> set:
     return out
 
 
-def qualifying_mask(star: "StarHost", tmpl: int, p) -> np.ndarray:
-    """Rows that satisfy every predicate of the query (numpy, vectorised)."""
-    c = star.cols
-    vals = getattr(star, "_joined", None)
-    if vals is None:
+def qualifying_mask(star: "StarHost", tmpl: int, p, nrows: int | None = None) -> np.ndarray:
+    """Rows among the first nrows (default: all) that satisfy every predicate
+    of the query (numpy, vectorised)."""
+    n = star.n if nrows is None else min(nrows, star.n)
+    cache = getattr(star, "_joined", None)
+    if cache is None or cache[0] != n:
+        c = {k: v[:n] for k, v in star.cols.items()}
         vals = {"date": c["orderdate"], "discount": c["discount"], "quantity": c["quantity"],
                 "suppcity": c["suppcity"], "custcity": star.custcity[c["custkey"]],
                 "partmfgr": star.partmfgr[c["partkey"]]}
-        star._joined = vals
-    m = np.ones(star.n, bool)
+        star._joined = cache = (n, vals)
+    vals = cache[1]
+    m = np.ones(n, bool)
     for col, a, b in PREDS[tmpl]:
         v = vals[col]
         m &= (v >= p[a]) & (v < p[b])
     return m
 
 
-def algo_bytes(star: "StarHost", scale: float, nrows: int, tmpl: int, p, ngroups: int, widths: dict) -> dict:
+def algo_bytes(star: "StarHost", scale: float, nrows: int, tmpl: int, p, ngroups: int, widths: dict,
+               sample_n: int | None = None) -> dict:
     """Plan-independent algorithmic bytes of one query over `nrows` rows:
     canonical bitmaps + the 32-byte sectors of every gathered column that hold
-    a qualifying row (counted exactly on the host sample `star`, scaled by
-    `scale`) + probed dimension arrays + the int64 group outputs."""
+    a qualifying row (counted exactly on the first sample_n rows of the host
+    table `star`, scaled by `scale`) + probed dimension arrays + the int64
+    group outputs."""
     W = (nrows + 31) // 32
     bm = canonical_bitmaps(tmpl, p) * W * 4
-    m = qualifying_mask(star, tmpl, p)
+    m = qualifying_mask(star, tmpl, p, sample_n)
     rows = np.flatnonzero(m)
     sec = 0
     for col in GATHER[tmpl]:

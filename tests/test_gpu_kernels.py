@@ -121,6 +121,65 @@ def test_bitmap_create_join(stars, orc):
     np.testing.assert_array_equal(host(got, np.uint32).reshape(1, -1)[:, :(n + 31) // 32], want)
 
 
+LEVEL_CASES = {
+    # the engine's hierarchies: years + months of a date, regions + nations of a city
+    "date": ("orderdate", [(np.array([0, 366, 731, 1096, 1461, 1827, 2192]),
+                            np.array([366, 731, 1096, 1461, 1827, 2192, 2557]))], True),
+    "city": ("suppcity", [(np.arange(0, 250, 50), np.arange(50, 300, 50)),
+                          (np.arange(0, 250, 10), np.arange(10, 260, 10))], False),
+    "quantity": ("quantity", [(np.arange(1, 51), np.arange(2, 52))], False),
+    # a level with gaps, values outside every bin, and three levels at once
+    "gaps3": ("suppcity", [([0, 3, 50, 51, 200, 240], [2, 40, 51, 52, 230, 241]),
+                           (np.arange(0, 240, 60), np.arange(60, 300, 60)),
+                           (np.arange(5, 245, 5), np.arange(10, 250, 5))], False),
+    # overlapping bins in one level: that level falls back to its own pass
+    "overlap": ("suppcity", [(np.arange(0, 250, 50), np.arange(50, 300, 50)),
+                             ([0, 10, 5], [20, 30, 250])], False),
+}
+
+
+@pytest.mark.parametrize("case", list(LEVEL_CASES))
+@pytest.mark.parametrize("n", [1, 31, 33, 4095, 4097, 100_003, 300_000])
+def test_bitmap_create_levels(stars, orc, case, n):
+    """One pass over a column builds several levels of bins: each level
+    equals its own single-level oracle pass word for word, tails zero,
+    popcounts exact."""
+    dev, ref = stars
+    colname, levels, months = LEVEL_CASES[case]
+    if months:
+        from merle_b200 import workload as WL
+        ms = np.array(WL.MONTH_START)
+        levels = levels + [(ms[:-1], ms[1:])]
+    col = ref[colname][:n]
+    s = abi.mb_src()
+    s.col, s.width = orc.ptr(col), col.dtype.itemsize
+    got = D.bitmap_create_levels(D.src_of(dev[colname]), n, levels)
+    W = (n + 31) // 32
+    for (lo, hi), (slab, pc) in zip(levels, got):
+        want, wpop = orc.bitmap_create(s, n, lo, hi)
+        gh = host(slab, np.uint32).reshape(len(lo), -1)
+        np.testing.assert_array_equal(gh[:, :W], want[:, :W], err_msg=case)
+        assert np.all(gh[:, W:] == 0)
+        np.testing.assert_array_equal(host(pc, np.uint64), wpop)
+
+
+def test_bitmap_create_levels_join(stars, orc):
+    """Regions and nations of the customer city through custkey -> custCity in
+    one pass, and keys >= dimsz give no bit."""
+    dev, ref = stars
+    n = ref.n
+    levels = [(np.arange(0, 250, 50), np.arange(50, 300, 50)), (np.arange(0, 250, 10), np.arange(10, 260, 10))]
+    for dimsz, dim_dev, dim_h in [(0, dev.custcity, ref.custcity), (1000, dev.custcity[:1000], ref.custcity[:1000])]:
+        s = abi.mb_src()
+        s.col, s.fk, s.width, s.dimsz = orc.ptr(dim_h), orc.ptr(ref["custkey"]), 1, dimsz
+        got = D.bitmap_create_levels(D.src_of(dim_dev, dev["custkey"], checked=dimsz != 0), n, levels)
+        W = (n + 31) // 32
+        for (lo, hi), (slab, pc) in zip(levels, got):
+            want, wpop = orc.bitmap_create(s, n, lo, hi)
+            np.testing.assert_array_equal(host(slab, np.uint32).reshape(len(lo), -1)[:, :W], want)
+            np.testing.assert_array_equal(host(pc, np.uint64), wpop)
+
+
 def _device_recipe(mb, dev, kind, preds, instrs, n):
     r = abi.mb_recipe()
     r.factsz = n

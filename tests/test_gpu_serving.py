@@ -159,3 +159,40 @@ def test_learned_planner_in_the_serving_loop(eng, mix, alone, mode, min_batch, r
         plans.add(info[i].plan)
     assert plans <= set(range(P.NC))
     assert st["launches"] == 60 and st["scan_launches"] == 0
+
+
+def test_device_wait_runs_out(eng, mix, alone, mb):
+    """A batched launch whose first staged tile is armed but never filled
+    (mb_engine_test_stall): the bounded wait for it runs out after a few
+    thousand tries, the kernel records the wait in the device error word and
+    returns, and the call reports MB_ERR_TIMEOUT with zeroed results; the
+    engine answers the next batch correctly.  In the server exactly the
+    requests of the stalled launch end with MB_ERR_TIMEOUT and every other
+    request is answered as alone."""
+    from merle_b200 import lib
+    qs = mix[:24]
+    lib().mb_engine_test_stall(eng.handle, 1, 4096)
+    with pytest.raises(mb.MbError) as ei:
+        eng.query_batch(qs)
+    assert ei.value.status == abi.MB_ERR_TIMEOUT and "code 1" in str(ei.value)
+    out, nq = eng.query_batch(qs)  # the stall was one launch: this one is whole
+    offs = _layout(qs)
+    for i in range(len(qs)):
+        np.testing.assert_array_equal(out[offs[i]:offs[i + 1]], alone[i][0])
+        assert nq[i] == alone[i][1]
+    # the server: every launch on the batched scan, one at a time
+    with SV.Server(eng, abi.SERVE_BATCHED, min_batch=1, max_inflight=1) as s:
+        lib().mb_engine_test_stall(eng.handle, 1, 4096)
+        out, info = s.run_load(mix, 20000.0, seed=5)
+        st = s.stats()
+    offs = _layout(mix)
+    stalled = {i.launch for i in info if i.status == abi.MB_ERR_TIMEOUT}
+    assert len(stalled) == 1, stalled
+    for i, q in enumerate(mix):
+        if info[i].launch in stalled:
+            assert info[i].status == abi.MB_ERR_TIMEOUT
+            continue
+        assert info[i].status == abi.MB_OK
+        np.testing.assert_array_equal(out[offs[i]:offs[i + 1]], alone[i][0], err_msg=str(WL.as_tuple(q)))
+        assert info[i].nqual == alone[i][1]
+    assert st["failed"] == sum(1 for i in info if i.status == abi.MB_ERR_TIMEOUT) > 0
