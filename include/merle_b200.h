@@ -521,11 +521,22 @@ typedef enum mb_plan_kind {
 } mb_plan_kind;
 
 /* Per-query plan knobs.  The arithmetic never depends on them. */
+/* How a predicate's range becomes bins (col::from_bin / from_bin2,
+ * bmpidx_create.cu:138-226, generalised). */
+typedef enum mb_cover {
+  MB_COVER_RULE = 0,     /* the fewest bitmap bytes: an exact cover on the coarsest levels that fit,
+                            the complement's, or an exact inner cover with checked edge bins */
+  MB_COVER_NOEDGE = 1,   /* exact covers (direct or complement) where one exists: no candidate checks */
+  MB_COVER_NOCOMPL = 2,  /* never the complement */
+  MB_COVER_FINE = 3      /* the finest level's bins only, never the complement */
+} mb_cover;
+
 typedef struct mb_plan {
   uint32_t kind;            /* mb_plan_kind */
   uint32_t order_mode;      /* 0: most selective predicate first; 1: template order */
   uint32_t materialise;     /* bit i: predicate i is evaluated into a bitmap first */
   mb_launch launch;         /* group-by strategy and tile shape */
+  uint32_t cover;           /* mb_cover, for every predicate */
 } mb_plan;
 
 typedef struct mb_query_stats {
@@ -621,6 +632,15 @@ MB_API mb_status mb_engine_query_batch(mb_engine *e, const mb_query *qs, uint32_
  * and exits on a launch error (ssb/lambdas.cuh:233-234). */
 MB_API mb_status mb_engine_test_stall(mb_engine *e, uint32_t launches, uint32_t tries);
 
+/* The batch with one plan per query: a fused plan (MB_PLAN_FUSED) puts its
+ * query in the batched scan with the plan's cover (mb_cover) and predicate
+ * order; any other kind runs the query alone on the plain path with that
+ * plan.  Results as mb_engine_enqueue_batch.  No counterpart in the
+ * reference (its queries run one at a time, ssb/lambdas.cuh:154-243). */
+MB_API mb_status mb_engine_enqueue_batch_plans(mb_engine *e, const mb_query *qs, const mb_plan *plans,
+                                               uint32_t n, const mb_batch_opts *opts, int64_t *out_dev,
+                                               uint64_t *nqual_dev);
+
 /* The launches a batch takes, planned on the host without GPU work: per
  * batched launch its queries, the bitmap rows it stages per tile, its
  * staging copies and its launch shape; *nalone = queries outside the batch
@@ -643,6 +663,10 @@ typedef struct mb_batch_graph mb_batch_graph;
 MB_API mb_status mb_batch_graph_create(mb_engine *e, const mb_query *qs, uint32_t n,
                                        const mb_batch_opts *opts, int64_t *out_dev,
                                        uint64_t *nqual_dev, mb_batch_graph **out);
+/* The same with one plan per query (as mb_engine_enqueue_batch_plans). */
+MB_API mb_status mb_batch_graph_create_plans(mb_engine *e, const mb_query *qs, const mb_plan *plans,
+                                             uint32_t n, const mb_batch_opts *opts, int64_t *out_dev,
+                                             uint64_t *nqual_dev, mb_batch_graph **out);
 MB_API mb_status mb_batch_graph_launch(mb_batch_graph *g);
 MB_API mb_status mb_batch_graph_destroy(mb_batch_graph *g);
 
@@ -718,6 +742,30 @@ MB_API mb_status mb_engine_set_planner(mb_engine *e, mb_mlp *m);
  * index (may be NULL).  Without a network: the rule plan. */
 MB_API mb_status mb_engine_plan_learned(mb_engine *e, const mb_query *qs, uint32_t n, mb_plan *plans,
                                         uint32_t *chosen);
+
+/* The learned batch planner.  The reference plans every query alone with the
+ * fixed rules of col::from_bin / from_bin2 (bmpidx_create.cu:138-226) and
+ * runs it with a fixed launch shape (ssb/lambdas.cuh:13-15); a batch here is
+ * planned as a whole: a second network of the mb_mlp kind maps
+ * MB_BATCH_FEATURES features of a batch (planned with the rule, on the host)
+ * to the predicted log device time of each of MB_BATCH_CANDIDATES batch plans
+ * - a launch shape (words per lane in {1, 2, 4} x warps per CTA in {8, 12,
+ * 16}) and the cover all its queries take (MB_COVER_RULE or
+ * MB_COVER_NOEDGE): candidate c = cover * 9 + (V index * 3 + warps index).
+ * Plans never change the arithmetic. */
+#define MB_BATCH_FEATURES 32
+#define MB_BATCH_CANDIDATES 18
+MB_API mb_status mb_engine_batch_features(mb_engine *e, const mb_query *qs, uint32_t n, float *features);
+/* The options and cover of batch candidate idx. */
+MB_API mb_status mb_engine_batch_candidate(uint32_t idx, mb_batch_opts *opts, uint32_t *cover);
+/* Sets (or clears, m = NULL) the batch planner network, borrowed: batches
+ * enqueued without options then take its plan (the server's scan launches
+ * among them).  The network must map MB_BATCH_FEATURES to MB_BATCH_CANDIDATES. */
+MB_API mb_status mb_engine_set_batch_planner(mb_engine *e, mb_mlp *m);
+/* The batch plan the planner picks (without a network: zero options, the
+ * rule cover, *choice = 0xffffffff). */
+MB_API mb_status mb_engine_plan_batch(mb_engine *e, const mb_query *qs, uint32_t n, mb_batch_opts *opts,
+                                      uint32_t *cover, uint32_t *choice);
 
 /* ------------------------------------------------------------------------
  * Serving loop.  No counterpart in the reference (its drivers run a fixed

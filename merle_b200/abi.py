@@ -139,10 +139,15 @@ class mb_batch_launch_info(C.Structure):
 
 class mb_plan(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("order_mode", C.c_uint32), ("materialise", C.c_uint32),
-                ("launch", mb_launch)]
+                ("launch", mb_launch), ("cover", C.c_uint32)]
+
+
+COVER_RULE, COVER_NOEDGE, COVER_NOCOMPL, COVER_FINE = range(4)
 
 
 MB_PLAN_FEATURES = 32
+MB_BATCH_FEATURES = 32
+MB_BATCH_CANDIDATES = 18
 MB_PLAN_CANDIDATES = 16
 
 
@@ -205,6 +210,12 @@ SIGNATURES: dict[str, tuple] = {
                                VOIDP, VOIDP]),
     "mb_bitmap_create_levels": (I32, [C.POINTER(mb_src), U64, C.POINTER(mb_level), U32, U64, VOIDP]),
     "mb_engine_test_stall": (I32, [VOIDP, U32, U32]),
+    "mb_engine_enqueue_batch_plans": (I32, [VOIDP, VOIDP, VOIDP, U32, VOIDP, VOIDP, VOIDP]),
+    "mb_engine_batch_features": (I32, [VOIDP, VOIDP, U32, VOIDP]),
+    "mb_engine_batch_candidate": (I32, [U32, VOIDP, VOIDP]),
+    "mb_engine_set_batch_planner": (I32, [VOIDP, VOIDP]),
+    "mb_engine_plan_batch": (I32, [VOIDP, VOIDP, U32, VOIDP, VOIDP, VOIDP]),
+    "mb_batch_graph_create_plans": (I32, [VOIDP, VOIDP, VOIDP, U32, VOIDP, VOIDP, VOIDP, VOIDP]),
     "mb_vprg_eval": (I32, [C.POINTER(mb_vprg), I32, VOIDP, VOIDP, VOIDP, VOIDP]),
     "mb_bitmap_to_rows": (I32, [VOIDP, VOIDP, U64, VOIDP, VOIDP, VOIDP]),
     "mb_bitmap_to_rows_noalloc": (I32, [VOIDP, VOIDP, U64, VOIDP, VOIDP, VOIDP]),

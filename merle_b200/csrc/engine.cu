@@ -305,13 +305,15 @@ static const uint32_t *bin_ptr(const Level &L, int j, uint64_t stride) {
   return L.slab + (uint64_t)j * stride;
 }
 
-// Exact cover of [lo, hi) with the coarsest bins that fit (levels nest).
+// Exact cover of [lo, hi) with the coarsest bins that fit (levels nest);
+// with fine_only, with the finest level's bins alone.
 static bool exact_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t stride,
-                        std::vector<const uint32_t *> &out, uint64_t &rows) {
+                        std::vector<const uint32_t *> &out, uint64_t &rows, bool fine_only = false) {
   uint64_t x = lo;
   while (x < hi) {
     bool found = false;
-    for (const Level &L : c.levels) {
+    for (size_t li = fine_only ? c.levels.size() - 1 : 0; li < c.levels.size(); ++li) {
+      const Level &L = c.levels[li];
       int j = bin_at(L, x);
       if (j >= 0 && L.bounds[j + 1] <= hi) {
         out.push_back(bin_ptr(L, j, stride));
@@ -326,7 +328,9 @@ static bool exact_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t stri
   return true;
 }
 
-Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t stride, int nchk_sources, uint64_t *cost_out) {
+Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t stride, int nchk_sources, uint64_t *cost_out,
+                 uint32_t mode) {
+  const bool fine = mode == MB_COVER_FINE, nocompl = mode == MB_COVER_NOCOMPL || fine, noedge = mode == MB_COVER_NOEDGE;
   Cover best;
   if (cost_out) *cost_out = 0;
   lo = std::max(lo, c.dom_lo);
@@ -344,13 +348,13 @@ Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t stride, int
   // (a) exact direct cover
   {
     Cover cv;
-    if (exact_cover(c, lo, hi, stride, cv.mid, cv.est_rows)) {
+    if (exact_cover(c, lo, hi, stride, cv.mid, cv.est_rows, fine)) {
       uint64_t cost = (uint64_t)cv.nb() * W * 4;
       if (cost < best_cost) best = cv, best_cost = cost;
     }
   }
   // (b) complement: NOT of the exact cover of [dom_lo, lo) u [hi, dom_hi)
-  {
+  if (!nocompl) {
     Cover cv;
     uint64_t rows = 0;
     bool ok = true;
@@ -390,12 +394,14 @@ Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t stride, int
           cv.right = bin_ptr(F, r, stride);
           cv.edge_rows += F.pop.empty() ? 0 : F.pop[r];
         }
-        if (ilo < ihi) ok = exact_cover(c, ilo, ihi, stride, cv.mid, cv.est_rows);
+        if (ilo < ihi) ok = exact_cover(c, ilo, ihi, stride, cv.mid, cv.est_rows, fine);
       }
       if (ok && cv.nb() > 0) {
         // the check gathers ~one 32-byte sector per filter source per edge row
         uint64_t cost = (uint64_t)cv.nb() * W * 4 + cv.edge_rows * 32ull * (uint64_t)nchk_sources;
         cv.est_rows += cv.edge_rows / 2;
+        // without candidate checks, edges only where no exact cover exists
+        if (noedge && best_cost != UINT64_MAX) cost = UINT64_MAX;
         if (cost < best_cost) best = cv, best_cost = cost;
       }
     }
@@ -566,6 +572,7 @@ mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered
   if (q.tmpl < 1 || q.tmpl > 4) return fail(MB_ERR_INVALID, "query: template %u not in 1..4", q.tmpl);
   if (!E.indexed) return fail(MB_ERR_INVALID, "query: the engine has no index (mb_engine_build_index)");
   if (plan.kind > MB_PLAN_HASH) return fail(MB_ERR_INVALID, "query: plan kind %u", plan.kind);
+  if (plan.cover > MB_COVER_FINE) return fail(MB_ERR_INVALID, "query: cover mode %u", plan.cover);
   L.reset();
   L.ngroups = query_ngroups(q);
   build_op(E, q, L.op, plan.kind == MB_PLAN_HASH);
@@ -574,7 +581,9 @@ mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered
   L.covers.resize(L.preds.size());
   for (size_t i = 0; i < L.preds.size(); ++i) {
     const Pred &pr = L.preds[i];
-    L.covers[i] = plan_cover(E.idx[pr.col], pr.lo, pr.hi, E.stride, nchk);
+    L.covers[i] = plan_cover(E.idx[pr.col], pr.lo, pr.hi, E.stride, nchk, nullptr, plan.cover);
+    if (plan.cover != MB_COVER_RULE && L.covers[i].mid.size() > MB_MAXBINS)  // over the limit: the rule's cover
+      L.covers[i] = plan_cover(E.idx[pr.col], pr.lo, pr.hi, E.stride, nchk);
     if (L.covers[i].empty) L.empty = true;
     if (stats) {
       // plan-independent canonical count: the fewer of direct and complement exact covers
@@ -1407,13 +1416,22 @@ struct BatchPlanned {
   std::vector<std::unique_ptr<BatchHdr>> hdrs;
   std::vector<BatchCfg> cfgs;
   std::vector<uint32_t> alone;
+  std::vector<mb_plan> alone_plan;  // the plan each query of `alone` runs with
+  std::vector<double> sel;          // per query: estimated selected-row fraction (rule covers)
+  std::vector<uint8_t> chk;         // per query: its covers have edge bins (uncertain rows)
   std::vector<uint64_t> offs;
   uint64_t total = 0;
 };
 
-static mb_status batch_plan(Engine &E, const mb_query *qs, uint32_t n, const mb_batch_opts &o, BatchPlanned &P) {
+// plans (optional, one per query): a fused plan puts its query in the batch
+// with the plan's cover and order; any other kind runs the query alone on the
+// plain path with that plan.  Without plans every query takes the rule plan.
+static mb_status batch_plan(Engine &E, const mb_query *qs, uint32_t n, const mb_batch_opts &o, BatchPlanned &P,
+                            const mb_plan *plans = nullptr) {
   P.offs.resize(n);
   P.total = mb_queries_layout(qs, n, P.offs.data());
+  P.sel.assign(n, 0.0);
+  P.chk.assign(n, 0);
   mb_plan pl;  // the rule plan
   memset(&pl, 0, sizeof(pl));
   pl.kind = MB_PLAN_FUSED;
@@ -1440,18 +1458,29 @@ static mb_status batch_plan(Engine &E, const mb_query *qs, uint32_t n, const mb_
   Lowered L;
   DevPrg D;
   for (uint32_t i = 0; i < n; ++i) {
-    MB_CHECK(lower_query(E, qs[i], pl, L));
+    const mb_plan &qp = plans ? plans[i] : pl;
+    if (qp.kind != MB_PLAN_FUSED) {
+      P.alone.push_back(i);
+      P.alone_plan.push_back(qp);
+      continue;
+    }
+    mb_plan bp = pl;  // in the batch: the query's cover and predicate order
+    bp.cover = qp.cover;
+    bp.order_mode = qp.order_mode;
+    MB_CHECK(lower_query(E, qs[i], bp, L));
     if (L.empty) continue;  // outputs stay zero
     bool v4 = false;
     MB_CHECK(flatten_prg(&L.prg, L.chk ? 1 : 0, &D, &v4));
     const double sel = est_selectivity(E, L);
+    P.sel[i] = sel;
+    P.chk[i] = L.chk ? 1 : 0;
     int r = batch_add(B, L, D, P.offs[i], i, sel);
     if (r == BADD_FULL) {
       MB_CHECK(close());
       MB_CHECK(fresh());
       r = batch_add(B, L, D, P.offs[i], i, sel);
     }
-    if (r != BADD_OK) P.alone.push_back(i);
+    if (r != BADD_OK) P.alone.push_back(i), P.alone_plan.push_back(pl);
   }
   return close();
 }
@@ -1516,12 +1545,10 @@ static mb_status batch_launch(Engine &E, const mb_query *qs, const BatchPlanned 
     MB_CHECK(batch_scan(h, dh, c, maps, out, nq, E.stream));
   }
   if (!P.alone.empty()) {
-    mb_plan pl;
-    memset(&pl, 0, sizeof(pl));
-    pl.kind = MB_PLAN_FUSED;
-    pl.launch.grp_strategy = MB_GRP_AUTO;
     Lowered L;
-    for (uint32_t i : P.alone) {
+    for (size_t k = 0; k < P.alone.size(); ++k) {
+      const uint32_t i = P.alone[k];
+      const mb_plan &pl = P.alone_plan[k];
       MB_CHECK(lower_query(E, qs[i], pl, L));
       MB_CHECK(run_lowered(E, L, pl, out + P.offs[i], nq + i, false));
     }
@@ -1548,6 +1575,11 @@ static mb_status batch_staging(Engine &E, BatchHdr **out, uint32_t *slot) {
 
 }  // namespace mb
 
+namespace mb {
+static mb_status batch_plan_learned(Engine &E, const mb_query *qs, uint32_t n, mb_batch_opts &o, uint32_t &cover,
+                                    uint32_t &choice);
+}
+
 extern "C" mb_status mb_engine_enqueue_batch(mb_engine *e, const mb_query *qs, uint32_t n, const mb_batch_opts *opts,
                                              int64_t *out_dev, uint64_t *nqual_dev) {
   NvtxRange nvtx_("mb_engine_enqueue_batch");
@@ -1555,12 +1587,41 @@ extern "C" mb_status mb_engine_enqueue_batch(mb_engine *e, const mb_query *qs, u
   Engine &E = e->E;
   MB_CUDA(cudaSetDevice(E.device));
   mb_batch_opts o;
-  if (opts) o = *opts;
-  else if (E.have_tuned) o = E.tuned;  // the autotuner's last choice
-  else memset(&o, 0, sizeof(o));
+  std::vector<mb_plan> plans;
+  if (opts) {
+    o = *opts;
+  } else if (E.batch_planner) {  // the learned batch plan: launch shape and covers
+    uint32_t cover = 0, choice = 0;
+    MB_CHECK(batch_plan_learned(E, qs, n, o, cover, choice));
+    plans.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+      MB_CHECK(mb_engine_plan_rule(e, &qs[i], &plans[i]));
+      plans[i].cover = cover;
+    }
+  } else if (E.have_tuned) {
+    o = E.tuned;  // the autotuner's last choice
+  } else {
+    memset(&o, 0, sizeof(o));
+  }
   MB_CHECK(batch_opts_check(o, "mb_engine_enqueue_batch"));
   BatchPlanned P;
-  MB_CHECK(batch_plan(E, qs, n, o, P));
+  MB_CHECK(batch_plan(E, qs, n, o, P, plans.empty() ? nullptr : plans.data()));
+  return batch_launch(E, qs, P, out_dev, nqual_dev, n, nullptr);
+}
+
+extern "C" mb_status mb_engine_enqueue_batch_plans(mb_engine *e, const mb_query *qs, const mb_plan *plans, uint32_t n,
+                                                   const mb_batch_opts *opts, int64_t *out_dev, uint64_t *nqual_dev) {
+  NvtxRange nvtx_("mb_engine_enqueue_batch_plans");
+  if (!e || (!qs && n) || !out_dev || !nqual_dev) return fail(MB_ERR_INVALID, "mb_engine_enqueue_batch_plans: NULL argument");
+  Engine &E = e->E;
+  MB_CUDA(cudaSetDevice(E.device));
+  mb_batch_opts o;
+  if (opts) o = *opts;
+  else if (E.have_tuned) o = E.tuned;
+  else memset(&o, 0, sizeof(o));
+  MB_CHECK(batch_opts_check(o, "mb_engine_enqueue_batch_plans"));
+  BatchPlanned P;
+  MB_CHECK(batch_plan(E, qs, n, o, P, plans));
   return batch_launch(E, qs, P, out_dev, nqual_dev, n, nullptr);
 }
 
@@ -1646,6 +1707,12 @@ extern "C" mb_status mb_batch_graph_destroy(mb_batch_graph *g) {
 
 extern "C" mb_status mb_batch_graph_create(mb_engine *e, const mb_query *qs, uint32_t n, const mb_batch_opts *opts,
                                            int64_t *out_dev, uint64_t *nqual_dev, mb_batch_graph **out) {
+  return mb_batch_graph_create_plans(e, qs, nullptr, n, opts, out_dev, nqual_dev, out);
+}
+
+extern "C" mb_status mb_batch_graph_create_plans(mb_engine *e, const mb_query *qs, const mb_plan *plans, uint32_t n,
+                                                 const mb_batch_opts *opts, int64_t *out_dev, uint64_t *nqual_dev,
+                                                 mb_batch_graph **out) {
   if (!e || (!qs && n) || !out_dev || !nqual_dev || !out) return fail(MB_ERR_INVALID, "mb_batch_graph_create: NULL argument");
   *out = nullptr;
   Engine &E = e->E;
@@ -1656,7 +1723,7 @@ extern "C" mb_status mb_batch_graph_create(mb_engine *e, const mb_query *qs, uin
   else memset(&o, 0, sizeof(o));
   MB_CHECK(batch_opts_check(o, "mb_batch_graph_create"));
   BatchPlanned P;
-  MB_CHECK(batch_plan(E, qs, n, o, P));
+  MB_CHECK(batch_plan(E, qs, n, o, P, plans));
   std::unique_ptr<mb_batch_graph, mb_status (*)(mb_batch_graph *)> G(new mb_batch_graph(), mb_batch_graph_destroy);
   G->e = e;
   const size_t nh = P.hdrs.size();
@@ -1989,3 +2056,131 @@ extern "C" mb_status mb_engine_plan_learned(mb_engine *e, const mb_query *qs, ui
   }
   return MB_OK;
 }
+
+// ------------------------------------------------------------ learned batch planner
+// A batch plan: the launch shape (words per lane x warps per CTA) and the
+// cover every query of the batch takes.  Candidate c = cover * 9 + shape,
+// shape = V index * 3 + warps index, V in {1, 2, 4}, warps in {8, 12, 16},
+// cover in {MB_COVER_RULE, MB_COVER_NOEDGE}.
+namespace mb {
+static void batch_candidate_of(uint32_t idx, mb_batch_opts &o, uint32_t &cover) {
+  static const uint32_t Vs[3] = {1, 2, 4}, Ws[3] = {8, 12, 16};
+  memset(&o, 0, sizeof(o));
+  const uint32_t shape = idx % 9;
+  o.words_per_lane = Vs[shape / 3];
+  o.warps = Ws[shape % 3];
+  cover = idx / 9 == 0 ? MB_COVER_RULE : MB_COVER_NOEDGE;
+}
+
+// Features of a batch (planned with the rule, on the host): its size, the
+// bitmaps it stages and reads per word, the stages each tile width leaves, its
+// queries' estimated selectivities, group counts and templates.  The table
+// size is left out, as for the single-query planner: the network is trained
+// at one size and plans at another.
+static mb_status batch_features_of(Engine &E, const mb_query *qs, uint32_t n, float *f) {
+  memset(f, 0, MB_BATCH_FEATURES * sizeof(float));
+  mb_batch_opts o;
+  memset(&o, 0, sizeof(o));
+  BatchPlanned P;
+  MB_CHECK(batch_plan(E, qs, n, o, P));
+  uint32_t staged = 0, nchain = 0, nconj = 0, nstab = 0;
+  for (auto &h : P.hdrs) staged += h->nu, nchain += h->nchain, nconj += h->nconj, nstab += h->nstab;
+  double ssel = 0, msel = 0, sg = 0, mg = 0, nmulti = 0, n3 = 0, n2 = 0, n1 = 0, nchk = 0;
+  uint32_t tm[4] = {0, 0, 0, 0};
+  for (uint32_t i = 0; i < n; ++i) {
+    const double sl = P.sel[i];
+    ssel += sl, msel = std::max(msel, sl);
+    n3 += sl > 1e-3, n2 += sl > 1e-2, n1 += sl > 1e-1;
+    const uint32_t ng = query_ngroups(qs[i]);
+    sg += ng, mg = std::max<double>(mg, ng), nmulti += ng > 1;
+    nchk += P.chk[i];
+    if (qs[i].tmpl >= 1 && qs[i].tmpl <= 4) ++tm[qs[i].tmpl - 1];
+  }
+  const float fn = (float)std::max<uint32_t>(1, n);
+  f[0] = log2f(1.f + (float)n) / 8.f;
+  f[1] = (float)P.hdrs.size() / 4.f;
+  f[2] = (float)P.alone.size() / fn;
+  f[3] = (float)staged / 256.f;
+  f[4] = log2f(1.f + (float)nchain) / 12.f;
+  f[5] = log2f(1.f + (float)nconj) / 10.f;
+  if (!P.hdrs.empty()) {
+    const BatchHdr &h = *P.hdrs[0];
+    static const uint32_t Vs[3] = {1, 2, 4};
+    for (int k = 0; k < 3; ++k) {
+      mb_batch_opts ov;
+      memset(&ov, 0, sizeof(ov));
+      ov.words_per_lane = Vs[k];
+      const BatchCfg c = batch_cfg(h, ov);
+      f[6 + k] = (float)c.stages / 4.f;
+    }
+  }
+  f[9] = nlog10(ssel, 1e-7, 7.0);
+  f[10] = nlog10(msel, 1e-7, 7.0);
+  f[11] = (float)(n3 / fn), f[12] = (float)(n2 / fn), f[13] = (float)(n1 / fn);
+  f[14] = log2f(1.f + (float)(ssel * 1024.0)) / 12.f;  // selected rows per 1024-row tile
+  f[15] = log2f(1.f + (float)sg) / 16.f;
+  f[16] = log2f(1.f + (float)mg) / 16.f;
+  f[17] = (float)(nmulti / fn);
+  for (int t = 0; t < 4; ++t) f[18 + t] = (float)tm[t] / fn;
+  f[22] = (float)nstab / 6144.f;
+  f[23] = (float)(nchk / fn);
+  f[24] = (float)nchain / fn / 64.f;  // bitmaps a query reads per word
+  f[31] = 1.f;
+  return MB_OK;
+}
+
+// The learned batch plan of a query batch (the planner network's argmin),
+// or the default (rule covers, the engine's launch shape) without a network.
+static mb_status batch_plan_learned(Engine &E, const mb_query *qs, uint32_t n, mb_batch_opts &o, uint32_t &cover,
+                                    uint32_t &choice) {
+  memset(&o, 0, sizeof(o));
+  cover = MB_COVER_RULE;
+  choice = 0xffffffffu;
+  if (!E.batch_planner || n == 0) return MB_OK;
+  float x[MB_BATCH_FEATURES], y[MB_BATCH_CANDIDATES];
+  MB_CHECK(batch_features_of(E, qs, n, x));
+  MB_CHECK(mb_mlp_forward(E.batch_planner, x, 1, 1, y));
+  uint32_t best = 0;
+  for (uint32_t c = 1; c < MB_BATCH_CANDIDATES; ++c)
+    if (y[c] < y[best]) best = c;
+  batch_candidate_of(best, o, cover);
+  choice = best;
+  return MB_OK;
+}
+}  // namespace mb
+
+extern "C" mb_status mb_engine_batch_features(mb_engine *e, const mb_query *qs, uint32_t n, float *features) {
+  if (!e || (!qs && n) || !features) return fail(MB_ERR_INVALID, "mb_engine_batch_features: NULL argument");
+  MB_CUDA(cudaSetDevice(e->E.device));
+  return batch_features_of(e->E, qs, n, features);
+}
+
+extern "C" mb_status mb_engine_batch_candidate(uint32_t idx, mb_batch_opts *opts, uint32_t *cover) {
+  if (!opts || !cover || idx >= MB_BATCH_CANDIDATES) return fail(MB_ERR_INVALID, "mb_engine_batch_candidate: bad argument");
+  batch_candidate_of(idx, *opts, *cover);
+  return MB_OK;
+}
+
+extern "C" mb_status mb_engine_set_batch_planner(mb_engine *e, mb_mlp *m) {
+  if (!e) return fail(MB_ERR_INVALID, "mb_engine_set_batch_planner: NULL engine");
+  if (m) {
+    uint32_t in = 0, out = 0;
+    if (!mlp_shape(m, &in, &out) || in != MB_BATCH_FEATURES || out != MB_BATCH_CANDIDATES)
+      return fail(MB_ERR_INVALID, "mb_engine_set_batch_planner: the network maps %u features to %u outputs, not %u to %u",
+                  in, out, MB_BATCH_FEATURES, MB_BATCH_CANDIDATES);
+  }
+  e->E.batch_planner = m;
+  return MB_OK;
+}
+
+extern "C" mb_status mb_engine_plan_batch(mb_engine *e, const mb_query *qs, uint32_t n, mb_batch_opts *opts,
+                                          uint32_t *cover, uint32_t *choice) {
+  if (!e || (!qs && n) || !opts) return fail(MB_ERR_INVALID, "mb_engine_plan_batch: NULL argument");
+  MB_CUDA(cudaSetDevice(e->E.device));
+  uint32_t cv = 0, ch = 0;
+  MB_CHECK(batch_plan_learned(e->E, qs, n, *opts, cv, ch));
+  if (cover) *cover = cv;
+  if (choice) *choice = ch;
+  return MB_OK;
+}
+

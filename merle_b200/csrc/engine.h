@@ -123,6 +123,7 @@ struct Engine {
   // queries in flight on the engine stream
   cudaStream_t pstream = nullptr;
   mb_mlp *planner = nullptr;             // borrowed (mb_engine_set_planner)
+  mb_mlp *batch_planner = nullptr;       // borrowed (mb_engine_set_batch_planner)
   // batch descriptors: a ring of pinned host staging headers (each reusable
   // once its copy event completed) and the device copy
   static constexpr int BQ_RING = 4;
@@ -174,7 +175,8 @@ bool mlp_shape(const mb_mlp *m, uint32_t *in, uint32_t *out);
 // Planner and lowering (engine.cu).
 // The cheapest cover of [lo, hi) with c's levels; *cost_out (if given) = its
 // cost in bytes (bitmap bytes + candidate-check sectors of its edge rows).
-Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t W, int nchk_sources, uint64_t *cost_out = nullptr);
+Cover plan_cover(const IdxCol &c, uint64_t lo, uint64_t hi, uint64_t W, int nchk_sources, uint64_t *cost_out = nullptr,
+                 uint32_t mode = MB_COVER_RULE);
 // stats: also count the plan-independent canonical bitmaps (query stats only)
 mb_status lower_query(Engine &E, const mb_query &q, const mb_plan &plan, Lowered &L, bool stats = false);
 uint32_t query_ngroups(const mb_query &q);

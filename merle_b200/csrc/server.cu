@@ -387,7 +387,13 @@ bool mb_server::launch_some(std::unique_lock<std::mutex> &lk) {
   if (s == MB_OK) {
     if (o.mode == MB_SERVE_PLAIN) s = mb_engine_enqueue(eng, qs.data(), 1, &take[0]->plan, out_dev, nq_dev, 0);
     else if (!L->scan) s = mb_engine_enqueue(eng, qs.data(), n, learned ? lplan : nullptr, out_dev, nq_dev, 0);
-    else s = mb_engine_enqueue_batch(eng, qs.data(), n, &o.batch, out_dev, nq_dev);
+    else {
+      // the server's batch options, or, left all zero with a batch planner on
+      // the engine, the learned batch plan of this launch's queries
+      static const mb_batch_opts zero = {};
+      const bool learned_batch = eng->E.batch_planner && memcmp(&o.batch, &zero, sizeof(zero)) == 0;
+      s = mb_engine_enqueue_batch(eng, qs.data(), n, learned_batch ? nullptr : &o.batch, out_dev, nq_dev);
+    }
   }
   if (s == MB_OK && cudaMemcpyAsync(mirror + off, arena + off, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
     s = fail(MB_ERR_CUDA, "serving: result copy");

@@ -115,9 +115,10 @@ class MLP:
         at path, the shape and training log as JSON at path + '.json'."""
         path = Path(path)
         self.get_params().astype("<f4").tofile(path)
+        names = BATCH_CANDIDATE_NAMES if self.nout == abi.MB_BATCH_CANDIDATES else CANDIDATE_NAMES
         path.with_name(path.name + ".json").write_text(json.dumps(
             {"in": self.nin, "hidden": self.hidden, "out": self.nout, "nparams": self.nparams(),
-             "candidates": CANDIDATE_NAMES, "log": self.log}, indent=1))
+             "candidates": names, "log": self.log}, indent=1))
 
     @classmethod
     def load(cls, path: str | Path, device: int = 0) -> "MLP":
@@ -300,6 +301,170 @@ def experiment(train_rows: int, train_queries: int, eval_rows: int, eval_queries
     return rep
 
 
+# ------------------------------------------------------------ batch planner
+# A batch plan: a launch shape of the batched scan and the cover all the
+# batch's queries take (mb_engine_batch_candidate).  The network maps
+# MB_BATCH_FEATURES features of a batch to the log time of each plan relative
+# to the batch's best; its training data are device times of CUDA-graph
+# replays of every plan on random batches, recorded by the engine.
+NBF = abi.MB_BATCH_FEATURES
+NBC = abi.MB_BATCH_CANDIDATES
+BATCH_CANDIDATE_NAMES = [f"{cov}/V{v}w{w}" for cov in ("rule", "noedge") for v in (1, 2, 4) for w in (8, 12, 16)]
+
+
+def batch_features(eng, qs) -> np.ndarray:
+    qarr = (abi.mb_query * max(1, len(qs)))(*qs)
+    f = np.zeros(NBF, np.float32)
+    check(lib().mb_engine_batch_features(eng.handle, qarr, len(qs), f.ctypes.data))
+    return f
+
+
+def batch_candidate(idx: int) -> tuple[abi.mb_batch_opts, int]:
+    o = abi.mb_batch_opts()
+    cover = C.c_uint32(0)
+    check(lib().mb_engine_batch_candidate(idx, C.byref(o), C.byref(cover)))
+    return o, int(cover.value)
+
+
+def _rule_plans(qs, cover: int = 0):
+    ps = []
+    for _ in qs:
+        p = abi.mb_plan()
+        p.kind = abi.PLAN_FUSED
+        p.cover = cover
+        ps.append(p)
+    return ps
+
+
+def time_batch(eng, qs, opts, cover: int = 0, reps: int = 3, want: np.ndarray | None = None) -> float:
+    """Median device time (ms) of `reps` CUDA-graph replays of the batch
+    under (opts, cover); with `want`, the results must equal it."""
+    import torch
+    L = lib()
+    n = len(qs)
+    qarr = (abi.mb_query * n)(*qs)
+    parr = (abi.mb_plan * n)(*_rule_plans(qs, cover))
+    tot = int(L.mb_queries_layout(qarr, n, None))
+    out = torch.zeros(max(tot, 1), dtype=torch.int64, device="cuda")
+    nq = torch.zeros(n, dtype=torch.int64, device="cuda")
+    g = C.c_void_p()
+    check(L.mb_batch_graph_create_plans(eng.handle, qarr, parr, n, C.byref(opts) if opts is not None else None,
+                                        out.data_ptr(), nq.data_ptr(), C.byref(g)))
+    ts = []
+    try:
+        for _ in range(reps):
+            check(L.mb_engine_mark(eng.handle, 6))
+            check(L.mb_batch_graph_launch(g))
+            check(L.mb_engine_mark(eng.handle, 7))
+            ms = C.c_float(0)
+            check(L.mb_engine_marks_ms(eng.handle, 6, 7, C.byref(ms)))
+            ts.append(ms.value)
+    finally:
+        check(L.mb_batch_graph_destroy(g))
+    if want is not None and not np.array_equal(out.cpu().numpy()[:tot], want):
+        raise AssertionError("a batch plan changed the results")
+    return float(np.median(ts))
+
+
+def batch_results(eng, qs) -> np.ndarray:
+    out, _ = eng.query_batch(qs, abi.mb_batch_opts())
+    return out
+
+
+def measure_batch_candidates(eng, batches, reps: int = 3, check_results: bool = True) -> np.ndarray:
+    """times[b, c]: device time (ms) of batch b under batch plan c."""
+    T = np.zeros((len(batches), NBC), np.float64)
+    for b, qs in enumerate(batches):
+        want = batch_results(eng, qs) if check_results else None
+        for c in range(NBC):
+            o, cover = batch_candidate(c)
+            T[b, c] = time_batch(eng, qs, o, cover, reps, want)
+    return T
+
+
+def random_batches(seed: int, count: int, sizes=(2, 4, 8, 16, 24, 32, 48, 64, 96, 128)):
+    """Batches of seeded template queries: selectivity-spanning mixes of
+    varied size and spread, and level-based mixes."""
+    from .workload import random_mix, span_mix
+    r = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(r.choice(sizes))
+        if r.random() < 0.7:
+            lo = float(10 ** r.uniform(-6.5, -3))
+            hi = float(10 ** r.uniform(np.log10(lo) + 1, np.log10(0.5)))
+            out.append(span_mix(int(r.integers(1 << 30)), n, lo, hi, tries=400))
+        else:
+            out.append(random_mix(int(r.integers(1 << 30)), n, float(r.choice([0.1, 0.3, 0.6]))))
+    return out
+
+
+def plan_batches_learned(eng, batches, mlp: "MLP | None") -> np.ndarray:
+    """The engine's learned choice (candidate index) for each batch."""
+    L = lib()
+    check(L.mb_engine_set_batch_planner(eng.handle, mlp.handle if mlp is not None else None))
+    ch = np.zeros(len(batches), np.int64)
+    try:
+        for b, qs in enumerate(batches):
+            qarr = (abi.mb_query * len(qs))(*qs)
+            o = abi.mb_batch_opts()
+            cover, choice = C.c_uint32(0), C.c_uint32(0)
+            check(L.mb_engine_plan_batch(eng.handle, qarr, len(qs), C.byref(o), C.byref(cover), C.byref(choice)))
+            ch[b] = choice.value
+    finally:
+        check(L.mb_engine_set_batch_planner(eng.handle, None))
+    return ch
+
+
+def batch_regret_report(T: np.ndarray, chosen: np.ndarray, t_rule: np.ndarray) -> dict:
+    """Regret of the chosen batch plans (time / best measured plan) and their
+    speedup over the rule-planned batch (rule covers, the engine's default
+    launch shape)."""
+    n = len(chosen)
+    best = T.min(axis=1)
+    t_ch = T[np.arange(n), chosen]
+    reg = t_ch / best
+    return {"batches": int(n), "regret_mean": float(reg.mean()), "regret_p90": float(np.quantile(reg, 0.9)),
+            "regret_max": float(reg.max()), "regret_total": float(t_ch.sum() / best.sum()),
+            "rule_regret_total": float(t_rule.sum() / best.sum()),
+            "speedup_vs_rule_total": float(t_rule.sum() / t_ch.sum()),
+            "speedup_vs_rule_geomean": float(np.exp(np.mean(np.log(t_rule / t_ch)))),
+            "chosen_hist": {BATCH_CANDIDATE_NAMES[c]: int((chosen == c).sum()) for c in range(NBC) if (chosen == c).any()}}
+
+
+def batch_experiment(train_rows: int, train_batches: int, eval_rows: int, eval_batches: int, reps: int = 3,
+                     epochs: int = 300, seed: int = 2, bseed: int = 7, weights: str | None = None) -> dict:
+    """Train the batch planner on engine-timed random batches over a
+    train_rows table; plan and time held-out batches over an eval_rows one."""
+    rep: dict = {"train_rows": train_rows, "train_batches": train_batches, "eval_rows": eval_rows,
+                 "eval_batches": eval_batches, "reps": reps, "seed": seed, "batch_seed": bseed}
+    t0 = time.perf_counter()
+    eng, _ = _engine(seed, train_rows)
+    tb = random_batches(bseed, train_batches)
+    X = np.stack([batch_features(eng, b) for b in tb])
+    T = measure_batch_candidates(eng, tb, reps)
+    rep["train_collect_s"] = time.perf_counter() - t0
+    eng.close()
+    tt, mk = targets(T)
+    mlp = MLP(NBF, 64, NBC, seed=seed)
+    t1 = time.perf_counter()
+    rep["train_loss"] = mlp.train(X, tt, mk, epochs=epochs, batch=64, lr=2e-3, seed=seed)
+    rep["train_s"] = time.perf_counter() - t1
+    y = mlp.forward(X, bf16=True)
+    rep["train_fit_regret_total"] = float(T[np.arange(len(tb)), y.argmin(1)].sum() / T.min(1).sum())
+    if weights:
+        mlp.save(weights)
+    eng, _ = _engine(seed + 1, eval_rows)
+    eb = random_batches(bseed + 1000, eval_batches)
+    chosen = plan_batches_learned(eng, eb, mlp)
+    TE = measure_batch_candidates(eng, eb, reps)
+    t_rule = np.array([time_batch(eng, b, abi.mb_batch_opts(), 0, reps) for b in eb])
+    rep["eval"] = batch_regret_report(TE, chosen, t_rule)
+    eng.close()
+    mlp.close()
+    return rep
+
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--train-rows", type=int, default=120_000_000)
@@ -310,9 +475,15 @@ def main(argv=None) -> None:
     ap.add_argument("--epochs", type=int, default=150)
     ap.add_argument("--out", type=str, default="")
     ap.add_argument("--weights", type=str, default="")
+    ap.add_argument("--batch", action="store_true", help="the batch planner: --train-queries / --eval-queries "
+                                                          "count batches")
     a = ap.parse_args(argv)
-    rep = experiment(a.train_rows, a.train_queries, a.eval_rows, a.eval_queries, a.reps, a.epochs,
-                     weights=a.weights or None)
+    if a.batch:
+        rep = batch_experiment(a.train_rows, a.train_queries, a.eval_rows, a.eval_queries, a.reps, a.epochs,
+                               weights=a.weights or None)
+    else:
+        rep = experiment(a.train_rows, a.train_queries, a.eval_rows, a.eval_queries, a.reps, a.epochs,
+                         weights=a.weights or None)
     s = json.dumps(rep, indent=1)
     print(s)
     if a.out:

@@ -158,3 +158,53 @@ def test_planner_network_shape_checked(net, eng24, mb):
         assert lib().mb_engine_set_planner(eng24.handle, None) == mb.abi.MB_OK
     finally:
         m.close()
+
+
+# ------------------------------------------------------------ batch planner
+def test_batch_features_and_network_shape(eng24, net, mb):
+    from merle_b200 import lib
+    qs = WL.span_mix(5, 24)
+    f = P.batch_features(eng24, qs)
+    assert f.shape == (P.NBF,) and np.isfinite(f).all() and f[31] == 1.0
+    np.testing.assert_array_equal(f, P.batch_features(eng24, qs))
+    assert lib().mb_engine_set_batch_planner(eng24.handle, net.handle) == mb.abi.MB_ERR_INVALID  # 32 -> 12
+    m = P.MLP(P.NBF, 64, P.NBC, seed=3)
+    try:
+        assert lib().mb_engine_set_batch_planner(eng24.handle, m.handle) == mb.abi.MB_OK
+        assert lib().mb_engine_set_batch_planner(eng24.handle, None) == mb.abi.MB_OK
+    finally:
+        m.close()
+
+
+def test_every_batch_plan_gives_the_same_answer(eng24):
+    """Every launch shape and cover of the batch plans: the same group sums
+    and row counts as the rule-planned batch (time_batch checks them)."""
+    for qs in (WL.span_mix(6, 24), WL.ssb13() + WL.random_mix(22, 9, narrow=0.5)):
+        want = P.batch_results(eng24, qs)
+        for c in range(P.NBC):
+            o, cover = P.batch_candidate(c)
+            P.time_batch(eng24, qs, o, cover, reps=1, want=want)
+
+
+def test_batch_planner_gains_over_rule(eng24):
+    """Train the batch planner on engine timings of 48 random batches (2 to
+    128 queries), plan 16 held-out batches with the BF16 network inside the
+    engine, and time every plan: the learned plans are at least 5 % faster in
+    total than the rule-planned batches and within 15 % of the best plan."""
+    tb = P.random_batches(41, 48)
+    X = np.stack([P.batch_features(eng24, b) for b in tb])
+    T = P.measure_batch_candidates(eng24, tb, reps=2, check_results=False)
+    t, mask = P.targets(T)
+    m = P.MLP(P.NBF, 64, P.NBC, seed=5)
+    eb = P.random_batches(42, 16)
+    try:
+        m.train(X, t, mask, epochs=300, batch=32, lr=2e-3, seed=2)
+        chosen = P.plan_batches_learned(eng24, eb, m)
+    finally:
+        m.close()
+    TE = P.measure_batch_candidates(eng24, eb, reps=3, check_results=False)
+    t_rule = np.array([P.time_batch(eng24, b, None, 0, 3) for b in eb])
+    r = P.batch_regret_report(TE, chosen, t_rule)
+    print("batch planner, 16 held-out batches at 24M rows:", r)
+    assert r["regret_total"] <= 1.15
+    assert r["speedup_vs_rule_total"] >= 1.05
