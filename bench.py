@@ -58,6 +58,7 @@ METRIC = "fact rows/s + %HBM roofline, learned+batched vs plain plan; p50/p99 la
 UNIT = "fact rows/s"
 SEED_DATA, SEED_QUERIES = 2, 3
 CPU_SAMPLE_ROWS = 24_000_000
+BATCH_WEIGHTS = ROOT / "merle_b200" / "weights" / "batch_planner.f32"
 PEAK_FALLBACK_GBS = 6650.0
 
 
@@ -77,8 +78,11 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true", help="skip the host parity pass and the CPU baseline")
     ap.add_argument("--serve-requests", type=int, default=1024, help="requests per serving run (0: no serving leg)")
-    ap.add_argument("--no-tune", action="store_true", help="default launch shape instead of the autotuner's")
+    ap.add_argument("--plan", default="learned", choices=["learned", "tuned", "rule"],
+                    help="the batch plan: the learned batch planner's (merle_b200/weights/batch_planner.f32), "
+                         "the autotuner's (shapes timed on the mix), or the rule's (default shape, rule covers)")
     ap.add_argument("--no-graph", action="store_true", help="enqueue each step instead of replaying a CUDA graph")
+    ap.add_argument("--no-plan-check", action="store_true", help="skip timing every batch plan of the mix")
     ap.add_argument("--wah", action="store_true",
                     help="instead of the headline: the WAH baseline (compress two predicate bitmaps, AND the "
                          "streams) on the GPU beside the reference's CPU WAH code")
@@ -374,16 +378,38 @@ def main():
             with torch.cuda.stream(ext):
                 shard.combine(out, nq)
 
-    # the launch shape from the autotuner (timed on this mix, before the
-    # measured steps), and the batch captured once as a CUDA graph
+    # the batch plan (launch shape and covers): the learned batch planner's,
+    # the autotuner's (timed on this mix before the measured steps) or the
+    # rule's; the batch captured once as a CUDA graph
     bopts = abi.mb_batch_opts()
-    tune = {"tuned": False}
-    if not args.no_tune:
+    cover = 0
+    tune = {"planner": args.plan}
+    bnet = None
+    if args.plan == "learned" and BATCH_WEIGHTS.exists():
+        from merle_b200.planner import BATCH_CANDIDATE_NAMES, MLP
+        bnet = MLP.load(BATCH_WEIGHTS)
+        check(L.mb_engine_set_batch_planner(eng.handle, bnet.handle))
+        cv, choice = C.c_uint32(0), C.c_uint32(0)
+        t0 = time.perf_counter()
+        check(L.mb_engine_plan_batch(eng.handle, qarr, Q, C.byref(bopts), C.byref(cv), C.byref(choice)))
+        cover = int(cv.value)
+        tune.update({"choice": BATCH_CANDIDATE_NAMES[choice.value], "plan_ms": (time.perf_counter() - t0) * 1e3,
+                     "weights": str(BATCH_WEIGHTS.relative_to(ROOT))})
+    elif args.plan == "tuned":
         tms, tried = C.c_float(0), C.c_uint32(0)
         t0 = time.perf_counter()
         check(L.mb_engine_tune_batch(eng.handle, qarr, Q, 3, C.byref(bopts), C.byref(tms), C.byref(tried)))
-        tune = {"tuned": True, "shapes_timed": tried.value, "best_ms": tms.value, "tune_s": time.perf_counter() - t0,
-                "opts": {f: getattr(bopts, f) for f, _ in bopts._fields_ if f != "pad_"}}
+        tune.update({"shapes_timed": tried.value, "best_ms": tms.value, "tune_s": time.perf_counter() - t0})
+    else:
+        tune["planner"] = "rule"
+    tune["opts"] = {f: getattr(bopts, f) for f, _ in bopts._fields_ if f != "pad_"}
+    tune["cover"] = ["rule", "noedge", "nocompl", "fine"][cover]
+    plans = []
+    for _ in qs:
+        p = abi.mb_plan()
+        p.kind, p.cover = abi.PLAN_FUSED, cover
+        plans.append(p)
+    parr = (abi.mb_plan * Q)(*plans)
     binfo = (abi.mb_batch_launch_info * 16)()
     nlaunch, nalone = C.c_uint32(0), C.c_uint32(0)
     check(L.mb_engine_batch_info(eng.handle, qarr, Q, C.byref(bopts), binfo, 16, C.byref(nlaunch), C.byref(nalone)))
@@ -392,14 +418,15 @@ def main():
     tune["queries_alone"] = nalone.value
     graph = C.c_void_p()
     if not args.no_graph:
-        check(L.mb_batch_graph_create(eng.handle, qarr, Q, C.byref(bopts), out.data_ptr(), nq.data_ptr(),
-                                      C.byref(graph)))
+        check(L.mb_batch_graph_create_plans(eng.handle, qarr, parr, Q, C.byref(bopts), out.data_ptr(), nq.data_ptr(),
+                                            C.byref(graph)))
 
     def step_batch():
         if graph:
             check(L.mb_batch_graph_launch(graph))
         else:
-            check(L.mb_engine_enqueue_batch(eng.handle, qarr, Q, C.byref(bopts), out.data_ptr(), nq.data_ptr()))
+            check(L.mb_engine_enqueue_batch_plans(eng.handle, qarr, parr, Q, C.byref(bopts), out.data_ptr(),
+                                                  nq.data_ptr()))
         allreduce()
 
     def step_plain(record=False):
@@ -450,13 +477,13 @@ def main():
     # ---- e2e through the public API with host buffers: mb_engine_query_batch
     res_host = np.zeros(total_g, np.int64)
     nq_host = np.zeros(Q, np.uint64)
-    check(L.mb_engine_query_batch(eng.handle, qarr, Q, C.byref(bopts), res_host.ctypes.data, nq_host.ctypes.data))
+    e2e_opts = None if bnet is not None else C.byref(bopts)  # None: the engine plans the batch with its network
+    check(L.mb_engine_query_batch(eng.handle, qarr, Q, e2e_opts, res_host.ctypes.data, nq_host.ctypes.data))
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        check(L.mb_engine_query_batch(eng.handle, qarr, Q, C.byref(bopts), res_host.ctypes.data,
-                                      nq_host.ctypes.data))
+        check(L.mb_engine_query_batch(eng.handle, qarr, Q, e2e_opts, res_host.ctypes.data, nq_host.ctypes.data))
     e2e_ms = float((time.perf_counter() - t0) * 1e3)
     if world > 1:
         t = torch.tensor([e2e_ms], device="cuda")
@@ -465,15 +492,28 @@ def main():
     e2e = {"value": rows_total * Q * args.e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": C.sizeof(abi.mb_query) * Q + BATCH_HDR_BYTES,
            "d2h_bytes_per_step": 8 * total_g + 8 * Q,
-           "api": "mb_engine_query_batch (host query descriptors in, host int64 group sums and row counts out, "
-                  "returns when they are on the host)",
+           "api": "mb_engine_query_batch (host query descriptors in, the batch planned by the engine's network, "
+                  "host int64 group sums and row counts out, returns when they are on the host)",
            "timing": "host wall clock around each call", "ms_per_step": e2e_ms / args.e2e_steps}
     e2e_same = bool(np.array_equal(res_host, batch_out.cpu().numpy())) if world == 1 else None
+
+    # ---- the batch plans of this mix, timed (CUDA-graph replays): regret
+    # of the chosen plan and its speedup over the rule-planned batch
+    if world == 1 and not args.no_plan_check:
+        from merle_b200 import planner as PL
+        ref = batch_out.cpu().numpy()
+        cand = [PL.time_batch(eng, qs, *PL.batch_candidate(c), reps=3, want=ref) for c in range(PL.NBC)]
+        t_rule = PL.time_batch(eng, qs, None, 0, reps=3, want=ref)
+        t_ch = ms_total / args.steps
+        tune.update({"candidates_ms": {PL.BATCH_CANDIDATE_NAMES[c]: round(cand[c], 4) for c in range(PL.NBC)},
+                     "rule_ms": t_rule, "regret": t_ch / min(cand + [t_ch]), "speedup_vs_rule": t_rule / t_ch,
+                     "heldout_eval": json.loads((ROOT / "merle_b200" / "weights" / "batch_planner_eval.json")
+                                                .read_text()).get("eval") if bnet is not None else None})
 
     # ---- serving: Poisson arrivals through the batched and the plain server
     serving = None
     if args.serve_requests and world == 1:
-        serving = serve_leg(eng, args, bopts, float(qtimes.mean()))
+        serving = serve_leg(eng, args, None if bnet is not None else bopts, float(qtimes.mean()))
 
     line = None
     if rank == 0:
@@ -530,9 +570,11 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
                 "config": config_of(args, n), "impl": "ours",
-                "plan": "batched: the whole mix in one persistent launch per step (rule-planner covers)"
+                "plan": ("learned+batched: the whole mix in one persistent launch per step, its launch shape and "
+                         "covers chosen by the learned batch planner" if bnet is not None else
+                         f"batched ({tune['planner']} plan): the whole mix in one persistent launch per step")
                         + ("; replayed as a CUDA graph" if graph else ""),
-                "batch_shape": tune,
+                "batch_plan": tune,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "parity": parity,
                 "plain": {"value": rows_total * Q * args.steps / (plain_ms / 1e3), "ms_per_step": plain_ms / args.steps,
                           "batched_speedup": plain_ms / ms_total, "results_identical": same,
@@ -551,6 +593,9 @@ def main():
         print(json.dumps(line))
     if graph:
         check(L.mb_batch_graph_destroy(graph))
+    if bnet is not None:
+        check(L.mb_engine_set_batch_planner(eng.handle, None))
+        bnet.close()
     eng.close()
     if world > 1:
         dist.barrier()

@@ -271,7 +271,10 @@ MB_API mb_status mb_bitmap_to_rows(const uint32_t *possible, const uint32_t *unc
  *    with MB_ERR_INVALID before any device work.
  *  - The first call on each device looks up the array's device address with
  *    that device current; make that first call before capturing the stream
- *    into a CUDA graph.
+ *    into a CUDA graph.  The address is kept for the life of the process: a
+ *    cudaDeviceReset while the library is loaded is not supported (it would
+ *    leave the kept address stale; mb_bitmap_to_rows keeps its scratch
+ *    buffer the same way).
  *  - Every call on a device shares the one array.  Calls that may overlap on
  *    the GPU (different streams, or different host threads without ordering)
  *    race on it and corrupt each other's results; order them on one stream.

@@ -13,8 +13,9 @@
  *     stderr instead of exit() or assert();
  *   - ssb_cpujoin and synth_ref compute their results on the GPU (the
  *     library has no CPU path; the reference's CPU code is the test oracle);
- *   - ssb_wah and synth_wah (the WAH compressed-bitmap baseline) print that
- *     the baseline is not built and return;
+ *   - ssb_wah and synth_wah run the reference's WAH pipelines on this
+ *     library's WAH kernels (mb_wah_*) and print "unavailable" in the RTScan
+ *     column (an OptiX ray-tracing competitor, not available on this system);
  *   - results are the reference's uint32 values: the int64 sums of the
  *     mb_* kernels truncated to 32 bits (the reference's atomics wrap).
  * Struct layouts, enum values and the bin tables are the reference's,

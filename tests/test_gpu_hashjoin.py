@@ -119,3 +119,30 @@ def test_engine_hash_plan(cuda, mb, probe_dims):
             e.query(WL.ssb13()[0], bad)
     finally:
         e.close()
+
+
+@pytest.mark.parametrize("width,n,offset", [(8, 100_003, 0), (4, 128 * 300 + 77, 0), (2, 4097, 0),
+                                            (1, 131, 0), (4, 50_001, 1)])
+def test_hash_probe_screen_widths_tails_alignment(orc, cuda, width, n, offset):
+    """The hash probe's screen: one range on a fact column of each width (four
+    rows a lane from one vector load), row counts that end inside a 128-row
+    chunk, and a column that is not 16-byte aligned (the generic screen), next
+    to a dimension clause through a foreign key (so a table is built and
+    probed); SUM(b * c) and the row count equal the oracle's no-index plan."""
+    rng = np.random.default_rng(width * 7000 + n)
+    dt = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[width]
+    a_full = rng.integers(0, 200, n + offset).astype(dt)
+    b = rng.integers(0, 1000, n).astype(np.uint32)
+    c = rng.integers(0, 50, n).astype(np.uint32)
+    dim = rng.integers(0, 1000, 5000).astype(np.uint16)
+    fk = rng.integers(0, 5000, n).astype(np.uint32)
+    a = a_full[offset:]
+
+    def op(cols):
+        return ops.Op(srcs=[ops.Src(cols[0]), ops.Src(cols[1]), ops.Src(cols[2]), ops.Src(cols[3], cols[4])],
+                      clauses=[[(0, 40, 90)], [(3, 100, 700)]], keys=[], vkind=abi.V_MUL, va=1, vb=2).to_c()
+    want, nqw = orc.join_grpby(n, op((np.ascontiguousarray(a), b, c, dim, fk)), 1)
+    da_full = D.from_host(a_full)
+    da = da_full[offset:] if offset else da_full
+    got, nq = hash_join(n, op((da, D.from_host(b), D.from_host(c), D.from_host(dim), D.from_host(fk))), 1)
+    assert int(got[0]) == int(want[0]) and nq == nqw

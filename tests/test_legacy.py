@@ -7,6 +7,8 @@ libmerleb200.so.  GPU (test_gpu_legacy.py): the SSB and synthetic demo drivers
 end to end."""
 from __future__ import annotations
 
+import os
+
 import ctypes as C
 import json
 import shutil
@@ -18,7 +20,7 @@ import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
 GOLDEN = ROOT / "tests" / "golden"
-REF = Path("/root/reference")
+REF = Path(os.environ.get("MERLE_REF", "/nonexistent-reference-tree"))
 
 
 def test_bin_tables_exported(mb):

@@ -39,15 +39,42 @@ def _rows(fn, poss, unc, n, cap):
 
 def test_noalloc_matches_allocating_entry_point(cuda, mb):
     L = mb.lib()
-    # two calls in a row on different inputs: the second must not see the
-    # first call's leftovers in the shared scratch array
-    for n, seed, density in [(3_000_017, 1, 0.02), (100_003, 2, 0.5)]:
+    # the no-allocation entry point runs FIRST, on a size larger than any
+    # call before it in this process, and the device's free memory must not
+    # move across it (a fallback to an allocating path would show there);
+    # then two calls in a row on different inputs: the second must not see
+    # the first call's leftovers in the shared scratch array
+    warm, wunc = _random_bitmaps(1000, 9, 0.5)
+    _rows(L.mb_bitmap_to_rows_noalloc, warm, wunc, 1000, 1032)  # loads the kernels and the array
+    for n, seed, density in [(40_000_017, 1, 0.02), (100_003, 2, 0.5)]:
         poss, unc = _random_bitmaps(n, seed, density)
         cap = n + 32
+        rows = D.empty(cap, 4, zero=True)
+        cnt = D.empty(1, 8, zero=True)
+        cuda.cuda.synchronize()
+        free0, reserved0 = cuda.cuda.mem_get_info()[0], cuda.cuda.memory_reserved()
+        check(L.mb_bitmap_to_rows_noalloc(poss.data_ptr(), unc.data_ptr(), n, rows.data_ptr(), cnt.data_ptr(),
+                                          D.stream_ptr()))
+        cuda.cuda.synchronize()
+        assert cuda.cuda.mem_get_info()[0] == free0 and cuda.cuda.memory_reserved() == reserved0
+        gc = int(D.to_host(cnt, np.uint64)[0])
+        got = D.to_host(rows, np.uint32)[:gc].copy()
         want, wc = _rows(L.mb_bitmap_to_rows, poss, unc, n, cap)
-        got, gc = _rows(L.mb_bitmap_to_rows_noalloc, poss, unc, n, cap)
         assert gc == wc and wc > 0
         np.testing.assert_array_equal(got, want)
+
+
+def test_noalloc_takes_exactly_its_limit(cuda, mb):
+    """nrows == MB_NOALLOC_MAX_ROWS (2^30) is accepted: an all-zero bitmap of
+    2^30 rows (128 MiB) gives no row, so a 4-entry output suffices."""
+    L = mb.lib()
+    limit = 1 << 30
+    zero = D.empty(limit // 32, 4, zero=True)
+    rows = D.empty(4, 4, zero=True)
+    cnt = D.empty(1, 8, zero=True)
+    check(L.mb_bitmap_to_rows_noalloc(zero.data_ptr(), None, limit, rows.data_ptr(), cnt.data_ptr(),
+                                      D.stream_ptr()))
+    assert int(D.to_host(cnt, np.uint64)[0]) == 0
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit(cuda, mb):
