@@ -417,11 +417,17 @@ static mb_status dispatch_w(uint32_t w, int mode, const BinSpec &S, const mb_src
 
 
 // ---------------------------------------------------------------- levels host
+// Shared memory of bitmap_levels_kernel<W>: column stages, barriers, bin
+// counts, the bins' word tiles and the lookup table.
+static size_t levels_smem(const LevelSpec &S, int W) {
+  return (size_t)BC_STAGES * BC_TILE_ROWS * W + 64 + (size_t)((S.total_bins + 1) & ~1u) * 8 +
+         (size_t)S.total_bins * BC_TILE_WORDS * 4 + round_up((uint64_t)S.dom_n * S.nlevels, 16);
+}
+
 template <int W, bool JOIN, int DW>
 static mb_status launch_levels(const LevelSpec &S, const mb_src *src, uint64_t n, uint64_t stride, cudaStream_t st) {
   auto kern = bitmap_levels_kernel<W, JOIN, DW>;
-  const size_t smem = (size_t)BC_STAGES * BC_TILE_ROWS * W + 64 + (size_t)((S.total_bins + 1) & ~1u) * 8 +
-                      (size_t)S.total_bins * BC_TILE_WORDS * 4 + round_up((uint64_t)S.dom_n * S.nlevels, 16);
+  const size_t smem = levels_smem(S, W);
   MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
   MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, BL_THREADS, smem));
@@ -439,8 +445,9 @@ static mb_status launch_levels(const LevelSpec &S, const mb_src *src, uint64_t n
 }
 
 // The levels as one LevelSpec, if the fast path takes them: each level
-// sorted and disjoint with at most 255 bins, the value domain small enough
-// for the lookup table, the tiles within shared memory.
+// sorted and disjoint with at most 254 bins, the value domain small enough
+// for the lookup table (the caller checks that the tiles fit in shared
+// memory).
 static bool levels_spec(const mb_level *lv, uint32_t nl, LevelSpec &S) {
   if (nl == 0 || nl > (uint32_t)BL_MAXLEVELS) return false;
   memset(&S, 0, sizeof(S));
@@ -575,7 +582,9 @@ extern "C" mb_status mb_bitmap_create_levels(const mb_src *src, uint64_t nrows, 
   if (nrows == 0) return MB_OK;
   cudaStream_t st = as_stream(stream);
   static thread_local LevelSpec S;  // 24 KB lookup table: not on the stack
-  const bool fast = levels_spec(levels, nlevels, S) && (w <= 4 || src->fk);
+  const int staged_w = src->fk ? 4 : (int)w;
+  const bool fast = levels_spec(levels, nlevels, S) && (w <= 4 || src->fk) &&
+                    levels_smem(S, staged_w) <= (size_t)dev_info().max_smem_optin;
   if (!fast) {  // one pass per level
     for (uint32_t l = 0; l < nlevels; ++l)
       MB_CHECK(mb_bitmap_create(src, nrows, levels[l].lo, levels[l].hi, levels[l].nbins, levels[l].out, stride_words,

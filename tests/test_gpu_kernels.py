@@ -132,6 +132,10 @@ LEVEL_CASES = {
     "gaps3": ("suppcity", [([0, 3, 50, 51, 200, 240], [2, 40, 51, 52, 230, 241]),
                            (np.arange(0, 240, 60), np.arange(60, 300, 60)),
                            (np.arange(5, 245, 5), np.arange(10, 250, 5))], False),
+    # 4 x 200 bins: their word tiles exceed shared memory, one pass per level
+    "wide4": ("suppcity", [(np.arange(0, 200), np.arange(1, 201)), (np.arange(10, 210), np.arange(11, 211)),
+                           (np.arange(20, 220), np.arange(21, 221)), (np.arange(49, 249), np.arange(50, 250))],
+              False),
     # overlapping bins in one level: that level falls back to its own pass
     "overlap": ("suppcity", [(np.arange(0, 250, 50), np.arange(50, 300, 50)),
                              ([0, 10, 5], [20, 30, 250])], False),
