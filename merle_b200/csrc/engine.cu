@@ -194,36 +194,58 @@ void Engine::free_denorm() {
   partmfgr_row = nullptr;
 }
 
-// out[r] = dim[fk[r]]; counts the rows whose key lies outside the dimension.
-template <typename D>
-__global__ void denorm_kernel(const uint32_t *__restrict__ fk, const D *__restrict__ dim, uint64_t dimsz,
-                              D *__restrict__ out, uint64_t n, unsigned long long *bad) {
-  uint32_t nbad = 0;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t k = __ldcs(fk + i);
-    D v = 0;
-    if (k < dimsz) v = __ldg(dim + k);
-    else ++nbad;
-    out[i] = v;
+// custcity_row[r] = custcity[custkey[r]] and partmfgr_row[r] =
+// partmfgr[partkey[r]], 0 where a key lies outside its dimension (counted in
+// bad[0] / bad[1]).  Four rows a thread per step: one 16-byte load of each
+// key column, eight dimension loads in flight, one 4-byte and one 8-byte
+// store.
+__global__ void denorm_kernel(const uint32_t *__restrict__ ck, const uint8_t *__restrict__ cdim, uint64_t csz,
+                              const uint32_t *__restrict__ pk, const uint16_t *__restrict__ pdim, uint64_t psz,
+                              uint8_t *__restrict__ cout, uint16_t *__restrict__ pout, uint64_t n,
+                              unsigned long long *bad) {
+  uint32_t bc = 0, bp = 0;
+  const uint64_t n4 = n / 4, step = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint64_t i = g; i < n4; i += step) {
+    const uint4 c = __ldcs(reinterpret_cast<const uint4 *>(ck) + i);
+    const uint4 p = __ldcs(reinterpret_cast<const uint4 *>(pk) + i);
+    const uint32_t cv[4] = {c.x, c.y, c.z, c.w}, pv[4] = {p.x, p.y, p.z, p.w};
+    uint32_t co = 0, po[2] = {0, 0};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (cv[j] < csz) co |= (uint32_t)__ldg(cdim + cv[j]) << (8 * j);
+      else ++bc;
+      if (pv[j] < psz) po[j >> 1] |= (uint32_t)__ldg(pdim + pv[j]) << (16 * (j & 1));
+      else ++bp;
+    }
+    reinterpret_cast<uint32_t *>(cout)[i] = co;
+    reinterpret_cast<uint2 *>(pout)[i] = make_uint2(po[0], po[1]);
   }
-  nbad = __reduce_add_sync(0xffffffffu, nbad);
-  if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad, (unsigned long long)nbad);
+  if (g < n - 4 * n4) {  // the last n % 4 rows
+    const uint64_t r = 4 * n4 + g;
+    const uint32_t c = ck[r], p = pk[r];
+    cout[r] = c < csz ? cdim[c] : 0;
+    pout[r] = p < psz ? pdim[p] : 0;
+    bc += c >= csz;
+    bp += p >= psz;
+  }
+  bc = __reduce_add_sync(0xffffffffu, bc);
+  bp = __reduce_add_sync(0xffffffffu, bp);
+  if ((threadIdx.x & 31) == 0) {
+    if (bc) atomicAdd(bad, (unsigned long long)bc);
+    if (bp) atomicAdd(bad + 1, (unsigned long long)bp);
+  }
 }
 
-// Builds custcity_row and partmfgr_row; a column whose foreign keys leave
-// their dimension is dropped again (its queries keep the probe, which
-// treats such rows as the op semantics say).
 // The denormalised per-row columns (allocated by the caller), filled on the
 // engine stream; d_bad (device, 2 counters) counts foreign keys outside their
 // dimension.
 mb_status Engine::enqueue_denorm(unsigned long long *d_bad) {
   MB_CUDA(cudaMemsetAsync(d_bad, 0, 16, stream));
-  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(nrows, 256), 148ull * 8));
-  denorm_kernel<uint8_t><<<grid, 256, 0, stream>>>(reinterpret_cast<const uint32_t *>(custkey), custcity,
-                                                    ncust + 1, custcity_row, nrows, d_bad);
-  MB_LAUNCH_CHECK("denorm_kernel");
-  denorm_kernel<uint16_t><<<grid, 256, 0, stream>>>(reinterpret_cast<const uint32_t *>(partkey), partmfgr,
-                                                     npart + 1, partmfgr_row, nrows, d_bad + 1);
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(nrows, 1024), 148ull * 8));
+  denorm_kernel<<<grid, 256, 0, stream>>>(reinterpret_cast<const uint32_t *>(custkey), custcity, ncust + 1,
+                                          reinterpret_cast<const uint32_t *>(partkey), partmfgr, npart + 1,
+                                          custcity_row, partmfgr_row, nrows, d_bad);
   MB_LAUNCH_CHECK("denorm_kernel");
   return MB_OK;
 }
