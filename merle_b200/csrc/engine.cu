@@ -237,13 +237,13 @@ __global__ void denorm_kernel(const uint32_t *__restrict__ ck, const uint8_t *__
   }
 }
 
-// The denormalised per-row columns (allocated by the caller), filled on the
-// engine stream; d_bad (device, 2 counters) counts foreign keys outside their
+// The denormalised per-row columns (allocated by the caller), filled on
+// stream st; d_bad (device, 2 counters) counts foreign keys outside their
 // dimension.
-mb_status Engine::enqueue_denorm(unsigned long long *d_bad) {
-  MB_CUDA(cudaMemsetAsync(d_bad, 0, 16, stream));
+mb_status Engine::enqueue_denorm(unsigned long long *d_bad, cudaStream_t st) {
+  MB_CUDA(cudaMemsetAsync(d_bad, 0, 16, st));
   const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(nrows, 1024), 148ull * 8));
-  denorm_kernel<<<grid, 256, 0, stream>>>(reinterpret_cast<const uint32_t *>(custkey), custcity, ncust + 1,
+  denorm_kernel<<<grid, 256, 0, st>>>(reinterpret_cast<const uint32_t *>(custkey), custcity, ncust + 1,
                                           reinterpret_cast<const uint32_t *>(partkey), partmfgr, npart + 1,
                                           custcity_row, partmfgr_row, nrows, d_bad);
   MB_LAUNCH_CHECK("denorm_kernel");
@@ -258,7 +258,7 @@ mb_status Engine::build_denorm() {
   MB_CHECK(alloc((void **)&d_bad, 16));
   MB_CHECK(alloc((void **)&custcity_row, nrows));
   MB_CHECK(alloc((void **)&partmfgr_row, nrows * 2));
-  MB_CHECK(enqueue_denorm(d_bad));
+  MB_CHECK(enqueue_denorm(d_bad, stream));
   unsigned long long bad[2] = {0, 0};
   MB_CUDA(cudaMemcpyAsync(bad, d_bad, 16, cudaMemcpyDeviceToHost, stream));
   MB_CUDA(cudaStreamSynchronize(stream));
@@ -788,15 +788,50 @@ extern "C" mb_status mb_engine_build_index_levels(mb_engine *e, uint32_t flags, 
   MB_CHECK(E.alloc((void **)&E.islab, (size_t)E.nbm * E.stride * 4));
   const uint64_t nwords = (E.nrows + 31) / 32;
 
+  // The denormalisation (bound by its random dimension reads) runs on the
+  // side stream while the columns that do not read its output are indexed;
+  // the customer-city and part-mfgr columns wait for it.
+  struct Events {
+    cudaEvent_t fork = nullptr, join = nullptr;
+    ~Events() {
+      if (fork) cudaEventDestroy(fork);
+      if (join) cudaEventDestroy(join);
+    }
+  } ev;
   MB_CUDA(cudaEventRecord(E.ev0, E.stream));
-  if (denorm) MB_CHECK(E.enqueue_denorm(d_bad));
+  if (denorm) {
+    if (!E.pstream) MB_CUDA(cudaStreamCreateWithFlags(&E.pstream, cudaStreamNonBlocking));
+    MB_CUDA(cudaEventCreateWithFlags(&ev.fork, cudaEventDisableTiming));
+    MB_CUDA(cudaEventCreateWithFlags(&ev.join, cudaEventDisableTiming));
+    MB_CUDA(cudaEventRecord(ev.fork, E.stream));
+    MB_CUDA(cudaStreamWaitEvent(E.pstream, ev.fork, 0));
+    MB_CHECK(E.enqueue_denorm(d_bad, E.pstream));
+    MB_CUDA(cudaEventRecord(ev.join, E.pstream));
+  }
   // only the padding words past each bitmap's end need clearing: the passes
   // write every word below it
   if (E.stride > nwords)
     MB_CUDA(cudaMemset2DAsync(E.islab + nwords, E.stride * 4, 0, (E.stride - nwords) * 4, E.nbm, E.stream));
   MB_CUDA(cudaMemsetAsync(d_pop, 0, (size_t)E.nbm * 8, E.stream));
   uint64_t first = 0;
+  std::vector<uint64_t> firsts;
   for (auto &c : E.idx) {
+    firsts.push_back(first);
+    for (auto &l : c.levels) first += l.nbins();
+  }
+  // columns that read no denormalised column first
+  std::vector<int> order;
+  for (int pass = 0; pass < 2; ++pass)
+    for (int i = 0; i < IC_N; ++i)
+      if ((i == IC_CCITY || i == IC_MFGR) == (pass == 1)) order.push_back(i);
+  bool joined = false;
+  for (int ci : order) {
+    IdxCol &c = E.idx[ci];
+    first = firsts[ci];
+    if (denorm && !joined && (ci == IC_CCITY || ci == IC_MFGR)) {
+      MB_CUDA(cudaStreamWaitEvent(E.stream, ev.join, 0));
+      joined = true;
+    }
     std::vector<std::vector<uint64_t>> lo(c.levels.size()), hi(c.levels.size());
     std::vector<mb_level> lv(c.levels.size());
     for (size_t i = 0; i < c.levels.size(); ++i) {
@@ -812,6 +847,7 @@ extern "C" mb_status mb_engine_build_index_levels(mb_engine *e, uint32_t flags, 
     }
     MB_CHECK(mb_bitmap_create_levels(&c.src, E.nrows, lv.data(), (uint32_t)lv.size(), E.stride, E.stream));
   }
+  if (denorm && !joined) MB_CUDA(cudaStreamWaitEvent(E.stream, ev.join, 0));
   MB_CUDA(cudaEventRecord(E.ev1, E.stream));
   std::vector<uint64_t> pops(E.nbm);
   unsigned long long bad[2] = {0, 0};

@@ -159,7 +159,7 @@ struct Engine {
   mb_src ccity_src() const;
   mb_src mfgr_src() const;
   mb_status build_denorm();
-  mb_status enqueue_denorm(unsigned long long *d_bad);
+  mb_status enqueue_denorm(unsigned long long *d_bad, cudaStream_t st);
 };
 
 // The op functors s1op..s4op (ssb/lambdas.cuh:19-152) of a template query as
