@@ -360,6 +360,11 @@ def main():
     eng = Engine(local)
     row0, n = shard.row_range(rank, n)
     eng.gen_star(SEED_DATA, args.k, n, width4=bool(args.width4), row0=row0)
+    # the index is built twice: the first build also loads the library's
+    # kernels into the context (a once-per-process cost); the second is the
+    # steady-state build the roofline line reports
+    eng.build_index()
+    first_build_ms = eng.info()["index_build_ms"]
     eng.build_index()
     info = eng.info()
     qs = mix_of(args)
@@ -585,10 +590,14 @@ def main():
                 "gpu_launches": args.steps * (nlaunch.value + nalone.value),
                 "clocks": clk.summary(),
                 "index": {"bitmaps": info["nbitmaps"], "bytes": info["index_bytes"],
-                          "build_ms": info["index_build_ms"], "denorm_bytes": info["denorm_bytes"],
+                          "build_ms": info["index_build_ms"], "first_build_ms": first_build_ms,
+                          "denorm_bytes": info["denorm_bytes"],
                           "algo_bytes": build_bytes,
                           "achieved_gbs": build_bytes / (info["index_build_ms"] / 1e3) / 1e9,
-                          "frac": build_bytes / (info["index_build_ms"] / 1e3) / 1e9 / peak},
+                          "frac": build_bytes / (info["index_build_ms"] / 1e3) / 1e9 / peak,
+                          "note": "build_ms: a second build of the same table (the first also loads the "
+                                  "library's kernels into the context: first_build_ms); algo_bytes: columns "
+                                  "and keys read once, bitmaps and denormalised columns written once"},
                 "selected_rows_per_step": int(batch_nq.sum().item())}
         print(json.dumps(line))
     if graph:
@@ -606,14 +615,16 @@ def index_build_bytes(n: int, info: dict, width4: int) -> int:
     """Algorithmic bytes of the index build: each indexed column read once
     (the date, discount, quantity and supplier city columns; the customer
     and part foreign keys plus their dimension arrays for the customer city
-    and part mfgr levels) and every bitmap written once."""
+    and part mfgr levels), every bitmap written once, and the denormalised
+    customer-city (1 byte a row) and part-mfgr (2 bytes) columns the same
+    passes write for the queries."""
     w = 4 if width4 else None
     k = max(1, info["k"])
     from oracle import oracle as O
     col = (w or 2) * n + (w or 1) * n + (w or 1) * n + (w or 1) * n  # date, discount, quantity, suppcity
     fk = 4 * n * 2 + (30000 * k + 1) * 1 + (O.star_npart(k) + 1) * 2
     bm = info["nbitmaps"] * ((n + 31) // 32) * 4
-    return int(col + fk + bm)
+    return int(col + fk + bm + info.get("denorm_bytes", 0))
 
 
 def serve_leg(eng, args, bopts, plain_query_ms: float) -> dict:

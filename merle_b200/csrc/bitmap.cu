@@ -23,6 +23,7 @@
 #include <stddef.h>
 #include <string.h>
 #include <algorithm>
+#include <type_traits>
 #include "common.cuh"
 #include "tma.cuh"
 
@@ -252,10 +253,38 @@ __device__ __forceinline__ uint32_t lv_word(uint32_t j, uint32_t wi) {
   return j * BC_TILE_WORDS + (wi ^ (j & 31u));
 }
 
-template <int W, bool JOIN, int DW>
-__global__ void __launch_bounds__(BL_THREADS)
+// Join output of the levels pass: the dimension value of every row (0 where
+// the key leaves the dimension) written to dout, and the rows whose key
+// leaves it counted in *bad; both optional.
+struct LevelsJoinOut {
+  void *dout;
+  unsigned long long *bad;
+};
+
+// The dimension value of key x (JOIN) or x itself; ok false for a key
+// outside the dimension.
+template <bool JOIN, int DW>
+__device__ __forceinline__ uint64_t lv_value(const void *dim, uint64_t dimsz, uint64_t x, bool &ok) {
+  if (!JOIN) return x;
+  ok = dimsz == 0 || x < dimsz;
+  return ok ? load_width(dim, x, DW) : 0;
+}
+
+template <int DW>
+__device__ __forceinline__ void lv_store(void *dout, uint64_t row, uint64_t v) {
+  if (DW == 1) reinterpret_cast<uint8_t *>(dout)[row] = (uint8_t)v;
+  else if (DW == 2) reinterpret_cast<uint16_t *>(dout)[row] = (uint16_t)v;
+  else if (DW == 4) reinterpret_cast<uint32_t *>(dout)[row] = (uint32_t)v;
+  else reinterpret_cast<unsigned long long *>(dout)[row] = v;
+}
+
+// (A join pass holds its dimension reads in flight: two CTAs an SM, at most
+// 64 registers; three CTAs at 42 registers spilled and measured 27 % slower.)
+template <int W, bool JOIN, int DW, int NLC>
+__global__ void __launch_bounds__(BL_THREADS, JOIN ? 2 : 1)
 bitmap_levels_kernel(const __grid_constant__ LevelSpec S, const void *__restrict__ col,
-                     const void *__restrict__ dim, uint64_t dimsz, uint64_t n, uint64_t stride, uint32_t *errw) {
+                     const void *__restrict__ dim, uint64_t dimsz, uint64_t n, uint64_t stride, uint32_t *errw,
+                     LevelsJoinOut jo) {
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr uint32_t STAGE_BYTES = BC_TILE_ROWS * W;
   uint8_t *stage = smem;
@@ -268,6 +297,10 @@ bitmap_levels_kernel(const __grid_constant__ LevelSpec S, const void *__restrict
   const uint64_t ntiles = (n + BC_TILE_ROWS - 1) / BC_TILE_ROWS;
   const uint8_t *colb = reinterpret_cast<const uint8_t *>(col);
   const uint32_t NL = S.nlevels, bit = 1u << lane;
+  uint32_t rw[NLC];  // first tile row of each level
+#pragma unroll
+  for (int l = 0; l < NLC; ++l) rw[l] = S.row0[l];
+  uint32_t nbad = 0;  // rows of this thread whose key leaves the dimension (JOIN)
 
   for (uint32_t i = tid; i < S.dom_n; i += BL_THREADS) lut[i] = S.lut[i];
   for (uint32_t b = tid; b < S.nrows_tile; b += BL_THREADS) cnt[b] = 0;
@@ -311,21 +344,47 @@ bitmap_levels_kernel(const __grid_constant__ LevelSpec S, const void *__restrict
     const uint64_t row0 = t * BC_TILE_ROWS;
     const uint32_t rows_here = n - row0 < (uint64_t)BC_TILE_ROWS ? (uint32_t)(n - row0) : (uint32_t)BC_TILE_ROWS;
 
-    for (uint32_t wi = warp; wi < BC_TILE_WORDS; wi += nwarps) {
-      const uint32_t r = wi * 32 + lane;
-      uint32_t bins = S.nobin;
-      if (r < rows_here) {
-        const uint64_t x = r < bulk_rows ? ld_smem_w<W>(sp, r) : load_width(col, row0 + r, W);
-        bool ok = true;
-        uint64_t v = x;
-        if (JOIN) {
-          if (dimsz != 0 && x >= dimsz) ok = false;
-          else v = load_width(dim, x, DW);
-        }
-        if (ok && v - S.dom_lo < (uint64_t)S.dom_n) bins = lut[(uint32_t)(v - S.dom_lo)];
+    if (rows_here == (uint32_t)BC_TILE_ROWS && bulk_rows == (uint32_t)BC_TILE_ROWS) {
+      // an interior tile: the warp's PER values (and dimension reads) first,
+      // then their bins
+      constexpr uint32_t PER = BC_TILE_WORDS / (BL_THREADS / 32);
+      using VT = typename std::conditional<((JOIN ? DW : W) <= 4), uint32_t, uint64_t>::type;
+      VT v[PER];
+      bool ok[PER];
+#pragma unroll
+      for (uint32_t k = 0; k < PER; ++k) {
+        ok[k] = true;
+        v[k] = (VT)lv_value<JOIN, DW>(dim, dimsz, ld_smem_w<W>(sp, (warp + k * nwarps) * 32 + lane), ok[k]);
       }
-      for (uint32_t l = 0; l < NL; ++l)
-        atomicOr(&tiles[lv_word(S.row0[l] + ((bins >> (8 * l)) & 0xffu), wi)], bit);
+#pragma unroll
+      for (uint32_t k = 0; k < PER; ++k) {
+        const uint32_t wi = warp + k * nwarps;
+        if (JOIN) {
+          if (jo.dout) lv_store<DW>(jo.dout, row0 + wi * 32 + lane, v[k]);
+          nbad += ok[k] ? 0u : 1u;
+        }
+        const uint32_t bins =
+            (ok[k] && (uint64_t)v[k] - S.dom_lo < (uint64_t)S.dom_n) ? lut[(uint32_t)((uint64_t)v[k] - S.dom_lo)] : S.nobin;
+#pragma unroll
+        for (int l = 0; l < NLC; ++l) atomicOr(&tiles[lv_word(rw[l] + ((bins >> (8 * l)) & 0xffu), wi)], bit);
+      }
+    } else {
+      for (uint32_t wi = warp; wi < BC_TILE_WORDS; wi += nwarps) {
+        const uint32_t r = wi * 32 + lane;
+        uint32_t bins = S.nobin;
+        if (r < rows_here) {
+          const uint64_t x = r < bulk_rows ? ld_smem_w<W>(sp, r) : load_width(col, row0 + r, W);
+          bool ok = true;
+          const uint64_t v = lv_value<JOIN, DW>(dim, dimsz, x, ok);
+          if (JOIN) {
+            if (jo.dout) lv_store<DW>(jo.dout, row0 + r, v);
+            nbad += ok ? 0u : 1u;
+          }
+          if (ok && v - S.dom_lo < (uint64_t)S.dom_n) bins = lut[(uint32_t)(v - S.dom_lo)];
+        }
+#pragma unroll
+        for (int l = 0; l < NLC; ++l) atomicOr(&tiles[lv_word(rw[l] + ((bins >> (8 * l)) & 0xffu), wi)], bit);
+      }
     }
     __syncthreads();  // stage s fully read, tiles complete
 
@@ -362,6 +421,10 @@ bitmap_levels_kernel(const __grid_constant__ LevelSpec S, const void *__restrict
       if (lane == 0 && c) cnt[g] += c;  // this warp owns row g in this tile
     }
     __syncthreads();  // tiles reused by the next tile
+  }
+  if (JOIN && jo.bad) {
+    nbad = __reduce_add_sync(0xffffffffu, nbad);
+    if (lane == 0 && nbad) atomicAdd(jo.bad, (unsigned long long)nbad);
   }
   __syncthreads();
   for (uint32_t g = tid; g < S.nrows_tile; g += BL_THREADS) {
@@ -427,8 +490,12 @@ static size_t levels_smem(const LevelSpec &S, int W) {
 }
 
 template <int W, bool JOIN, int DW>
-static mb_status launch_levels(const LevelSpec &S, const mb_src *src, uint64_t n, uint64_t stride, cudaStream_t st) {
-  auto kern = bitmap_levels_kernel<W, JOIN, DW>;
+static mb_status launch_levels(const LevelSpec &S, const mb_src *src, uint64_t n, uint64_t stride, cudaStream_t st,
+                               LevelsJoinOut jo) {
+  auto kern = S.nlevels == 1   ? bitmap_levels_kernel<W, JOIN, DW, 1>
+              : S.nlevels == 2 ? bitmap_levels_kernel<W, JOIN, DW, 2>
+              : S.nlevels == 3 ? bitmap_levels_kernel<W, JOIN, DW, 3>
+                               : bitmap_levels_kernel<W, JOIN, DW, 4>;
   const size_t smem = levels_smem(S, W);
   MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
@@ -441,7 +508,7 @@ static mb_status launch_levels(const LevelSpec &S, const mb_src *src, uint64_t n
   if (!errw) return fail(MB_ERR_OOM, "bitmap_create_levels: device error word");
   const void *colp = JOIN ? (const void *)src->fk : src->col;
   const void *dimp = JOIN ? src->col : nullptr;
-  kern<<<(unsigned)grid, BL_THREADS, smem, st>>>(S, colp, dimp, src->dimsz, n, stride, errw);
+  kern<<<(unsigned)grid, BL_THREADS, smem, st>>>(S, colp, dimp, src->dimsz, n, stride, errw, jo);
   MB_LAUNCH_CHECK("bitmap_levels_kernel");
   return MB_OK;
 }
@@ -560,8 +627,9 @@ extern "C" mb_status mb_bitmap_create(const mb_src *src, uint64_t nrows, const u
   return MB_OK;
 }
 
-extern "C" mb_status mb_bitmap_create_levels(const mb_src *src, uint64_t nrows, const mb_level *levels,
-                                             uint32_t nlevels, uint64_t stride_words, void *stream) {
+mb_status mb::bitmap_create_levels_join(const mb_src *src, uint64_t nrows, const mb_level *levels,
+                                        uint32_t nlevels, uint64_t stride_words, void *stream, void *dout,
+                                        unsigned long long *bad) {
   if (!src || (!levels && nlevels)) return fail(MB_ERR_INVALID, "mb_bitmap_create_levels: NULL argument");
   if (nlevels == 0) return MB_OK;
   const uint32_t w = src->width;
@@ -577,6 +645,8 @@ extern "C" mb_status mb_bitmap_create_levels(const mb_src *src, uint64_t nrows, 
   const void *staged = src->fk ? (const void *)src->fk : src->col;
   if (((uintptr_t)staged & 15) != 0)
     return fail(MB_ERR_INVALID, "mb_bitmap_create_levels: staged column not 16-byte aligned");
+  const bool join_out = dout || bad;
+  if (join_out && !src->fk) return fail(MB_ERR_INVALID, "bitmap levels: join outputs without a foreign key");
   if (nrows == 0) return MB_OK;
   cudaStream_t st = as_stream(stream);
   static thread_local LevelSpec S;  // 24 KB lookup table: not on the stack
@@ -584,22 +654,29 @@ extern "C" mb_status mb_bitmap_create_levels(const mb_src *src, uint64_t nrows, 
   const bool fast = levels_spec(levels, nlevels, S) && (w <= 4 || src->fk) &&
                     levels_smem(S, staged_w) <= (size_t)dev_info().max_smem_optin;
   if (!fast) {  // one pass per level
+    if (join_out) return fail(MB_ERR_INVALID, "bitmap levels: join outputs need the one-pass form");
     for (uint32_t l = 0; l < nlevels; ++l)
       MB_CHECK(mb_bitmap_create(src, nrows, levels[l].lo, levels[l].hi, levels[l].nbins, levels[l].out, stride_words,
                                 levels[l].popcounts, stream));
     return MB_OK;
   }
+  const LevelsJoinOut jo = {dout, bad};
   if (src->fk == nullptr) {
     switch (w) {
-    case 1: return launch_levels<1, false, 1>(S, src, nrows, stride_words, st);
-    case 2: return launch_levels<2, false, 1>(S, src, nrows, stride_words, st);
-    default: return launch_levels<4, false, 1>(S, src, nrows, stride_words, st);
+    case 1: return launch_levels<1, false, 1>(S, src, nrows, stride_words, st, jo);
+    case 2: return launch_levels<2, false, 1>(S, src, nrows, stride_words, st, jo);
+    default: return launch_levels<4, false, 1>(S, src, nrows, stride_words, st, jo);
     }
   }
   switch (w) {  // staged column is the 4-byte key; w is the dimension width
-  case 1: return launch_levels<4, true, 1>(S, src, nrows, stride_words, st);
-  case 2: return launch_levels<4, true, 2>(S, src, nrows, stride_words, st);
-  case 4: return launch_levels<4, true, 4>(S, src, nrows, stride_words, st);
-  default: return launch_levels<4, true, 8>(S, src, nrows, stride_words, st);
+  case 1: return launch_levels<4, true, 1>(S, src, nrows, stride_words, st, jo);
+  case 2: return launch_levels<4, true, 2>(S, src, nrows, stride_words, st, jo);
+  case 4: return launch_levels<4, true, 4>(S, src, nrows, stride_words, st, jo);
+  default: return launch_levels<4, true, 8>(S, src, nrows, stride_words, st, jo);
   }
+}
+
+extern "C" mb_status mb_bitmap_create_levels(const mb_src *src, uint64_t nrows, const mb_level *levels,
+                                             uint32_t nlevels, uint64_t stride_words, void *stream) {
+  return mb::bitmap_create_levels_join(src, nrows, levels, nlevels, stride_words, stream, nullptr, nullptr);
 }

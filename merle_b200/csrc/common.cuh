@@ -99,6 +99,14 @@ enum { MB_DEVERR_NONE = 0, MB_DEVERR_TMA_WAIT = 1, MB_DEVERR_IDLE_WAIT = 2 };
 uint32_t *device_error_word();   // per-device, allocated on first use
 mb_status check_device_error(cudaStream_t s);
 
+// mb_bitmap_create_levels over a foreign key that also writes every row's
+// dimension value to dout (dimension width; 0 where the key leaves the
+// dimension) and counts such rows in *bad (either may be NULL): the
+// denormalised column comes out of the same pass.  MB_ERR_INVALID when the
+// levels need more than one pass.
+mb_status bitmap_create_levels_join(const mb_src *src, uint64_t nrows, const mb_level *levels, uint32_t nlevels,
+                                    uint64_t stride_words, void *stream, void *dout, unsigned long long *bad);
+
 // ssbDateToYear (ssb/ssbdemo.h:28-39): day 0 = 1992-01-01.
 __host__ __device__ inline uint32_t date_to_year(uint32_t d) {
   // the year starts 0, 366, 731, 1096, 1461, 1827, 2192 (1992 and 1996 leap)

@@ -788,50 +788,16 @@ extern "C" mb_status mb_engine_build_index_levels(mb_engine *e, uint32_t flags, 
   MB_CHECK(E.alloc((void **)&E.islab, (size_t)E.nbm * E.stride * 4));
   const uint64_t nwords = (E.nrows + 31) / 32;
 
-  // The denormalisation (bound by its random dimension reads) runs on the
-  // side stream while the columns that do not read its output are indexed;
-  // the customer-city and part-mfgr columns wait for it.
-  struct Events {
-    cudaEvent_t fork = nullptr, join = nullptr;
-    ~Events() {
-      if (fork) cudaEventDestroy(fork);
-      if (join) cudaEventDestroy(join);
-    }
-  } ev;
   MB_CUDA(cudaEventRecord(E.ev0, E.stream));
-  if (denorm) {
-    if (!E.pstream) MB_CUDA(cudaStreamCreateWithFlags(&E.pstream, cudaStreamNonBlocking));
-    MB_CUDA(cudaEventCreateWithFlags(&ev.fork, cudaEventDisableTiming));
-    MB_CUDA(cudaEventCreateWithFlags(&ev.join, cudaEventDisableTiming));
-    MB_CUDA(cudaEventRecord(ev.fork, E.stream));
-    MB_CUDA(cudaStreamWaitEvent(E.pstream, ev.fork, 0));
-    MB_CHECK(E.enqueue_denorm(d_bad, E.pstream));
-    MB_CUDA(cudaEventRecord(ev.join, E.pstream));
-  }
+  MB_CUDA(cudaMemsetAsync(d_bad, 0, 16, E.stream));
   // only the padding words past each bitmap's end need clearing: the passes
   // write every word below it
   if (E.stride > nwords)
     MB_CUDA(cudaMemset2DAsync(E.islab + nwords, E.stride * 4, 0, (E.stride - nwords) * 4, E.nbm, E.stream));
   MB_CUDA(cudaMemsetAsync(d_pop, 0, (size_t)E.nbm * 8, E.stream));
   uint64_t first = 0;
-  std::vector<uint64_t> firsts;
-  for (auto &c : E.idx) {
-    firsts.push_back(first);
-    for (auto &l : c.levels) first += l.nbins();
-  }
-  // columns that read no denormalised column first
-  std::vector<int> order;
-  for (int pass = 0; pass < 2; ++pass)
-    for (int i = 0; i < IC_N; ++i)
-      if ((i == IC_CCITY || i == IC_MFGR) == (pass == 1)) order.push_back(i);
-  bool joined = false;
-  for (int ci : order) {
+  for (int ci = 0; ci < IC_N; ++ci) {
     IdxCol &c = E.idx[ci];
-    first = firsts[ci];
-    if (denorm && !joined && (ci == IC_CCITY || ci == IC_MFGR)) {
-      MB_CUDA(cudaStreamWaitEvent(E.stream, ev.join, 0));
-      joined = true;
-    }
     std::vector<std::vector<uint64_t>> lo(c.levels.size()), hi(c.levels.size());
     std::vector<mb_level> lv(c.levels.size());
     for (size_t i = 0; i < c.levels.size(); ++i) {
@@ -845,9 +811,24 @@ extern "C" mb_status mb_engine_build_index_levels(mb_engine *e, uint32_t flags, 
       lv[i].out = l.slab, lv[i].popcounts = d_pop + first;
       first += nb;
     }
+    const bool dn = denorm && (ci == IC_CCITY || ci == IC_MFGR);
+    if (!dn) {
+      MB_CHECK(mb_bitmap_create_levels(&c.src, E.nrows, lv.data(), (uint32_t)lv.size(), E.stride, E.stream));
+      continue;
+    }
+    // the column's levels through the foreign key; the same pass writes the
+    // denormalised column and counts keys outside the dimension
+    const mb_src js = ci == IC_CCITY ? join_src(E.custcity, E.custkey, E.ncust + 1, 1)
+                                     : join_src(E.partmfgr, E.partkey, E.npart + 1, 2);
+    void *dout = ci == IC_CCITY ? (void *)E.custcity_row : (void *)E.partmfgr_row;
+    const mb_status st = bitmap_create_levels_join(&js, E.nrows, lv.data(), (uint32_t)lv.size(), E.stride,
+                                                   E.stream, dout, d_bad + (ci == IC_CCITY ? 0 : 1));
+    if (st == MB_OK) continue;
+    if (st != MB_ERR_INVALID) return st;
+    // the levels need more than one pass: denormalise first, then index the column
+    MB_CHECK(E.enqueue_denorm(d_bad, E.stream));
     MB_CHECK(mb_bitmap_create_levels(&c.src, E.nrows, lv.data(), (uint32_t)lv.size(), E.stride, E.stream));
   }
-  if (denorm && !joined) MB_CUDA(cudaStreamWaitEvent(E.stream, ev.join, 0));
   MB_CUDA(cudaEventRecord(E.ev1, E.stream));
   std::vector<uint64_t> pops(E.nbm);
   unsigned long long bad[2] = {0, 0};
