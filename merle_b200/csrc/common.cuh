@@ -107,6 +107,32 @@ mb_status check_device_error(cudaStream_t s);
 mb_status bitmap_create_levels_join(const mb_src *src, uint64_t nrows, const mb_level *levels, uint32_t nlevels,
                                     uint64_t stride_words, void *stream, void *dout, unsigned long long *bad);
 
+// Unsigned 32-bit division by an invariant divisor d >= 1 as a multiply-high
+// and shifts (Granlund and Montgomery, "Division by Invariant Integers using
+// Multiplication", PLDI 1994, figure 4.1): with l = ceil(log2 d),
+// m = floor(2^32 * (2^l - d) / d) + 1, sh1 = min(l, 1), sh2 = max(l - 1, 0),
+// x / d = (t + ((x - t) >> sh1)) >> sh2 where t = mulhi(m, x).
+struct DivMagic {
+  uint32_t m, sh1, sh2;
+};
+inline DivMagic div_magic(uint32_t d) {
+  uint32_t l = 0;
+  while (l < 32 && (1ull << l) < d) ++l;
+  DivMagic r;
+  r.m = (uint32_t)((((1ull << l) - d) << 32) / d + 1);
+  r.sh1 = l < 1 ? l : 1;
+  r.sh2 = l > 0 ? l - 1 : 0;
+  return r;
+}
+__host__ __device__ inline uint32_t div_by_magic(uint32_t x, uint32_t m, uint32_t sh1, uint32_t sh2) {
+#ifdef __CUDA_ARCH__
+  const uint32_t t = __umulhi(m, x);
+#else
+  const uint32_t t = (uint32_t)(((uint64_t)m * x) >> 32);
+#endif
+  return (t + ((x - t) >> sh1)) >> sh2;
+}
+
 // ssbDateToYear (ssb/ssbdemo.h:28-39): day 0 = 1992-01-01.
 __host__ __device__ inline uint32_t date_to_year(uint32_t d) {
   // the year starts 0, 366, 731, 1096, 1461, 1827, 2192 (1992 and 1996 leap)
