@@ -42,11 +42,6 @@ OpNeeds op_needs(const mb_op &O) {
   uint32_t nt = 0;
   for (uint32_t c = 0; c < O.nclause; ++c) nt += O.clause_len[c];
   for (uint32_t t = 0; t < nt; ++t) n.filt_mask |= 1u << O.terms[t].src;
-  for (uint32_t k = 0; k < O.nkey && k < MB_MAXKEY; ++k)
-    if (O.keys[k].xform == MB_X_DIV && O.keys[k].div != 0) {
-      const DivMagic m = div_magic(O.keys[k].div);
-      n.kdm[k] = m.m, n.kds[k] = m.sh1 | (m.sh2 << 8);
-    }
   return n;
 }
 
@@ -89,8 +84,8 @@ __device__ __forceinline__ void load_row(const mb_op &O, uint32_t need, uint32_t
 }
 
 // The op over loaded values (the same semantics as op_eval in opeval.cuh).
-__device__ __forceinline__ bool eval_row(const mb_op &O, const OpNeeds &N, const uint32_t (&v)[MB_MAXSRC],
-                                         uint32_t bad, bool chk, uint32_t nr_grp, int64_t &value, uint32_t &group) {
+__device__ __forceinline__ bool eval_row(const mb_op &O, const uint32_t (&v)[MB_MAXSRC], uint32_t bad, bool chk,
+                                         uint32_t nr_grp, int64_t &value, uint32_t &group) {
   if (chk) {
     uint32_t t = 0;
     for (uint32_t c = 0; c < O.nclause; ++c) {
@@ -109,7 +104,7 @@ __device__ __forceinline__ bool eval_row(const mb_op &O, const OpNeeds &N, const
     const mb_key &kk = O.keys[k];
     if ((bad >> kk.src) & 1u) return false;
     uint32_t x = pick(v, kk.src);
-    if (kk.xform == MB_X_DIV) x = div_by_magic(x, N.kdm[k], N.kds[k] & 0xffu, N.kds[k] >> 8);
+    if (kk.xform == MB_X_DIV) x = x / kk.div;
     else if (kk.xform == MB_X_YEAR) x = date_to_year(x);
     g += kk.mul * (x - kk.base);
   }
@@ -270,8 +265,8 @@ __device__ __forceinline__ void drain64(const mb_op &O, const OpNeeds &N, const 
   load_row(O, ok1 ? (N.kv_mask | (c1 ? N.filt_mask : 0u)) : 0u, e1 & 0x7fffffffu, v1, bad1);
   int64_t val0 = 0, val1 = 0;
   uint32_t g0 = 0, g1 = 0;
-  const bool k0 = ok0 && eval_row(O, N, v0, bad0, c0, nr_grp, val0, g0);
-  const bool k1 = ok1 && eval_row(O, N, v1, bad1, c1, nr_grp, val1, g1);
+  const bool k0 = ok0 && eval_row(O, v0, bad0, c0, nr_grp, val0, g0);
+  const bool k1 = ok1 && eval_row(O, v1, bad1, c1, nr_grp, val1, g1);
   cnt += (k0 ? 1u : 0u) + (k1 ? 1u : 0u);
   aggregate<GS>(G, k0, g0, val0, acc);
   if (nrows_avail > 32) aggregate<GS>(G, k1, g1, val1, acc);

@@ -219,8 +219,6 @@ bool fused_warp_applies(const DevPrg &P, const mb_op &O);
 // rows need (filter terms).
 struct OpNeeds {
   uint32_t kv_mask, filt_mask;
-  uint32_t kdm[MB_MAXKEY];  // per MB_X_DIV key: magic multiplier of its divisor
-  uint32_t kds[MB_MAXKEY];  // and its shifts, sh1 | sh2 << 8
 };
 OpNeeds op_needs(const mb_op &O);
 mb_status fused_warp(const DevPrg &P, const mb_op &O, uint32_t nr_grp, int gs, uint32_t hcap, uint32_t V,
