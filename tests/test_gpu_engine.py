@@ -138,6 +138,43 @@ def test_engine_width4_and_host_load(cuda, star, orc, mb):
     eh.close()
 
 
+def test_engine_keys_outside_dimension(cuda, star, orc, mb):
+    """A loaded table whose customer and part keys partly leave their
+    dimensions: the index build's join passes count those keys, the engine
+    keeps probing through the keys instead of denormalised columns, and the
+    plans and the batched scan answer as the oracle (such rows are
+    eliminated)."""
+    import copy
+    s = star.narrow()
+    b = copy.copy(s)
+    b.cols = {k: v.copy() for k, v in s.cols.items()}
+    b.cols["custkey"][::97] = len(s.custcity) + 3
+    b.cols["partkey"][5::113] = len(s.partmfgr) + 11
+    n = star.n
+    h = abi.mb_star_host(nrows=n, ncust=len(s.custcity), nsupp=len(s.suppcity), npart=len(s.partmfgr))
+    for f in ("custkey", "partkey", "orderdate", "extendedprice", "revenue", "supplycost", "quantity", "discount",
+              "suppcity"):
+        setattr(h, f, b.cols[f].ctypes.data)
+    h.custcity = s.custcity.ctypes.data
+    h.partmfgr = s.partmfgr.ctypes.data
+    e = Engine(0)
+    try:
+        e.load_star(h)
+        e.build_index()
+        assert e.info()["denorm_bytes"] == 0  # the keys are probed
+        qs = WL.ssb13() + WL.random_mix(11, 12)
+        wants = [oracle_query(orc, b, q) for q in qs]
+        for q, (want, nqw) in zip(qs, wants):
+            out, nq, _ = e.query(q)
+            np.testing.assert_array_equal(out, want, err_msg=str(WL.as_tuple(q)))
+            assert nq == nqw
+        out, nq = e.query_batch(qs)
+        np.testing.assert_array_equal(out, np.concatenate([w for w, _ in wants]))
+        np.testing.assert_array_equal(nq, np.array([x for _, x in wants], np.uint64))
+    finally:
+        e.close()
+
+
 def test_engine_errors(eng, mb):
     out = np.zeros(8, np.int64)
     q = abi.query(9, 1, 2)
