@@ -486,21 +486,33 @@ def main():
     check(L.mb_engine_query_batch(eng.handle, qarr, Q, e2e_opts, res_host.ctypes.data, nq_host.ctypes.data))
     if world > 1:
         dist.barrier()
+    def e2e_combine():
+        # the shards' host answers summed over the ranks (the whole table's
+        # answer on every rank): host -> device, all-reduce, device -> host
+        if world > 1:
+            t_out = torch.from_numpy(res_host).cuda()
+            t_nq = torch.from_numpy(nq_host.view(np.int64)).cuda()
+            shard.combine(t_out, t_nq)
+            res_host[:] = t_out.cpu().numpy()
+            nq_host.view(np.int64)[:] = t_nq.cpu().numpy()
+
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
         check(L.mb_engine_query_batch(eng.handle, qarr, Q, e2e_opts, res_host.ctypes.data, nq_host.ctypes.data))
+        e2e_combine()
     e2e_ms = float((time.perf_counter() - t0) * 1e3)
     if world > 1:
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e = {"value": rows_total * Q * args.e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
-           "h2d_bytes_per_step": C.sizeof(abi.mb_query) * Q + BATCH_HDR_BYTES,
-           "d2h_bytes_per_step": 8 * total_g + 8 * Q,
+           "h2d_bytes_per_step": C.sizeof(abi.mb_query) * Q + BATCH_HDR_BYTES + (8 * total_g + 8 * Q if world > 1 else 0),
+           "d2h_bytes_per_step": (8 * total_g + 8 * Q) * (2 if world > 1 else 1),
            "api": "mb_engine_query_batch (host query descriptors in, the batch planned by the engine's network, "
-                  "host int64 group sums and row counts out, returns when they are on the host)",
+                  "host int64 group sums and row counts out, returns when they are on the host; with N GPUs "
+                  "the ranks' host answers are then summed by an all-reduce, inside the timed region)",
            "timing": "host wall clock around each call", "ms_per_step": e2e_ms / args.e2e_steps}
-    e2e_same = bool(np.array_equal(res_host, batch_out.cpu().numpy())) if world == 1 else None
+    e2e_same = bool(np.array_equal(res_host, batch_out.cpu().numpy()))
 
     # ---- the batch plans of this mix, timed (CUDA-graph replays): regret
     # of the chosen plan and its speedup over the rule-planned batch
