@@ -432,20 +432,17 @@ __device__ __forceinline__ void b_rows(const BCtx &C, uint32_t q, uint32_t (&p)[
     if (total == 0) break;
     uint32_t pos = incl - take;
     cnt -= take;
-    for (uint32_t t = 0; t < take; ++t) {
-      uint32_t k = 0;
+    uint32_t left = take;
 #pragma unroll
-      for (int kk = V - 1; kk >= 0; --kk)
-        if (p[kk]) k = kk;
-      uint32_t m = p[0], um = u[0];
-#pragma unroll
-      for (int kk = 1; kk < V; ++kk)
-        if (k == (uint32_t)kk) m = p[kk], um = u[kk];
-      const uint32_t b = __ffs(m) - 1;
-#pragma unroll
-      for (int kk = 0; kk < V; ++kk)
-        if (k == (uint32_t)kk) p[kk] &= p[kk] - 1;
-      buf[pos++] = (rowbase + k * 32 + b) | (((um >> b) & 1u) << 31);
+    for (int kk = 0; kk < V; ++kk) {
+      uint32_t mm = p[kk];
+      while (mm && left) {
+        const uint32_t b = __ffs(mm) - 1;
+        mm &= mm - 1;
+        --left;
+        buf[pos++] = (rowbase + kk * 32 + b) | (((u[kk] >> b) & 1u) << 31);
+      }
+      p[kk] = mm;
     }
     __syncwarp();
     for (uint32_t i0 = 0; i0 < total; i0 += 32 * R) {
