@@ -52,20 +52,21 @@ namespace {
 constexpr uint32_t BT_THREADS_MAX = BW_MAX * 32;
 constexpr uint32_t BT_NOTABLE = 0xffffffffu;
 
-constexpr uint32_t BT_BUF = 256;  // rows a warp compacts per (query, tile) through shared memory
+constexpr uint32_t BT_BUF = 256;  // rows of a warp's chunk buffer (or 1024 where shared memory allows)
 
 
 // Shared-memory layout of one launch (identical on host and device).
 struct BLayout {
   uint32_t off_Q, off_src, off_sum, off_cnt, off_toff, off_bar, off_ctr, off_order, off_chain, off_conj, off_stab,
-      off_buf, off_stage, stage_words, total;
+      off_buf, off_stage, stage_words, total, buf;
 };
 
 __host__ __device__ inline uint32_t align_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 
 __host__ __device__ inline BLayout blayout(uint32_t nq, uint32_t nchain, uint32_t nconj, uint32_t nu, uint32_t S,
-                                           uint32_t T, uint32_t nstab, uint32_t nw) {
+                                           uint32_t T, uint32_t nstab, uint32_t nw, uint32_t buf) {
   BLayout L;
+  L.buf = buf ? buf : BT_BUF;
   uint32_t o = 0;
   L.off_Q = o;
   o += nq * BQD_WORDS * 4;
@@ -90,7 +91,7 @@ __host__ __device__ inline BLayout blayout(uint32_t nq, uint32_t nchain, uint32_
   L.off_stab = o = align_up(o, 16);  // 64-bit atomics: 8-byte aligned at least
   o += nstab * 8;
   L.off_buf = o = align_up(o, 16);
-  o += nw * BT_BUF * 4;
+  o += nw * L.buf * 4;
   L.off_stage = o = align_up(o, 128);
   L.stage_words = nu * T;
   o += S * L.stage_words * 4;
@@ -409,10 +410,10 @@ struct BDrainAny {
 // but a chunk's last is full however unevenly the rows fall on the lanes
 // (6 % faster over the selectivity-spanning mix than draining dense words
 // by each lane's lowest set bit).
-template <class DR, int V, int R>
+template <class DR, int V, int R, int CH>
 __device__ __forceinline__ void b_rows(const BCtx &C, uint32_t q, uint32_t (&p)[V], const uint32_t (&u)[V],
                                        uint32_t rowbase, uint32_t *buf) {
-  constexpr uint32_t CH = BT_BUF / 32;  // rows a lane adds to the buffer per chunk
+  // CH: rows a lane adds to the buffer per chunk (the buffer holds 32 * CH)
   const uint32_t lane = threadIdx.x & 31;
   uint32_t cnt = 0;
 #pragma unroll
@@ -481,7 +482,7 @@ __device__ __forceinline__ void lds_words(const uint32_t *p, uint32_t (&x)[V]) {
 // Query q on the staged tile (words w0 + lane*V + k of the table; word
 // lane*V + k of the stage): the conjunctive chain, then the op on its
 // selected rows.
-template <int V>
+template <int V, int CH>
 __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, const uint32_t *conj,
                                         const uint32_t *stage, uint64_t w0,
                                         uint64_t nwords, uint32_t tail, uint32_t q, uint32_t *buf) {
@@ -545,15 +546,15 @@ __device__ __forceinline__ void b_query(const BCtx &C, const uint16_t *chain, co
   const uint32_t rowbase = (uint32_t)((w0 + lane * V) * 32);  // first row of the lane's words
   // word 7: slots read through a foreign key (generic drain); word 6: shape
   switch (C.Qd[q * BQD_WORDS + 7] ? 0u : C.Qd[q * BQD_WORDS + 6]) {
-  case 1: b_rows<BDrain<0>, V, 1>(C, q, p, u, rowbase, buf); break;
-  case 2: b_rows<BDrain<1>, V, 1>(C, q, p, u, rowbase, buf); break;
-  case 3: b_rows<BDrain<2>, V, 1>(C, q, p, u, rowbase, buf); break;
-  case 4: b_rows<BDrain<3>, V, 1>(C, q, p, u, rowbase, buf); break;
-  default: b_rows<BDrainAny, V, 1>(C, q, p, u, rowbase, buf); break;
+  case 1: b_rows<BDrain<0>, V, 1, CH>(C, q, p, u, rowbase, buf); break;
+  case 2: b_rows<BDrain<1>, V, 1, CH>(C, q, p, u, rowbase, buf); break;
+  case 3: b_rows<BDrain<2>, V, 1, CH>(C, q, p, u, rowbase, buf); break;
+  case 4: b_rows<BDrain<3>, V, 1, CH>(C, q, p, u, rowbase, buf); break;
+  default: b_rows<BDrainAny, V, 1, CH>(C, q, p, u, rowbase, buf); break;
   }
 }
 
-template <int V>
+template <int V, int CH>
 __global__ void __launch_bounds__(BT_THREADS_MAX, 1)
 batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParams P,
                   const CUtensorMap *__restrict__ maps, unsigned long long *__restrict__ out,
@@ -575,7 +576,7 @@ batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParam
   uint16_t *chain = reinterpret_cast<uint16_t *>(smem + L.off_chain);
   uint32_t *conj = reinterpret_cast<uint32_t *>(smem + L.off_conj);
   unsigned long long *stab = reinterpret_cast<unsigned long long *>(smem + L.off_stab);
-  uint32_t *wbuf = reinterpret_cast<uint32_t *>(smem + L.off_buf) + warp * BT_BUF;
+  uint32_t *wbuf = reinterpret_cast<uint32_t *>(smem + L.off_buf) + warp * L.buf;
   uint32_t *stages = reinterpret_cast<uint32_t *>(smem + L.off_stage);
 
   for (uint32_t i = tid; i < P.nq * BQD_WORDS; i += blockDim.x) Qd[i] = H->Qd[i];
@@ -686,7 +687,7 @@ batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParam
         if (lane == 0) qi = atomicAdd(&qctr[s], 1u);
         qi = __shfl_sync(0xffffffffu, qi, 0);
         if (qi >= P.nq) break;
-        b_query<V>(C, chain, conj, st, w0, P.nwords, tail, order[qi], wbuf);
+        b_query<V, CH>(C, chain, conj, st, w0, P.nwords, tail, order[qi], wbuf);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
@@ -714,7 +715,8 @@ batch_scan_kernel(const BatchHdr *__restrict__ H, const __grid_constant__ BParam
 size_t batch_smem(const BatchHdr &h, const BatchCfg &c) {
   if (c.V != 1 && c.V != 2 && c.V != 4 && c.V != 6) return 0;
   if (c.warps < 2 || c.warps > BW_MAX || c.stages == 0 || c.stages > 4) return 0;  // a producer and workers
-  return blayout(h.nq, h.nchain, h.nconj, h.nu, c.stages, 32 * c.V, h.nstab, c.warps).total;
+  if (c.buf != 0 && c.buf != BT_BUF && c.buf != 1024) return 0;
+  return blayout(h.nq, h.nchain, h.nconj, h.nu, c.stages, 32 * c.V, h.nstab, c.warps, c.buf).total;
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
@@ -750,7 +752,7 @@ mb_status batch_encode_maps(const uint32_t *slab, uint64_t stride, uint32_t nsla
 template <int V>
 static mb_status launch_bs(const BatchHdr &h, const BatchHdr *dh, const BatchCfg &c, const void *maps, int64_t *out,
                            uint64_t *nqual, cudaStream_t st) {
-  auto kern = batch_scan_kernel<V>;
+  auto kern = c.buf == 1024 ? batch_scan_kernel<V, 32> : batch_scan_kernel<V, BT_BUF / 32>;
   BParams P;
   memset(&P, 0, sizeof(P));
   P.nrows = h.nrows;
@@ -767,7 +769,7 @@ static mb_status launch_bs(const BatchHdr &h, const BatchHdr *dh, const BatchCfg
   P.S = c.stages;
   P.wait_tries = c.wait_tries ? c.wait_tries : (1u << 20);
   P.skip_stage0 = c.skip_stage0;
-  P.L = blayout(h.nq, h.nchain, h.nconj, h.nu, c.stages, 32 * V, h.nstab, c.warps);
+  P.L = blayout(h.nq, h.nchain, h.nconj, h.nu, c.stages, 32 * V, h.nstab, c.warps, c.buf);
   // the 64-bit areas (sums, counts, group tables, mbarriers) must be 8-byte
   // aligned, the stage 128-byte aligned (tensor copies): refuse a layout that
   // is not, rather than launch it

@@ -111,6 +111,7 @@ struct BatchCfg {
   uint32_t cps;     // CTAs per SM (0: as many as fit)
   uint32_t wait_tries;   // try limit of a stage wait (0: 2^20, about a second)
   uint32_t skip_stage0;  // tests only: the first stage is armed and never filled, so its wait runs out
+  uint32_t buf;          // rows of a worker warp's chunk buffer: 256 (or 0) or 1024
 };
 
 // Tensor maps of a bitmap slab for one tile width T (words): map h - 1 has

@@ -1353,8 +1353,22 @@ static double est_selectivity(const Engine &E, const Lowered &L) {
 }
 
 // The most stages (up to smax) of shape c that fit in shared memory.
+// Stages and chunk buffers of a launch shape: the larger buffer (1,024, then
+// 256 rows a warp) that fits beside at least two stages (or the
+// stages asked for, if fewer), the most stages (up to smax) beside it; else
+// 256-row buffers and whatever number of stages fits.  (Larger buffers make
+// fewer, fuller drain chunks: 1,024 rows and two stages measured 4 % faster
+// than 256 rows and three stages on the 600M-row selectivity-spanning mix.)
 static bool fit_stages(const BatchHdr &h, BatchCfg &c, uint32_t smax) {
   const size_t cap = (size_t)dev_info().max_smem_optin;
+  const uint32_t smin = smax < 2 ? smax : 2u;
+  for (uint32_t buf : {1024u, 256u})
+    for (c.stages = smax; c.stages >= smin; --c.stages) {
+      c.buf = buf;
+      const size_t b = batch_smem(h, c);
+      if (b && b <= cap) return true;
+    }
+  c.buf = 256;
   for (c.stages = smax; c.stages >= 1; --c.stages) {
     const size_t b = batch_smem(h, c);
     if (b && b <= cap) return true;
