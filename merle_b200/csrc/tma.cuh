@@ -1,6 +1,7 @@
-// tma.cuh - 1-D TMA bulk copies (cp.async.bulk) global -> shared with mbarrier
-// completion, and a bounded mbarrier wait.  Single-GPU, CTA-local only: no
-// cluster multicast anywhere in this library.
+// tma.cuh - TMA bulk and tensor copies (cp.async.bulk, cp.async.bulk.tensor)
+// global -> shared with mbarrier completion, and a bounded mbarrier wait.
+// Every copy lands in the issuing CTA's own shared memory, from this GPU's
+// memory.
 #pragma once
 #include <cuda.h>
 #include <stdint.h>
